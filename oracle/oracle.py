@@ -1,0 +1,347 @@
+"""ctypes front end to the CPU oracle (TEST INFRASTRUCTURE ONLY).
+
+Two libraries sit under ``oracle/_ref/`` after ``make -C oracle all ref``:
+
+* ``libmbir_oracle.so`` -- the C restatement of the phasecon MBIR_4D hot path
+  (oracle/mbir_oracle.c, each function citing the reference file:line it
+  restates);
+* ``libref_mbir4d.so`` -- the reference C itself, built from its own sources
+  with a single-rank MPI shim (oracle/Makefile, oracle/ref_harness.c).
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline
+leg may import this module, as the checker or the timed CPU baseline.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from dataclasses import dataclass, field
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(HERE, "_ref")
+RESP_BINS = 64
+
+_f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+_i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+_u8p = np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")
+
+
+class OrcGeom(C.Structure):
+    _fields_ = [
+        ("N_r", C.c_int32), ("N_t", C.c_int32), ("N_p", C.c_int32), ("z_overlap", C.c_int32),
+        ("delta_r", C.c_double), ("delta_t", C.c_double), ("R0", C.c_double), ("RMax", C.c_double),
+        ("T0", C.c_double), ("TMax", C.c_double), ("OffsetR", C.c_double), ("OffsetT", C.c_double),
+        ("N_time", C.c_int32), ("N_x", C.c_int32), ("N_y", C.c_int32), ("N_z", C.c_int32),
+        ("mult_xy", C.c_int32), ("mult_z", C.c_int32),
+        ("x0", C.c_double), ("y0", C.c_double), ("z0", C.c_double), ("delta_xy", C.c_double),
+        ("delta_z", C.c_double), ("delta_recon", C.c_double), ("radius_obj", C.c_double),
+        ("p", C.c_double), ("q", C.c_double), ("alpha", C.c_double), ("c_s", C.c_double), ("c_t", C.c_double),
+        ("sigma_s_q", C.c_double), ("sigma_s_q_p", C.c_double), ("sigma_t_q", C.c_double),
+        ("sigma_t_q_p", C.c_double),
+        ("spatial_filter", C.c_double * 27), ("time_filter", C.c_double),
+        ("huber_T", C.c_double), ("huber_delta", C.c_double),
+        ("num_z_blocks", C.c_int32),
+    ]
+
+
+class RefProblem(C.Structure):
+    """Mirror of RefProblem in oracle/ref_harness.c."""
+    _fields_ = [
+        ("projections", C.c_void_p), ("weights", C.c_void_p), ("proj_angles", C.c_void_p),
+        ("proj_times", C.c_void_p), ("recon_times", C.c_void_p),
+        ("proj_rows", C.c_int32), ("proj_cols", C.c_int32), ("proj_num", C.c_int32), ("recon_num", C.c_int32),
+        ("vox_wid", C.c_float), ("rot_center", C.c_float), ("sig_s", C.c_float), ("sig_t", C.c_float),
+        ("c_s", C.c_float), ("c_t", C.c_float), ("convg_thresh", C.c_float),
+        ("quad_convex", C.c_int32), ("huber_delta", C.c_float), ("huber_T", C.c_float),
+        ("mult_xy", C.c_int32), ("mult_z", C.c_int32),
+    ]
+
+
+@dataclass
+class Problem:
+    """One reconstruction problem in the reference's ABI layout.
+
+    projections/weights are [proj_num][proj_rows][proj_cols] (col fastest), as
+    passed to ``reconstruct`` (MBIR_4D/XT_Engine.c:81).
+    """
+    projections: np.ndarray
+    weights: np.ndarray
+    proj_angles: np.ndarray
+    proj_times: np.ndarray
+    recon_times: np.ndarray
+    proj_rows: int
+    proj_cols: int
+    proj_num: int
+    recon_num: int
+    vox_wid: float = 1.0
+    rot_center: float = 0.0
+    sig_s: float = 0.01
+    sig_t: float = 1.0
+    c_s: float = 1.0
+    c_t: float = 1.0
+    convg_thresh: float = 0.0
+    quad_convex: int = 1
+    huber_delta: float = 0.5
+    huber_T: float = 4.0
+    mrf_p: float = 1.2
+    _keep: list = field(default_factory=list, repr=False)
+
+    def ref_struct(self, mult_xy: int = 1, mult_z: int = 1) -> RefProblem:
+        arrs = [np.ascontiguousarray(a, dtype=np.float32) for a in
+                (self.projections, self.weights, self.proj_angles, self.proj_times, self.recon_times)]
+        self._keep = arrs
+        return RefProblem(*(a.ctypes.data for a in arrs), self.proj_rows, self.proj_cols, self.proj_num,
+                          self.recon_num, self.vox_wid, self.rot_center, self.sig_s, self.sig_t, self.c_s,
+                          self.c_t, self.convg_thresh, self.quad_convex, self.huber_delta, self.huber_T,
+                          mult_xy, mult_z)
+
+
+def build(with_reference: bool | None = None) -> None:
+    """Build the oracle libraries (the reference only where its sources exist)."""
+    subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
+    if with_reference is None:
+        with_reference = os.path.isdir("/root/reference/Source_Code/MBIR_4D")
+    if with_reference:
+        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+
+
+_orc = None
+_ref = None
+
+
+def orc_lib() -> C.CDLL:
+    global _orc
+    if _orc is None:
+        path = os.path.join(REF_DIR, "libmbir_oracle.so")
+        if not os.path.exists(path):
+            build(with_reference=False)
+        lib = C.CDLL(path)
+        P = C.POINTER(OrcGeom)
+        lib.orc_init_geometry.argtypes = [P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_double,
+                                          C.c_double, C.c_double, C.c_double, C.c_double, C.c_int32, C.c_int32,
+                                          C.c_double, C.c_int32, C.c_double, C.c_double, C.c_int32, _f32p, _f32p,
+                                          _i32p, _i32p]
+        lib.orc_init_geometry.restype = C.c_int
+        lib.orc_detector_response.argtypes = [P, _f32p, _f32p]
+        lib.orc_amatrix_column.argtypes = [P, _f32p, C.c_double, C.c_double, C.c_int32, C.c_int32, C.c_int32,
+                                           _i32p, _f64p]
+        lib.orc_amatrix_column.restype = C.c_int32
+        lib.orc_forward_project.argtypes = [P, _f32p, _f32p, _i32p, _i32p, _f32p, _f64p]
+        lib.orc_cost.argtypes = [P, _f32p, _f32p, _f32p, _f64p]
+        lib.orc_cost.restype = C.c_double
+        lib.orc_functional_substitution.argtypes = [P, C.c_double, C.c_double, C.c_double, _f64p, _u8p, _f64p,
+                                                    _u8p]
+        lib.orc_functional_substitution.restype = C.c_double
+        lib.orc_random2_sequence.argtypes = [C.c_uint32, C.c_int32, _f64p]
+        lib.orc_icd_pass.argtypes = [P, _f32p, _f32p, _i32p, _i32p, _u8p, _i32p, C.c_int32, C.c_int32, _f32p,
+                                     _f32p, _f32p]
+        lib.orc_icd_pass.restype = C.c_int64
+        _orc = lib
+    return _orc
+
+
+def ref_available() -> bool:
+    return os.path.exists(os.path.join(REF_DIR, "libref_mbir4d.so"))
+
+
+def ref_lib() -> C.CDLL:
+    global _ref
+    if _ref is None:
+        lib = C.CDLL(os.path.join(REF_DIR, "libref_mbir4d.so"))
+        P = C.POINTER(RefProblem)
+        lib.ref_set_options.argtypes = [C.c_double, C.c_int, C.c_int]
+        lib.ref_geometry.argtypes = [P, _f64p, _f64p, _f32p, _f32p, _i32p, _i32p]
+        lib.ref_amatrix.argtypes = [P, C.c_int32, _u8p, _i32p, _f64p]
+        lib.ref_error_sino_and_cost.argtypes = [P, _f32p, _f32p, _u8p, C.POINTER(C.c_double)]
+        lib.ref_functional_substitution.argtypes = [P, C.c_int32, _f64p, _f64p, _f64p, _f64p, _u8p, _f64p, _u8p,
+                                                    _f64p]
+        lib.ref_random2_sequence.argtypes = [C.c_uint32, C.c_int32, _f64p]
+        lib.ref_reconstruct.argtypes = [P, C.c_int32, C.POINTER(C.POINTER(C.c_float))]
+        lib.ref_reconstruct.restype = C.c_int
+        lib.ref_free.argtypes = [C.c_void_p]
+        lib.ref_vox_updates.restype = C.c_longlong
+        _ref = lib
+    return _ref
+
+
+# --------------------------------------------------------------------------- restatement
+
+
+class Oracle:
+    """Geometry plus the restated kernels for one problem at one voxel scale."""
+
+    def __init__(self, pb: Problem, mult_xy: int = 1, mult_z: int = 1, num_threads: int = 2):
+        lib = orc_lib()
+        self.pb = pb
+        self.g = OrcGeom()
+        self.proj_idx = np.zeros(pb.proj_num, np.int32)
+        self.proj_cnt = np.zeros(pb.recon_num, np.int32)
+        f = lambda v: float(np.float32(v))  # the ABI passes these as float (MBIR_4D/XT_Engine.c:81)
+        rc = lib.orc_init_geometry(C.byref(self.g), pb.proj_rows, pb.proj_cols, pb.proj_num, pb.recon_num,
+                                   f(pb.vox_wid), f(pb.rot_center), f(pb.sig_s), f(pb.sig_t), f(pb.c_s), f(pb.c_t),
+                                   mult_xy, mult_z, pb.mrf_p, pb.quad_convex, f(pb.huber_delta), f(pb.huber_T),
+                                   num_threads,
+                                   np.ascontiguousarray(pb.proj_times, np.float32),
+                                   np.ascontiguousarray(pb.recon_times, np.float32), self.proj_idx, self.proj_cnt)
+        if rc != 0:
+            raise ValueError("oracle geometry rejected the problem")
+        self.angles = np.ascontiguousarray(pb.proj_angles, np.float32)
+        self.H_r = np.zeros((pb.proj_num, RESP_BINS + 1), np.float32)
+        lib.orc_detector_response(C.byref(self.g), self.angles, self.H_r)
+        # internal [view][col][row] sinogram layout (MBIR_4D/XT_Init.c:292-301)
+        self.y = np.ascontiguousarray(pb.projections.reshape(pb.proj_num, pb.proj_rows, pb.proj_cols)
+                                      .transpose(0, 2, 1), np.float32)
+        self.w = np.ascontiguousarray(pb.weights.reshape(pb.proj_num, pb.proj_rows, pb.proj_cols)
+                                      .transpose(0, 2, 1), np.float32)
+
+    @property
+    def shape(self):
+        g = self.g
+        return (g.N_time, g.N_z, g.N_y, g.N_x)
+
+    def amatrix_column(self, view: int, row: int, col: int):
+        idx = np.zeros(64, np.int32)
+        val = np.zeros(64, np.float64)
+        a = float(self.angles[view])
+        n = orc_lib().orc_amatrix_column(C.byref(self.g), self.H_r, np.cos(np.float64(a)), np.sin(np.float64(a)),
+                                         view, row, col, idx, val)
+        return idx[:n].copy(), val[:n].copy()
+
+    def forward(self, obj: np.ndarray) -> np.ndarray:
+        ax = np.zeros((self.pb.proj_num, self.pb.proj_cols, self.pb.proj_rows), np.float64)
+        orc_lib().orc_forward_project(C.byref(self.g), self.H_r, self.angles, self.proj_idx, self.proj_cnt,
+                                      np.ascontiguousarray(obj, np.float32), ax)
+        return ax
+
+    def error_sino(self, obj: np.ndarray) -> np.ndarray:
+        return (self.y.astype(np.float64) - self.forward(obj)).astype(np.float32)
+
+    def cost(self, err: np.ndarray, obj: np.ndarray) -> tuple[float, float, float]:
+        parts = np.zeros(2, np.float64)
+        c = orc_lib().orc_cost(C.byref(self.g), np.ascontiguousarray(err, np.float32), self.w,
+                               np.ascontiguousarray(obj, np.float32), parts)
+        return c, parts[0], parts[1]
+
+    def mask(self) -> np.ndarray:
+        """Circular field-of-view mask of ICD_BackProject (XT_ICD_update.c:1127-1136)."""
+        g = self.g
+        k = np.arange(g.N_x, dtype=np.float64)
+        j = np.arange(g.N_y, dtype=np.float64)
+        x = g.x0 + (k + 0.5) * g.delta_xy
+        y = g.y0 + (j + 0.5) * g.delta_xy
+        return ((x[None, :] ** 2 + y[:, None] ** 2) < g.radius_obj * g.radius_obj).astype(np.uint8)
+
+    def icd_pass(self, obj: np.ndarray, err: np.ndarray, order: np.ndarray, it: int) -> int:
+        return int(orc_lib().orc_icd_pass(C.byref(self.g), self.H_r, self.angles, self.proj_idx, self.proj_cnt,
+                                          np.ascontiguousarray(self.mask()), np.ascontiguousarray(order, np.int32),
+                                          len(order), it, obj, err, self.w))
+
+    def functional_substitution(self, V, th1, th2, nhood, nflag, tnhood, tflag) -> float:
+        return orc_lib().orc_functional_substitution(C.byref(self.g), V, th1, th2,
+                                                     np.ascontiguousarray(nhood, np.float64),
+                                                     np.ascontiguousarray(nflag, np.uint8),
+                                                     np.ascontiguousarray(tnhood, np.float64),
+                                                     np.ascontiguousarray(tflag, np.uint8))
+
+
+def random2_sequence(seed: int, n: int) -> np.ndarray:
+    out = np.zeros(n, np.float64)
+    orc_lib().orc_random2_sequence(seed, n, out)
+    return out
+
+
+# --------------------------------------------------------------------------- reference (built from source)
+
+
+def ref_geometry(pb: Problem, mult_xy: int = 1, mult_z: int = 1):
+    lib = ref_lib()
+    lib.ref_set_options(pb.mrf_p, 1000, 0)
+    s = pb.ref_struct(mult_xy, mult_z)
+    scal = np.zeros(32, np.float64)
+    filt = np.zeros(27, np.float64)
+    H_r = np.zeros((pb.proj_num, RESP_BINS + 1), np.float32)
+    H_t = np.zeros(RESP_BINS + 1, np.float32)
+    idx = np.zeros(pb.proj_num, np.int32)
+    cnt = np.zeros(pb.recon_num, np.int32)
+    if lib.ref_geometry(C.byref(s), scal, filt, H_r, H_t, idx, cnt) != 0:
+        raise RuntimeError("reference initStructures failed")
+    return dict(scal=scal, filt=filt, H_r=H_r, H_t=H_t, proj_idx=idx, proj_cnt=cnt)
+
+
+def ref_amatrix(pb: Problem, mult_xy: int = 1, mult_z: int = 1):
+    lib = ref_lib()
+    lib.ref_set_options(pb.mrf_p, 1000, 0)
+    s = pb.ref_struct(mult_xy, mult_z)
+    n = pb.proj_cols // mult_xy
+    kmax = 2 * mult_xy + 1
+    count = np.zeros((pb.proj_num, n, n), np.uint8)
+    index = np.zeros((pb.proj_num, n, n, kmax), np.int32)
+    value = np.zeros((pb.proj_num, n, n, kmax), np.float64)
+    if lib.ref_amatrix(C.byref(s), kmax, count, index, value) != 0:
+        raise RuntimeError("reference A-matrix failed")
+    return count, index, value
+
+
+def ref_error_sino_and_cost(pb: Problem, obj: np.ndarray, mult_xy: int = 1, mult_z: int = 1):
+    lib = ref_lib()
+    lib.ref_set_options(pb.mrf_p, 1000, 0)
+    s = pb.ref_struct(mult_xy, mult_z)
+    err = np.zeros((pb.proj_num, pb.proj_cols, pb.proj_rows), np.float32)
+    sel = np.zeros(err.shape, np.uint8)
+    cost = C.c_double(0)
+    if lib.ref_error_sino_and_cost(C.byref(s), np.ascontiguousarray(obj, np.float32), err, sel,
+                                   C.byref(cost)) != 0:
+        raise RuntimeError("reference error sinogram failed")
+    return err, sel, cost.value
+
+
+def ref_functional_substitution(pb: Problem, V, th1, th2, nhood, nflag, tnhood, tflag):
+    lib = ref_lib()
+    lib.ref_set_options(pb.mrf_p, 1000, 0)
+    s = pb.ref_struct()
+    n = len(V)
+    out = np.zeros(n, np.float64)
+    lib.ref_functional_substitution(C.byref(s), n, np.ascontiguousarray(V, np.float64),
+                                    np.ascontiguousarray(th1, np.float64), np.ascontiguousarray(th2, np.float64),
+                                    np.ascontiguousarray(nhood, np.float64), np.ascontiguousarray(nflag, np.uint8),
+                                    np.ascontiguousarray(tnhood, np.float64), np.ascontiguousarray(tflag, np.uint8),
+                                    out)
+    return out
+
+
+def ref_random2_sequence(seed: int, n: int) -> np.ndarray:
+    out = np.zeros(n, np.float64)
+    ref_lib().ref_random2_sequence(seed, n, out)
+    return out
+
+
+def ref_reconstruct(pb: Problem, workdir: str, max_iter: int = 1000, num_stages: int = 0, threads: int = 0):
+    """Run the reference's ``reconstruct`` in ``workdir``.
+
+    Returns (object with halo [N_time][N_z+2][N_y][N_x] as the reference
+    returns it, FP64 cost per iteration from cost.bin, voxel updates counted).
+    """
+    lib = ref_lib()
+    lib.ref_set_options(pb.mrf_p, max_iter, num_stages)
+    lib.ref_reset_vox_updates()
+    s = pb.ref_struct()
+    out = C.POINTER(C.c_float)()
+    cwd = os.getcwd()
+    os.makedirs(workdir, exist_ok=True)
+    os.chdir(workdir)
+    try:
+        rc = lib.ref_reconstruct(C.byref(s), threads, C.byref(out))
+    finally:
+        os.chdir(cwd)
+    if rc != 0:
+        raise RuntimeError(f"reference reconstruct returned {rc}")
+    n = pb.recon_num * (pb.proj_rows + 2) * pb.proj_cols * pb.proj_cols
+    obj = np.ctypeslib.as_array(out, shape=(n,)).copy().reshape(pb.recon_num, pb.proj_rows + 2, pb.proj_cols,
+                                                                  pb.proj_cols)
+    lib.ref_free(out)
+    cost = np.fromfile(os.path.join(workdir, "cost.bin"), dtype=np.float64)
+    return obj, cost, int(lib.ref_vox_updates())
