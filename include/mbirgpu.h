@@ -1,0 +1,173 @@
+/*
+ * mbirgpu -- B200 (sm_100a) implementation of phasecon's MBIR hot path.
+ *
+ * C ABI of libmbirgpu.so (phasecon_b200/libmbirgpu.so). Plain pointers and
+ * sizes only. Every function returns 0 on success and -1 on failure, like the
+ * reference's check_error/goto error convention (MBIR_4D/XT_Debug.h:22); the
+ * message of the last failure on the calling thread is mbirgpu_last_error().
+ * All pointers are HOST pointers unless the parameter name starts with d_.
+ *
+ * Paths cited below are relative to the phasecon project root.
+ */
+#ifndef MBIRGPU_H
+#define MBIRGPU_H
+
+#include <stdint.h>
+#include <stdio.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* --------------------------------------------------------------------------
+ * Drop-in entry point.
+ *
+ * Replaces reconstruct() of MBIR_4D/XT_Engine.c:81 (declared void in
+ * include/mbir4d.h:35; defined int, returns 0 / -1). Same arguments, same
+ * meaning, same output: *object receives a malloc'ed buffer the caller
+ * free()s, laid out [recon_num][proj_rows+2][proj_cols][proj_cols] -- the
+ * reference returns its backing array with one halo slice above and below
+ * each frame's volume (MBIR_4D/XT_IOMisc.c:331-336, XT_Init.c:362-363); the
+ * halo slices are zero. Writes the reference's side-effect files in the
+ * working directory (object_time_<i>.bin, cost.bin, status.bin,
+ * variance_estimate.bin, mag_update.bin, proj_offset.bin) unless disabled by
+ * mbirgpu_set_options. remove_rings != 0 is rejected (ring correction is not
+ * built). restart = 1 resumes from status.bin like XT_Engine.c:143-150.
+ * No MPI is required.
+ * ------------------------------------------------------------------------ */
+int reconstruct(float **object, float *projections, float *weights, float *proj_angles, float *proj_times,
+                float *recon_times, int32_t proj_rows, int32_t proj_cols, int32_t proj_num, int32_t recon_num,
+                float vox_wid, float rot_center, float sig_s, float sig_t, float c_s, float c_t,
+                float convg_thresh, int32_t remove_rings, int32_t quad_convex, float huber_delta, float huber_T,
+                uint8_t restart, FILE *debug_msg_ptr);
+
+/* --------------------------------------------------------------------------
+ * Former compile-time constants of MBIR_4D/XT_Constants.h, now runtime.
+ * ------------------------------------------------------------------------ */
+typedef struct {
+    double mrf_p;            /* MRF_P (XT_Constants.h:62), default 1.2 */
+    double mrf_q;            /* MRF_Q (XT_Constants.h:63), default 2.0 */
+    double alpha;            /* OVER_RELAXATION_FACTOR (XT_Constants.h:87), default 1.5 */
+    int32_t max_iterations;  /* MAX_NUM_ITERATIONS (XT_Constants.h:86), default 1000 */
+    int32_t num_stages;      /* multi-resolution stages: 0 = reference plan (XT_Engine.c:111-141),
+                                n > 0 = the n finest stages of that plan */
+    double cost_rel_tol;     /* also stop a stage when |cost_k - cost_{k-1}| / |cost_k| < tol; 0 = off */
+    int32_t zero_skipping;   /* ZERO_SKIPPING (XT_Constants.h:47), default 1 */
+    int32_t write_files;     /* reference side-effect files, default 1 */
+    int32_t compute_cost;    /* FP64 MAP cost every iteration (cost.bin), default 1 */
+    int32_t refresh_every;   /* FP64 recomputation of e = y - Ax every n iterations, default 4 */
+    int32_t sv_size;         /* super-voxel edge in voxel columns; 0 = autotuned */
+    int32_t cta_warps;       /* warps cooperating on one voxel column; 0 = autotuned */
+    uint64_t seed;           /* voxel-order seed */
+} mbirgpu_options;
+
+/* Defaults as listed above. */
+void mbirgpu_default_options(mbirgpu_options *opt);
+int mbirgpu_set_options(const mbirgpu_options *opt);
+int mbirgpu_get_options(mbirgpu_options *opt);
+const char *mbirgpu_last_error(void);
+
+/* --------------------------------------------------------------------------
+ * Session API: one problem resident in GPU memory at one voxel scale.
+ *
+ * The problem fields carry the same meaning as reconstruct()'s arguments
+ * (MBIR_4D/XT_Engine.c:50-80). A session is one stage of the reference's
+ * multi-resolution loop: initStructures (MBIR_4D/XT_Init.c:211-432) plus the
+ * state ICD_BackProject keeps (XT_ICD_update.c:1095-1230).
+ * Device layouts: sinograms [N_p][N_r][N_t] (t fastest, as the reference's
+ * internal arrays, XT_Init.c:292-301); the object [N_time][N_y][N_x][N_z]
+ * (z fastest). Host object buffers exchanged through this API use the
+ * reference's volume order [N_time][N_z][N_y][N_x] without halo.
+ * ------------------------------------------------------------------------ */
+typedef struct mbirgpu_session mbirgpu_session;
+
+typedef struct {
+    const float *projections; /* [proj_num][proj_rows][proj_cols] */
+    const float *weights;     /* [proj_num][proj_rows][proj_cols] */
+    const float *proj_angles; /* [proj_num], radians */
+    const float *proj_times;  /* [proj_num], nondecreasing */
+    const float *recon_times; /* [recon_num + 1] frame edges */
+    int32_t proj_rows, proj_cols, proj_num, recon_num;
+    float vox_wid, rot_center, sig_s, sig_t, c_s, c_t, convg_thresh;
+    int32_t quad_convex;
+    float huber_delta, huber_T;
+} mbirgpu_problem;
+
+typedef struct {
+    int32_t N_r, N_t, N_p, N_time, N_x, N_y, N_z, mult_xy, mult_z;
+    int32_t max_views;       /* most views in one frame */
+    int32_t kmax;            /* most detector channels one voxel column hits per view */
+    int32_t sv_size, cta_warps;
+    int64_t masked_columns;  /* voxel columns inside the reconstruction circle, all frames */
+    int64_t nnz;             /* A-matrix nonzeros over all frames (x z_overlap per slice) */
+    double delta_t;
+    size_t device_bytes;     /* device memory the session holds */
+} mbirgpu_session_info;
+
+typedef struct {
+    int64_t voxel_updates;   /* updates that ran (zero-skipped ones excluded) */
+    int64_t zero_skipped;
+    double sum_abs_update;   /* sum |x_new - x_old| */
+    double sum_abs_value;    /* sum |x_new| over updated voxels */
+    double kernel_ms;        /* device time of the ICD sweep kernels (when timing is on) */
+    int32_t kernel_launches;
+} mbirgpu_iter_stats;
+
+/* Replaces initStructures + DetectorResponseProfile (MBIR_4D/XT_Init.c:211,
+ * XT_Profile.c:129) for one stage with voxel scale (mult_xy, mult_z), and
+ * builds the compressed A-matrix table on the device. stream may be NULL
+ * (the default stream) or a cudaStream_t every launch of the session uses. */
+int mbirgpu_session_create(mbirgpu_session **out, const mbirgpu_problem *pb, const mbirgpu_options *opt,
+                           int32_t mult_xy, int32_t mult_z, void *stream);
+int mbirgpu_session_destroy(mbirgpu_session *s);
+int mbirgpu_session_info_get(const mbirgpu_session *s, mbirgpu_session_info *info);
+int mbirgpu_session_set_stream(mbirgpu_session *s, void *stream);
+int mbirgpu_session_set_timing(mbirgpu_session *s, int32_t enable);
+
+/* Object upload / download, [N_time][N_z][N_y][N_x] without halo. */
+int mbirgpu_session_set_object(mbirgpu_session *s, const float *object);
+int mbirgpu_session_get_object(mbirgpu_session *s, float *object);
+/* Device pointer to the resident object ([N_time][N_y][N_x][N_z]). */
+int mbirgpu_session_object_device(mbirgpu_session *s, float **d_object);
+
+/* Replaces initErrorSinogam (MBIR_4D/XT_ICD_update.c:651-712): e = y - A x
+ * with the projection accumulated in FP64; also the periodic refresh. */
+int mbirgpu_session_refresh_error(mbirgpu_session *s);
+int mbirgpu_session_get_error(mbirgpu_session *s, float *err); /* [N_p][N_r][N_t] */
+
+/* Replaces computeCost (MBIR_4D/XT_ICD_update.c:185-318); FP64. */
+int mbirgpu_session_cost(mbirgpu_session *s, double *total, double *data_term, double *prior_term);
+
+/* One ICD iteration: every voxel column inside the reconstruction circle of
+ * every frame updated once, super-voxel parallel. Replaces
+ * updateVoxelsTimeSlices (MBIR_4D/XT_ICD_update.c:932-1092) with
+ * updateVoxels_Atten / compute_voxel_update_Atten (XT_VoxUpdate.c:45-283). */
+int mbirgpu_session_icd_iteration(mbirgpu_session *s, int32_t iter, mbirgpu_iter_stats *stats);
+
+/* Forward projection A x of a host object (no error, no weights) and the
+ * adjoint A^T s of a host sinogram, both FP64-accumulated; replaces
+ * forward_project_voxel_AMat1D (MBIR_4D/XT_ForwardProject.c:44-61) and the
+ * back-projection implicit in theta1 (XT_VoxUpdate.c:56-85). */
+int mbirgpu_session_forward_project(mbirgpu_session *s, const float *object, float *sino);
+int mbirgpu_session_back_project(mbirgpu_session *s, const float *sino, float *object);
+
+/* The device A-matrix table, for inspection: per (frame view, voxel column)
+ * the first detector channel, the count and kmax FP32 values.
+ * first/count: [N_p][N_y][N_x]; values: [N_p][N_y][N_x][kmax]. */
+int mbirgpu_session_get_amatrix(mbirgpu_session *s, int32_t *first, int32_t *count, float *values);
+
+/* H_r detector response [N_p][65] as built on the host (XT_Profile.c:129-218). */
+int mbirgpu_session_get_detector_response(mbirgpu_session *s, float *H_r);
+
+/* Run ICD iterations until the reference's convergence test
+ * (100 sum|dx| / sum|x| < convg_thresh after iteration 1, XT_ICD_update.c:1083-1090),
+ * the cost test of opt->cost_rel_tol, or max_iter. costs (may be NULL) gets
+ * the FP64 cost before iteration 1 and after each iteration; returns the
+ * iteration count in *iters. */
+int mbirgpu_session_run(mbirgpu_session *s, int32_t max_iter, double *costs, int32_t *iters,
+                        mbirgpu_iter_stats *total);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

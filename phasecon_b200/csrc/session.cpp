@@ -1,0 +1,617 @@
+// Session layer of libmbirgpu: one stage of one problem resident in GPU
+// memory, and the C ABI functions declared in include/mbirgpu.h that act on it.
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/mbirgpu.h"
+#include "mbir_internal.h"
+#include "session.h"
+
+namespace mbirgpu {
+
+thread_local std::string g_last_error;
+
+int fail(const char *fmt, ...)
+{
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return -1;
+}
+
+namespace {
+std::mutex g_opt_mu;
+mbirgpu_options g_opt;
+bool g_opt_init = false;
+}  // namespace
+
+mbirgpu_options current_options()
+{
+    std::lock_guard<std::mutex> lk(g_opt_mu);
+    if (!g_opt_init) {
+        mbirgpu_default_options(&g_opt);
+        g_opt_init = true;
+    }
+    return g_opt;
+}
+
+#define CK(call)                                                                               \
+    do {                                                                                       \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess) return fail("%s failed: %s", #call, cudaGetErrorString(e_)); \
+    } while (0)
+
+template <typename T>
+static int dalloc(T **p, size_t n, size_t *acc)
+{
+    *p = nullptr;
+    if (n == 0) n = 1;
+    cudaError_t e = cudaMalloc((void **)p, n * sizeof(T));
+    if (e != cudaSuccess) return fail("cudaMalloc of %zu bytes failed: %s", n * sizeof(T), cudaGetErrorString(e));
+    *acc += n * sizeof(T);
+    return 0;
+}
+
+Session::~Session()
+{
+    void *ptrs[] = {d_y, d_w, d_err, d_x, d_tmp, d_table, d_Hr, d_cos, d_sin, d_views, d_view_first, d_view_frame,
+                    d_mask, d_mag, d_stats, d_cost_partials, d_cost_out, d_flag};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    for (auto &ev : ev_pairs) {
+        cudaEventDestroy(ev.first);
+        cudaEventDestroy(ev.second);
+    }
+}
+
+int Session::init(const mbirgpu_problem *pb, const mbirgpu_options *o, int mult_xy, int mult_z, void *stream)
+{
+    opt = o ? *o : current_options();
+    st = (cudaStream_t)stream;
+    ProblemDesc pd{};
+    pd.proj_rows = pb->proj_rows;
+    pd.proj_cols = pb->proj_cols;
+    pd.proj_num = pb->proj_num;
+    pd.recon_num = pb->recon_num;
+    pd.vox_wid = pb->vox_wid;
+    pd.rot_center = pb->rot_center;
+    pd.sig_s = pb->sig_s;
+    pd.sig_t = pb->sig_t;
+    pd.c_s = pb->c_s;
+    pd.c_t = pb->c_t;
+    pd.quad_convex = pb->quad_convex;
+    pd.huber_delta = pb->huber_delta;
+    pd.huber_T = pb->huber_T;
+    pd.mrf_p = opt.mrf_p;
+    pd.mrf_q = opt.mrf_q;
+    pd.alpha = opt.alpha;
+    convg_thresh = pb->convg_thresh;
+    std::string msg = build_setup(hs, pd, pb->proj_angles, pb->proj_times, pb->recon_times, mult_xy, mult_z);
+    if (!msg.empty()) return fail("%s", msg.c_str());
+    const Geom &g = hs.g;
+    for (int f = 0; f < g.N_time; f++)
+        if (hs.view_first[f + 1] == hs.view_first[f])
+            return fail("Time frame %d has no projection views.", f);
+
+    n_sino = (size_t)g.N_p * g.N_r * g.N_t;
+    n_vox = (size_t)g.N_time * g.N_y * g.N_x * g.N_z;
+    const size_t nxy = (size_t)g.N_x * g.N_y;
+    const size_t table_words = (size_t)g.N_p * nxy * g.rec_words;
+    size_t &acc = device_bytes;
+    if (dalloc(&d_y, n_sino, &acc) || dalloc(&d_w, n_sino, &acc) || dalloc(&d_err, n_sino, &acc) ||
+        dalloc(&d_x, n_vox, &acc) || dalloc(&d_tmp, std::max(n_sino, n_vox), &acc) ||
+        dalloc(&d_table, table_words, &acc) || dalloc(&d_Hr, hs.H_r.size(), &acc) ||
+        dalloc(&d_cos, (size_t)g.N_p, &acc) || dalloc(&d_sin, (size_t)g.N_p, &acc) ||
+        dalloc(&d_views, (size_t)g.N_p, &acc) || dalloc(&d_view_first, (size_t)g.N_time + 1, &acc) ||
+        dalloc(&d_view_frame, (size_t)g.N_p, &acc) || dalloc(&d_mask, nxy, &acc) ||
+        dalloc(&d_mag, (size_t)g.N_time * nxy, &acc) || dalloc(&d_stats, 1, &acc) ||
+        dalloc(&d_cost_partials, (size_t)cost_partials_needed(g), &acc) || dalloc(&d_cost_out, 2, &acc) ||
+        dalloc(&d_flag, 1, &acc))
+        return -1;
+
+    // views not assigned to any frame keep no A records; frame map for the builder
+    std::vector<int32_t> view_frame(g.N_p, 0);
+    for (int f = 0; f < g.N_time; f++)
+        for (int i = hs.view_first[f]; i < hs.view_first[f + 1]; i++) view_frame[i] = f;
+    n_assigned = hs.view_first[g.N_time];
+
+    CK(cudaMemcpyAsync(d_Hr, hs.H_r.data(), hs.H_r.size() * sizeof(float), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(d_cos, hs.cosv.data(), g.N_p * sizeof(double), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(d_sin, hs.sinv.data(), g.N_p * sizeof(double), cudaMemcpyHostToDevice, st));
+    CK(cudaMemsetAsync(d_views, 0, g.N_p * sizeof(int32_t), st));
+    if (n_assigned)
+        CK(cudaMemcpyAsync(d_views, hs.views.data(), n_assigned * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(d_view_first, hs.view_first.data(), (g.N_time + 1) * sizeof(int32_t), cudaMemcpyHostToDevice,
+                       st));
+    CK(cudaMemcpyAsync(d_view_frame, view_frame.data(), g.N_p * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(d_mask, hs.mask.data(), nxy, cudaMemcpyHostToDevice, st));
+    CK(cudaMemsetAsync(d_flag, 0, sizeof(int), st));
+    CK(cudaMemsetAsync(d_table, 0, table_words * sizeof(uint32_t), st));
+
+    // measurements: [view][row][col] -> [view][col][row]
+    CK(cudaMemcpyAsync(d_tmp, pb->projections, n_sino * sizeof(float), cudaMemcpyHostToDevice, st));
+    launch_transpose_sino(d_tmp, d_y, g.N_p, g.N_t, g.N_r, st);
+    CK(cudaStreamSynchronize(st));
+    CK(cudaMemcpyAsync(d_tmp, pb->weights, n_sino * sizeof(float), cudaMemcpyHostToDevice, st));
+    launch_transpose_sino(d_tmp, d_w, g.N_p, g.N_t, g.N_r, st);
+
+    // A table over the assigned views (records of view position i in views[])
+    Geom gb = g;
+    gb.N_p = n_assigned;
+    if (n_assigned) launch_build_amatrix(gb, d_Hr, d_cos, d_sin, d_views, d_view_first, d_view_frame, d_table, d_flag, st);
+    CK(cudaGetLastError());
+    int flag = 0;
+    CK(cudaMemcpyAsync(&flag, d_flag, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (flag) return fail("A-matrix build: a voxel column hit %s detector channels.",
+                          (flag & 2) ? "more than the record holds" : "non-contiguous");
+
+    // nonzero count (host side, from geometry-free table statistics would need a
+    // copy; count on the device lazily in info_get)
+    CK(cudaMemsetAsync(d_x, 0, n_vox * sizeof(float), st));
+    CK(cudaMemsetAsync(d_mag, 0, (size_t)g.N_time * nxy * sizeof(float), st));
+    masked_columns = 0;
+    for (uint8_t m : hs.mask) masked_columns += m;
+    masked_columns *= g.N_time;
+    choose_schedule();
+    return refresh_error();
+}
+
+void Session::choose_schedule()
+{
+    const Geom &g = hs.g;
+    sv = opt.sv_size;
+    if (sv <= 0) {
+        // largest super-voxel that still gives every SM several CTAs per phase
+        sv = 4;
+        for (int cand : {16, 8}) {
+            const long long per_phase = (long long)g.N_time * ((g.N_x + cand - 1) / cand) *
+                                        ((g.N_y + cand - 1) / cand) / 4;
+            if (per_phase >= 148LL * 8) {
+                sv = cand;
+                break;
+            }
+        }
+    }
+    sv = std::max(1, std::min(sv, 16));
+    warps = opt.cta_warps;
+    if (warps <= 0) {
+        int ntp = 4;
+        while (ntp < g.N_t) ntp <<= 1;
+        const int groups = 32 / ntp;
+        warps = std::max(2, std::min(8, g.max_views / (16 * groups)));
+    }
+    warps = std::max(1, std::min(warps, 8));
+}
+
+int Session::refresh_error()
+{
+    const Geom &g = hs.g;
+    Geom gb = g;
+    gb.N_p = n_assigned;
+    // views outside every frame keep e = y (they never enter the problem)
+    CK(cudaMemcpyAsync(d_err, d_y, n_sino * sizeof(float), cudaMemcpyDeviceToDevice, st));
+    if (n_assigned)
+        launch_forward_project(gb, d_table, d_view_first, d_views, nullptr, d_view_frame, d_x, d_y, d_err, st);
+    CK(cudaGetLastError());
+    return 0;
+}
+
+int Session::set_object(const float *obj)
+{
+    const Geom &g = hs.g;
+    CK(cudaMemcpyAsync(d_tmp, obj, n_vox * sizeof(float), cudaMemcpyHostToDevice, st));
+    launch_vol_to_zfast(d_tmp, d_x, g.N_time, g.N_z, g.N_y, g.N_x, st);
+    CK(cudaGetLastError());
+    return refresh_error();
+}
+
+int Session::get_object(float *obj)
+{
+    const Geom &g = hs.g;
+    launch_zfast_to_vol(d_x, d_tmp, g.N_time, g.N_z, g.N_y, g.N_x, st);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(obj, d_tmp, n_vox * sizeof(float), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return 0;
+}
+
+int Session::cost(double *total, double *data, double *prior)
+{
+    const Geom &g = hs.g;
+    launch_cost(g, d_err, d_w, d_x, d_cost_partials, cost_partials_needed(g), d_cost_out, st);
+    CK(cudaGetLastError());
+    double h[2];
+    CK(cudaMemcpyAsync(h, d_cost_out, sizeof(h), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (data) *data = h[0];
+    if (prior) *prior = h[1];
+    if (total) *total = h[0] + h[1];
+    return 0;
+}
+
+int Session::icd_iteration(int iter, mbirgpu_iter_stats *out)
+{
+    const Geom &g = hs.g;
+    CK(cudaMemsetAsync(d_stats, 0, sizeof(IcdStats), st));
+    IcdLaunch L{};
+    L.sv = sv;
+    L.n_sv_x = (g.N_x + sv - 1) / sv;
+    L.n_sv_y = (g.N_y + sv - 1) / sv;
+    L.warps = warps;
+    L.iter = iter;
+    L.zero_skipping = opt.zero_skipping;
+    L.seed = opt.seed;
+    Geom gb = g;
+    gb.N_p = n_assigned;
+    if (timing && ev_pairs.size() < 4) {
+        while (ev_pairs.size() < 4) {
+            cudaEvent_t a, b;
+            CK(cudaEventCreate(&a));
+            CK(cudaEventCreate(&b));
+            ev_pairs.push_back({a, b});
+        }
+    }
+    for (int ph = 0; ph < 4; ph++) {
+        L.phase = ph;
+        if (timing) CK(cudaEventRecord(ev_pairs[ph].first, st));
+        launch_icd_phase(gb, L, d_table, d_view_first, d_views, d_mask, d_x, d_err, d_w, d_mag, d_stats, st);
+        if (timing) CK(cudaEventRecord(ev_pairs[ph].second, st));
+    }
+    CK(cudaGetLastError());
+    if (opt.refresh_every > 0 && iter % opt.refresh_every == 0)
+        if (refresh_error()) return -1;
+    IcdStats hst;
+    CK(cudaMemcpyAsync(&hst, d_stats, sizeof(hst), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (out) {
+        std::memset(out, 0, sizeof(*out));
+        out->voxel_updates = (int64_t)hst.updates;
+        out->zero_skipped = (int64_t)hst.skipped;
+        out->sum_abs_update = hst.sum_abs_dx;
+        out->sum_abs_value = hst.sum_abs_x;
+        out->kernel_launches = 4;
+        if (timing) {
+            double ms = 0;
+            for (int ph = 0; ph < 4; ph++) {
+                float m = 0;
+                CK(cudaEventElapsedTime(&m, ev_pairs[ph].first, ev_pairs[ph].second));
+                ms += m;
+            }
+            out->kernel_ms = ms;
+        }
+    }
+    return 0;
+}
+
+int Session::run(int max_iter, double *costs, int *iters, mbirgpu_iter_stats *total)
+{
+    double c_prev = 0, c = 0;
+    if (opt.compute_cost) {
+        if (cost(&c, nullptr, nullptr)) return -1;
+        if (costs) costs[0] = c;
+        c_prev = c;
+    }
+    if (total) std::memset(total, 0, sizeof(*total));
+    int it = 1;
+    for (; it <= max_iter; it++) {
+        mbirgpu_iter_stats s;
+        if (icd_iteration(it, &s)) return -1;
+        if (total) {
+            total->voxel_updates += s.voxel_updates;
+            total->zero_skipped += s.zero_skipped;
+            total->sum_abs_update += s.sum_abs_update;
+            total->sum_abs_value += s.sum_abs_value;
+            total->kernel_ms += s.kernel_ms;
+            total->kernel_launches += s.kernel_launches;
+        }
+        bool stop = false;
+        // the reference's test, XT_ICD_update.c:1083-1090 and :1174
+        const double pct = s.sum_abs_value > 0 ? 100.0 * s.sum_abs_update / s.sum_abs_value : 0.0;
+        if (it > 1 && pct < convg_thresh) stop = true;
+        if (opt.compute_cost) {
+            if (cost(&c, nullptr, nullptr)) return -1;
+            if (costs) costs[it] = c;
+            if (opt.cost_rel_tol > 0 && it > 1 && std::fabs(c_prev - c) < opt.cost_rel_tol * std::fabs(c)) stop = true;
+            c_prev = c;
+        }
+        if (stop) break;
+    }
+    if (iters) *iters = std::min(it, max_iter);
+    return 0;
+}
+
+int Session::amatrix(int32_t *first, int32_t *count, float *values)
+{
+    const Geom &g = hs.g;
+    const size_t nxy = (size_t)g.N_x * g.N_y;
+    std::vector<uint32_t> tab((size_t)n_assigned * nxy * g.rec_words);
+    if (!tab.empty())
+        CK(cudaMemcpyAsync(tab.data(), d_table, tab.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    std::fill(first, first + (size_t)g.N_p * nxy, 0);
+    std::fill(count, count + (size_t)g.N_p * nxy, 0);
+    std::fill(values, values + (size_t)g.N_p * nxy * g.kmax, 0.0f);
+    for (int f = 0; f < g.N_time; f++) {
+        const int fv0 = hs.view_first[f], nv = hs.view_first[f + 1] - fv0;
+        for (size_t c = 0; c < nxy; c++)
+            for (int v = 0; v < nv; v++) {
+                const uint32_t *rec = tab.data() + (((size_t)fv0 * nxy) + c * nv + v) * g.rec_words;
+                const int view = hs.views[fv0 + v];
+                const size_t o = (size_t)view * nxy + c;
+                first[o] = rec[0] & 0xFFFF;
+                count[o] = rec[0] >> 16;
+                for (int q = 0; q < g.kmax; q++) std::memcpy(&values[o * g.kmax + q], &rec[1 + q], 4);
+            }
+    }
+    return 0;
+}
+
+int Session::forward_project(const float *obj, float *sino)
+{
+    const Geom &g = hs.g;
+    float *d_obj = nullptr, *d_out = nullptr;
+    size_t acc = 0;
+    if (dalloc(&d_obj, n_vox, &acc) || dalloc(&d_out, n_sino, &acc)) {
+        if (d_obj) cudaFree(d_obj);
+        return -1;
+    }
+    Geom gb = g;
+    gb.N_p = n_assigned;
+    cudaError_t e = cudaMemcpyAsync(d_tmp, obj, n_vox * sizeof(float), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) {
+        launch_vol_to_zfast(d_tmp, d_obj, g.N_time, g.N_z, g.N_y, g.N_x, st);
+        e = cudaMemsetAsync(d_out, 0, n_sino * sizeof(float), st);
+    }
+    if (e == cudaSuccess && n_assigned)
+        launch_forward_project(gb, d_table, d_view_first, d_views, nullptr, d_view_frame, d_obj, nullptr, d_out, st);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(sino, d_out, n_sino * sizeof(float), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(d_obj);
+    cudaFree(d_out);
+    if (e != cudaSuccess) return fail("forward projection failed: %s", cudaGetErrorString(e));
+    return 0;
+}
+
+int Session::back_project(const float *sino, float *obj)
+{
+    const Geom &g = hs.g;
+    float *d_s = nullptr, *d_o = nullptr;
+    size_t acc = 0;
+    if (dalloc(&d_s, n_sino, &acc) || dalloc(&d_o, n_vox, &acc)) {
+        if (d_s) cudaFree(d_s);
+        return -1;
+    }
+    cudaError_t e = cudaMemcpyAsync(d_s, sino, n_sino * sizeof(float), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) launch_back_project(g, d_table, d_view_first, d_views, d_s, d_o, st);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e == cudaSuccess) {
+        launch_zfast_to_vol(d_o, d_tmp, g.N_time, g.N_z, g.N_y, g.N_x, st);
+        e = cudaMemcpyAsync(obj, d_tmp, n_vox * sizeof(float), cudaMemcpyDeviceToHost, st);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(d_s);
+    cudaFree(d_o);
+    if (e != cudaSuccess) return fail("back projection failed: %s", cudaGetErrorString(e));
+    return 0;
+}
+
+}  // namespace mbirgpu
+
+using mbirgpu::fail;
+using mbirgpu::Session;
+
+extern "C" {
+
+void mbirgpu_default_options(mbirgpu_options *o)
+{
+    std::memset(o, 0, sizeof(*o));
+    o->mrf_p = 1.2;
+    o->mrf_q = 2.0;
+    o->alpha = 1.5;
+    o->max_iterations = 1000;
+    o->num_stages = 0;
+    o->cost_rel_tol = 0.0;
+    o->zero_skipping = 1;
+    o->write_files = 1;
+    o->compute_cost = 1;
+    o->refresh_every = 4;
+    o->sv_size = 0;
+    o->cta_warps = 0;
+    o->seed = 761521;  // the reference's srandom2 seed, XT_Engine.c:99
+}
+
+int mbirgpu_set_options(const mbirgpu_options *o)
+{
+    if (!o) return fail("options pointer is NULL");
+    if (!(o->mrf_p >= 1.0 && o->mrf_p <= o->mrf_q)) return fail("need 1 <= mrf_p <= mrf_q");
+    if (o->max_iterations < 1) return fail("max_iterations must be positive");
+    if (o->sv_size < 0 || o->sv_size > 16) return fail("sv_size must be 0 (auto) or 1..16");
+    if (o->cta_warps < 0 || o->cta_warps > 8) return fail("cta_warps must be 0 (auto) or 1..8");
+    mbirgpu_options cur = mbirgpu::current_options();
+    (void)cur;
+    std::lock_guard<std::mutex> lk(mbirgpu::g_opt_mu);
+    mbirgpu::g_opt = *o;
+    mbirgpu::g_opt_init = true;
+    return 0;
+}
+
+int mbirgpu_get_options(mbirgpu_options *o)
+{
+    if (!o) return fail("options pointer is NULL");
+    *o = mbirgpu::current_options();
+    return 0;
+}
+
+const char *mbirgpu_last_error(void) { return mbirgpu::g_last_error.c_str(); }
+
+int mbirgpu_session_create(mbirgpu_session **out, const mbirgpu_problem *pb, const mbirgpu_options *opt,
+                           int32_t mult_xy, int32_t mult_z, void *stream)
+{
+    if (!out || !pb) return fail("NULL argument");
+    *out = nullptr;
+    if (!pb->projections || !pb->weights || !pb->proj_angles || !pb->proj_times || !pb->recon_times)
+        return fail("NULL input array");
+    Session *s = new (std::nothrow) Session();
+    if (!s) return fail("out of host memory");
+    if (s->init(pb, opt, mult_xy, mult_z, stream)) {
+        std::string keep = mbirgpu::g_last_error;
+        delete s;
+        mbirgpu::g_last_error = keep;
+        return -1;
+    }
+    *out = reinterpret_cast<mbirgpu_session *>(s);
+    return 0;
+}
+
+int mbirgpu_session_destroy(mbirgpu_session *s)
+{
+    delete reinterpret_cast<Session *>(s);
+    return 0;
+}
+
+int mbirgpu_session_info_get(const mbirgpu_session *sp, mbirgpu_session_info *info)
+{
+    if (!sp || !info) return fail("NULL argument");
+    const Session *s = reinterpret_cast<const Session *>(sp);
+    const mbirgpu::Geom &g = s->hs.g;
+    std::memset(info, 0, sizeof(*info));
+    info->N_r = g.N_r;
+    info->N_t = g.N_t;
+    info->N_p = g.N_p;
+    info->N_time = g.N_time;
+    info->N_x = g.N_x;
+    info->N_y = g.N_y;
+    info->N_z = g.N_z;
+    info->mult_xy = g.mult_xy;
+    info->mult_z = g.mult_z;
+    info->max_views = g.max_views;
+    info->kmax = g.kmax;
+    info->sv_size = s->sv;
+    info->cta_warps = s->warps;
+    info->masked_columns = s->masked_columns;
+    info->delta_t = g.delta_t;
+    info->device_bytes = s->device_bytes;
+    return 0;
+}
+
+#define SESSION(sp)                                       \
+    if (!(sp)) return fail("session pointer is NULL");    \
+    Session *s = reinterpret_cast<Session *>(sp)
+
+int mbirgpu_session_set_stream(mbirgpu_session *sp, void *stream)
+{
+    SESSION(sp);
+    s->st = (cudaStream_t)stream;
+    return 0;
+}
+
+int mbirgpu_session_set_timing(mbirgpu_session *sp, int32_t enable)
+{
+    SESSION(sp);
+    s->timing = enable != 0;
+    return 0;
+}
+
+int mbirgpu_session_set_object(mbirgpu_session *sp, const float *object)
+{
+    SESSION(sp);
+    if (!object) return fail("NULL object");
+    return s->set_object(object);
+}
+
+int mbirgpu_session_get_object(mbirgpu_session *sp, float *object)
+{
+    SESSION(sp);
+    if (!object) return fail("NULL object");
+    return s->get_object(object);
+}
+
+int mbirgpu_session_object_device(mbirgpu_session *sp, float **d_object)
+{
+    SESSION(sp);
+    if (!d_object) return fail("NULL argument");
+    *d_object = s->d_x;
+    return 0;
+}
+
+int mbirgpu_session_refresh_error(mbirgpu_session *sp)
+{
+    SESSION(sp);
+    return s->refresh_error();
+}
+
+int mbirgpu_session_get_error(mbirgpu_session *sp, float *err)
+{
+    SESSION(sp);
+    if (!err) return fail("NULL argument");
+    cudaError_t e = cudaMemcpyAsync(err, s->d_err, s->n_sino * sizeof(float), cudaMemcpyDeviceToHost, s->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
+    if (e != cudaSuccess) return fail("copy of the error sinogram failed: %s", cudaGetErrorString(e));
+    return 0;
+}
+
+int mbirgpu_session_cost(mbirgpu_session *sp, double *total, double *data_term, double *prior_term)
+{
+    SESSION(sp);
+    return s->cost(total, data_term, prior_term);
+}
+
+int mbirgpu_session_icd_iteration(mbirgpu_session *sp, int32_t iter, mbirgpu_iter_stats *stats)
+{
+    SESSION(sp);
+    if (iter < 1) return fail("iterations are numbered from 1");
+    return s->icd_iteration(iter, stats);
+}
+
+int mbirgpu_session_forward_project(mbirgpu_session *sp, const float *object, float *sino)
+{
+    SESSION(sp);
+    if (!object || !sino) return fail("NULL argument");
+    return s->forward_project(object, sino);
+}
+
+int mbirgpu_session_back_project(mbirgpu_session *sp, const float *sino, float *object)
+{
+    SESSION(sp);
+    if (!object || !sino) return fail("NULL argument");
+    return s->back_project(sino, object);
+}
+
+int mbirgpu_session_get_amatrix(mbirgpu_session *sp, int32_t *first, int32_t *count, float *values)
+{
+    SESSION(sp);
+    if (!first || !count || !values) return fail("NULL argument");
+    return s->amatrix(first, count, values);
+}
+
+int mbirgpu_session_get_detector_response(mbirgpu_session *sp, float *H_r)
+{
+    SESSION(sp);
+    if (!H_r) return fail("NULL argument");
+    std::memcpy(H_r, s->hs.H_r.data(), s->hs.H_r.size() * sizeof(float));
+    return 0;
+}
+
+int mbirgpu_session_run(mbirgpu_session *sp, int32_t max_iter, double *costs, int32_t *iters,
+                        mbirgpu_iter_stats *total)
+{
+    SESSION(sp);
+    if (max_iter < 1) return fail("max_iter must be positive");
+    int it = 0;
+    int rc = s->run(max_iter, costs, &it, total);
+    if (iters) *iters = it;
+    return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,50 @@
+// Session object behind the opaque mbirgpu_session handle.
+#pragma once
+#include <utility>
+#include <vector>
+#include "../../include/mbirgpu.h"
+#include "mbir_internal.h"
+
+namespace mbirgpu {
+
+int fail(const char *fmt, ...);
+mbirgpu_options current_options();
+
+struct Session {
+    HostSetup hs;
+    mbirgpu_options opt{};
+    cudaStream_t st = nullptr;
+    float convg_thresh = 0;
+    size_t n_sino = 0, n_vox = 0, device_bytes = 0;
+    int n_assigned = 0;  // views that belong to some frame
+    int64_t masked_columns = 0;
+    int sv = 8, warps = 4;
+    bool timing = false;
+
+    float *d_y = nullptr, *d_w = nullptr, *d_err = nullptr, *d_x = nullptr, *d_tmp = nullptr;
+    uint32_t *d_table = nullptr;
+    float *d_Hr = nullptr;
+    double *d_cos = nullptr, *d_sin = nullptr;
+    int32_t *d_views = nullptr, *d_view_first = nullptr, *d_view_frame = nullptr;
+    uint8_t *d_mask = nullptr;
+    float *d_mag = nullptr;
+    IcdStats *d_stats = nullptr;
+    double *d_cost_partials = nullptr, *d_cost_out = nullptr;
+    int *d_flag = nullptr;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pairs;
+
+    ~Session();
+    int init(const mbirgpu_problem *pb, const mbirgpu_options *o, int mult_xy, int mult_z, void *stream);
+    void choose_schedule();
+    int refresh_error();
+    int set_object(const float *obj);
+    int get_object(float *obj);
+    int cost(double *total, double *data, double *prior);
+    int icd_iteration(int iter, mbirgpu_iter_stats *out);
+    int run(int max_iter, double *costs, int *iters, mbirgpu_iter_stats *total);
+    int amatrix(int32_t *first, int32_t *count, float *values);
+    int forward_project(const float *obj, float *sino);
+    int back_project(const float *sino, float *obj);
+};
+
+}  // namespace mbirgpu

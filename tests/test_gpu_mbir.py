@@ -1,0 +1,166 @@
+"""Parity of the sm_100a path (through the C ABI) with the oracle and the reference.
+
+Tolerances (stated per result):
+* detector response, A-matrix table: bit-exact (the table stores the
+  reference's double A value rounded once to float);
+* forward projection e = y - A x: max |diff| <= 1e-5 x max |e| (FP64 accumulation
+  on the GPU vs the reference's float accumulation);
+* adjoint: <A x, s> = <x, A^T s> to 1e-6 relative;
+* MAP cost kernel on a given state: 1e-10 relative (FP64, summation order);
+* ICD: converged cost within 1e-4 relative of the reference's and image RMSE
+  within 0.5 % of the dynamic range (voxel update order differs).
+"""
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+import phasecon_b200 as pc
+from problems import make_problem, to_gpu_problem
+from test_oracle import GOLD, golden_problem
+
+pytestmark = pytest.mark.gpu
+
+
+def gpu_session(pb, m=1, **opt):
+    o = pc.get_options()
+    o.mrf_p = pb.mrf_p
+    for k, v in opt.items():
+        setattr(o, k, v)
+    return pc.Session(to_gpu_problem(pb), mult_xy=m, mult_z=m, options=o)
+
+
+def test_detector_response_bit_exact():
+    pb = golden_problem("quad")
+    s = gpu_session(pb)
+    assert np.array_equal(s.detector_response(), GOLD["quad_H_r"])
+
+
+@pytest.mark.parametrize("m", [1, 2])
+def test_amatrix_table_bit_exact(m):
+    pb = golden_problem("amat")
+    s = gpu_session(pb, m)
+    first, count, vals = s.amatrix()
+    cnt, idx, val = GOLD[f"amat{m}_count"], GOLD[f"amat{m}_index"], GOLD[f"amat{m}_value"]
+    assert np.array_equal(count, cnt.astype(np.int32))
+    nz = cnt > 0
+    assert np.array_equal(first[nz], idx[..., 0][nz])
+    kmax = vals.shape[-1]
+    for q in range(min(kmax, val.shape[-1])):
+        has = cnt > q
+        assert np.array_equal(vals[..., q][has], val[..., q][has].astype(np.float32))
+
+
+def test_forward_projection_matches_reference():
+    pb = golden_problem("quad")
+    s = gpu_session(pb)
+    s.set_object(GOLD["quad_true_object"])
+    e = s.get_error()
+    ref = GOLD["quad_err_at_true"]
+    assert np.abs(e - ref).max() <= 1e-5 * np.abs(ref).max()
+
+
+def test_forward_projection_matches_oracle_multiframe_coarse():
+    pb, obj = make_problem(ncol=64, nrow=8, nview=48, nframe=3, seed=7, moving=True)
+    for m in (1, 2):
+        orc = O.Oracle(pb, m, m)
+        x = np.random.default_rng(m).uniform(0, 0.02, orc.shape).astype(np.float32)
+        s = gpu_session(pb, m)
+        ax = s.forward_project(x)
+        ref = orc.forward(x)
+        assert np.abs(ax - ref).max() <= 1e-6 * np.abs(ref).max()
+
+
+def test_back_projection_is_adjoint():
+    pb, _ = make_problem(ncol=64, nrow=16, nview=45, nframe=2, seed=2)
+    s = gpu_session(pb)
+    rng = np.random.default_rng(0)
+    x = rng.uniform(0, 1, s.shape).astype(np.float32)
+    y = rng.normal(0, 1, s.sino_shape).astype(np.float32)
+    lhs = np.dot(s.forward_project(x).astype(np.float64).ravel(), y.astype(np.float64).ravel())
+    rhs = np.dot(x.astype(np.float64).ravel(), s.back_project(y).astype(np.float64).ravel())
+    assert lhs == pytest.approx(rhs, rel=1e-6)
+
+
+@pytest.mark.parametrize("prefix", ["quad", "huber"])
+def test_cost_kernel_matches_oracle(prefix):
+    pb = golden_problem(prefix)
+    obj = GOLD["quad_true_object"] if prefix == "quad" else GOLD["huber_half_object"]
+    s = gpu_session(pb)
+    s.set_object(obj)
+    e = s.get_error()
+    c_gpu, d_gpu, p_gpu = s.cost()
+    c, d, p = O.Oracle(pb).cost(e, obj)
+    assert d_gpu == pytest.approx(d, rel=1e-10)
+    assert p_gpu == pytest.approx(p, rel=1e-10)
+
+
+def _run_icd(s, iters):
+    costs = [s.cost()[0]]
+    for it in range(1, iters + 1):
+        s.icd_iteration(it)
+        costs.append(s.cost()[0])
+    return np.array(costs)
+
+
+def test_icd_converges_to_reference_cost_4d():
+    pb = golden_problem("quad")
+    s = gpu_session(pb, sv_size=4)
+    costs = _run_icd(s, 60)
+    ref = GOLD["quad_icd20_cost"]
+    assert costs[0] == pytest.approx(ref[0], rel=1e-6)
+    # monotone up to FP32 atomic noise
+    assert np.all(np.diff(costs) <= 1e-6 * costs[:-1])
+    final_ref = ref[-1]
+    assert abs(costs[-1] - final_ref) / final_ref < 1e-4, (costs[-5:], final_ref)
+    x = s.get_object()
+    xr = GOLD["quad_icd20_object"]
+    rmse = np.sqrt(np.mean((x - xr) ** 2))
+    assert rmse <= 0.005 * (xr.max() - xr.min())
+
+
+def test_icd_huber_branch_converges():
+    pb = golden_problem("huber")
+    s = gpu_session(pb, sv_size=4)
+    costs = _run_icd(s, 40)
+    ref = GOLD["huber_icd10_cost"]
+    assert costs[0] == pytest.approx(ref[0], rel=1e-6)
+    assert costs[-1] <= ref[-1] * (1 + 1e-4)
+
+
+def test_error_sinogram_drift_is_bounded():
+    pb = golden_problem("quad")
+    s = gpu_session(pb, refresh_every=0)
+    _run_icd(s, 10)
+    e_run = s.get_error()
+    s.refresh_error()
+    e_exact = s.get_error()
+    assert np.abs(e_run - e_exact).max() <= 1e-4 * np.abs(e_exact).max()
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference build not present")
+def test_reconstruct_dropin_matches_reference(tmp_path):
+    pb, _ = make_problem(ncol=128, nrow=8, nview=90, nframe=1, seed=4)
+    args = (pb.projections, pb.weights, pb.proj_angles, pb.proj_times, pb.recon_times, pb.proj_rows,
+            pb.proj_cols, pb.proj_num, pb.recon_num, pb.vox_wid, pb.rot_center, pb.sig_s, pb.sig_t, pb.c_s,
+            pb.c_t)
+    cwd = os.getcwd()
+    os.chdir(tmp_path)
+    saved = pc.get_options()
+    try:
+        pc.set_options(mrf_p=pb.mrf_p, max_iterations=60, cost_rel_tol=0.0)
+        out = pc.reconstruct(*args, convg_thresh=0.05, remove_rings=0, quad_convex=1)
+        cost = np.fromfile("cost.bin", np.float64)
+        assert os.path.exists("object_time_0.bin") and os.path.exists("status.bin")
+    finally:
+        os.chdir(cwd)
+        import ctypes
+        pc.lib().mbirgpu_set_options(ctypes.byref(saved))
+    assert out.shape == (1, pb.proj_rows + 2, pb.proj_cols, pb.proj_cols)
+    assert np.all(out[:, 0] == 0) and np.all(out[:, -1] == 0)
+    pb.convg_thresh = 0.05
+    ref_obj, ref_cost, _ = O.ref_reconstruct(pb, str(tmp_path / "ref"), max_iter=60)
+    x, xr = out[:, 1:-1], ref_obj[:, 1:-1]
+    assert np.sqrt(np.mean((x - xr) ** 2)) <= 0.005 * (xr.max() - xr.min())
+    assert abs(cost[-1] - ref_cost[-1]) / ref_cost[-1] < 1e-3
