@@ -1,0 +1,398 @@
+"""Benchmark: plain GPU super-voxel ICD on the 4-D time-interlaced MBIR workload.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+A step is one ICD iteration over the whole 4-D problem (every voxel inside the
+reconstruction circle of all 8 frames updated once). The workload is seeded
+synthetic data with the shapes of the 4-D configuration: a Cahn-Hilliard
+two-phase microstructure on 256x256x32 voxels x 8 frames, 1,024 interlaced
+parallel-beam views (K=8 sub-frames, 4 rotations), a 256x32 detector,
+Poisson I0 = 2e4, qGGMRF p = 1.2 (see phasecon_b200/workloads.py).
+
+One JSON line on rank 0 carries:
+  value       voxel-updates/s over K timed iterations, inputs resident in HBM
+              (device time, CUDA events on the session's stream, max over ranks);
+  e2e         the same metric through the public API with host buffers: session
+              creation from host arrays (H2D of y, w, geometry; A-matrix build;
+              initial projection), K iterations, and the D2H read of the object;
+  time_to_converged_s  plain GPU ICD from zero to relative cost change < 1e-4;
+  roofline    the ICD sweep kernel's algorithmic bytes (12 nnz_v + 8 per voxel
+              update) over its measured launch time, against MEASURED_PEAKS.json;
+  cpu_baseline the reference C (oracle/_ref, built from source) on a bounded
+              sample of the workload on this host's cores.
+With --gpus N > 1 (torchrun) every rank runs an independent replica (the path
+does not shard on one problem); value is the sum over ranks / max time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "time-to-converged cost (rel 1e-4), voxel-updates/s; warm-start vs plain GPU ICD"
+UNIT = "voxel-updates/s"
+WORKLOAD = "4d_cahn_hilliard_256x256x32_8frames_1024views"
+SAMPLE_ROWS = 4  # detector rows of the CPU-baseline sample (4 of the 32 voxel slices)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-converge", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--max-converge-iters", type=int, default=400)
+    return ap.parse_args()
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return world, rank, local, pg
+
+
+def max_over_ranks(pg, v: float) -> float:
+    if pg is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(pg, v: float) -> float:
+    if pg is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.SUM)
+    return float(t.item())
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.path = tempfile.mktemp(suffix=".csv")
+
+    def __enter__(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if self.proc is None or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax = float(p[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """DRAM bytes per ICD sweep launch from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "icd_phase_kernel_4d.txt")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.startswith("dram_bytes_per_launch_full_size:"):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+# --------------------------------------------------------------------------- CPU sample (reference C)
+
+
+def cpu_sample_problem(seed: int = 0):
+    """A bounded sample of the 4-D workload for the CPU reference: the same
+    Cahn-Hilliard frames, views and detector columns, restricted to the first
+    SAMPLE_ROWS detector rows / voxel slices. Measurements are formed with the
+    oracle's restated reference projector, so no GPU kernel of this project is
+    involved."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    from phasecon_b200 import phantoms as P
+    angles, times = P.interlaced_views(8, 256, 1024)
+    rt = np.linspace(0.0, 1024.0, 9).astype(np.float32)
+    vol = P.cahn_hilliard_frames(256, 32, 8, steps=5000, seed=seed)[:, :SAMPLE_ROWS]
+    pb = O.Problem(np.zeros((1024, SAMPLE_ROWS, 256), np.float32), np.ones((1024, SAMPLE_ROWS, 256), np.float32),
+                   angles, times, rt, SAMPLE_ROWS, 256, 1024, 8, rot_center=128.0, sig_s=0.01, sig_t=0.01, c_s=1.0,
+                   c_t=1.0, mrf_p=1.2, convg_thresh=0.0)
+    orc = O.Oracle(pb)
+    ax = orc.forward(np.ascontiguousarray(vol))
+    y, w = P.poisson_measurements(ax, 2e4, seed)
+    pb.projections = np.ascontiguousarray(y.transpose(0, 2, 1))
+    pb.weights = np.ascontiguousarray(w.transpose(0, 2, 1))
+    return pb
+
+
+def reference_rate(pb, warmup: int, steps: int):
+    """Reference C (single stage, all host threads): voxel-updates/s over
+    `steps` ICD iterations after `warmup`, from two runs (warmup and
+    warmup+steps iterations) so set-up time cancels."""
+    import oracle as O
+    threads = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    _, c1, u1 = O.ref_reconstruct(pb, tempfile.mkdtemp(), max_iter=max(warmup, 1), num_stages=1, threads=threads)
+    t1 = time.perf_counter()
+    _, c2, u2 = O.ref_reconstruct(pb, tempfile.mkdtemp(), max_iter=max(warmup, 1) + steps, num_stages=1,
+                                  threads=threads)
+    t2 = time.perf_counter()
+    dt = (t2 - t1) - (t1 - t0)
+    upd = u2 - u1
+    return upd / dt if dt > 0 else float("nan"), dt, upd, threads
+
+
+def run_reference_arm(args, rank):
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    if not oracle.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref_mbir4d.so was not built"}))
+        return
+    pb = cpu_sample_problem()
+    rate, dt, upd, threads = reference_rate(pb, args.warmup, args.steps)
+    sample = (f"reference C MBIR_4D (built from source), single stage, {SAMPLE_ROWS} of 32 detector rows of the "
+              f"4-D workload, {args.steps} ICD iterations after {args.warmup} (two runs, set-up cancelled)")
+    line = {"metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * dt / max(args.steps, 1), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64/f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "sample_rows": SAMPLE_ROWS}, "impl": "reference",
+            "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference", "sample": sample},
+            "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "voxel_updates": upd}
+    print(json.dumps(line))
+
+
+# --------------------------------------------------------------------------- our arm
+
+
+def run_ours(args, world, rank, local, pg):
+    import torch
+
+    import phasecon_b200 as pc
+    from phasecon_b200 import workloads as W
+
+    torch.cuda.set_device(local)
+    stream = torch.cuda.current_stream()
+    pb, _, p = W.config_4d(seed=0)
+    opt = pc.get_options()
+    opt.mrf_p = p
+    s = pc.Session(pb, options=opt, stream=stream.cuda_stream)
+    s.set_timing(True)
+    info = s.info
+    refresh = opt.refresh_every
+
+    # warm-up, then K timed iterations (device events on the session stream)
+    for it in range(1, args.warmup + 1):
+        s.icd_iteration(it)
+    barrier(pg)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    kernel_ms, updates, launches = 0.0, 0, 0
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for it in range(args.warmup + 1, args.warmup + args.steps + 1):
+            st = s.icd_iteration(it)
+            kernel_ms += st.kernel_ms
+            updates += st.voxel_updates
+            launches += st.kernel_launches + (1 if refresh > 0 and it % refresh == 0 else 0)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    barrier(pg)
+    ms = ev0.elapsed_time(ev1)
+    ms_max = max_over_ranks(pg, ms)
+    total_updates = sum_over_ranks(pg, float(updates))
+    value = total_updates / (ms_max / 1e3)
+
+    # roofline of the ICD sweep kernel (4 launches per iteration)
+    n_launch = 4 * args.steps
+    entries = info.nnz * info.N_t  # (e, w) entries one full sweep reads: nnz_v summed over voxel slices
+    upd_per_iter = updates / args.steps
+    full = info.masked_columns * info.N_z
+    bytes_iter = (12.0 * entries + 8.0 * full) * (upd_per_iter / full if full else 1.0)
+    bytes_launch = bytes_iter / 4
+    avg_launch_s = kernel_ms / n_launch / 1e3
+    peak, peak_kind = measured_peaks()
+    achieved = bytes_launch / avg_launch_s / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": profiled_traffic(), "peak_source": peak_kind, "kernel": "icd_phase_kernel",
+                "algorithmic_bytes_per_launch": bytes_launch, "avg_launch_ms": avg_launch_s * 1e3}
+
+    # time to converged cost from zero (plain GPU ICD), FP64 cost every iteration
+    conv = {}
+    if not args.no_converge:
+        s.set_object(np.zeros(s.shape, np.float32))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        costs = [s.cost()[0]]
+        it = 0
+        while it < args.max_converge_iters:
+            it += 1
+            s.icd_iteration(it)
+            costs.append(s.cost()[0])
+            if it > 1 and abs(costs[-2] - costs[-1]) < 1e-4 * abs(costs[-1]):
+                break
+        torch.cuda.synchronize()
+        tconv = time.perf_counter() - t0
+        conv = {"time_to_converged_s": tconv, "iterations_to_converged": it, "converged_cost": costs[-1],
+                "initial_cost": costs[0], "converged": it < args.max_converge_iters}
+        # FP64 cost of the final state against the CPU oracle on the same (e, x)
+        try:
+            sys.path.insert(0, os.path.join(ROOT, "oracle"))
+            import oracle as O
+            s.refresh_error()
+            x = s.get_object()
+            e = s.get_error()
+            gpu_cost = s.cost()[0]
+            orc_pb = O.Problem(pb.projections, pb.weights, pb.proj_angles, pb.proj_times, pb.recon_times,
+                               pb.proj_rows, pb.proj_cols, pb.proj_num, pb.recon_num, rot_center=pb.rot_center,
+                               sig_s=pb.sig_s, sig_t=pb.sig_t, c_s=pb.c_s, c_t=pb.c_t, mrf_p=p)
+            orc_cost = O.Oracle(orc_pb).cost(e, x)[0]
+            conv["cost_rel_err_vs_fp64_oracle"] = abs(gpu_cost - orc_cost) / abs(orc_cost)
+        except Exception as ex:  # the oracle is the checker only; its absence does not stop the bench
+            conv["cost_rel_err_vs_fp64_oracle"] = f"unavailable: {ex}"
+    s.close()
+
+    # end to end through the public API with host buffers
+    h_arrays = pb.arrays()
+    h2d = sum(a.nbytes for a in h_arrays)
+    torch.cuda.synchronize()
+    barrier(pg)
+    t0 = time.perf_counter()
+    s2 = pc.Session(pb, options=opt, stream=stream.cuda_stream)
+    e2e_upd = 0
+    for it in range(1, args.steps + 1):
+        e2e_upd += s2.icd_iteration(it).voxel_updates
+    obj = s2.get_object()
+    torch.cuda.synchronize()
+    t_e2e = max_over_ranks(pg, time.perf_counter() - t0)
+    s2.close()
+    d2h = obj.nbytes
+    e2e = {"value": sum_over_ranks(pg, float(e2e_upd)) / t_e2e, "unit": UNIT,
+           "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
+           "steps_per_call": args.steps,
+           "note": "one session from host arrays (H2D of y, w, angles, times), A-matrix build, K iterations, "
+                   "D2H of the object; bytes per step = bytes per call / K"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            sys.path.insert(0, os.path.join(ROOT, "oracle"))
+            import oracle
+            if oracle.ref_available():
+                spb = cpu_sample_problem()
+                rate, dt, upd, threads = reference_rate(spb, 1, 2)
+                cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference",
+                       "sample": f"reference C MBIR_4D built from source, {SAMPLE_ROWS} of 32 detector rows of the "
+                                 f"same 4-D workload, 2 ICD iterations after 1 ({upd} voxel updates, {dt:.1f} s)"}
+            else:
+                cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
+                       "sample": "oracle/_ref not built on this host"}
+        except Exception as ex:
+            cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"failed: {ex}"}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": WORKLOAD, "voxels": [info.N_time, info.N_z, info.N_y, info.N_x],
+                           "views": info.N_p, "detector": [info.N_t, info.N_r], "sv_size": info.sv_size,
+                           "cta_warps": info.cta_warps, "parallelism": f"replicas{world}",
+                           "l2": "inputs larger than L2: A table %.2f GB, y/w/e %.0f MB, x %.0f MB" % (
+                               info.device_bytes / 1e9, 3 * info.N_p * info.N_r * info.N_t * 4 / 1e6,
+                               info.N_time * info.N_z * info.N_y * info.N_x * 4 / 1e6)},
+                "voxel_updates_per_step": updates / args.steps, "roofline": roofline, "cpu_baseline": cpu,
+                "e2e": e2e, "clocks": clk.summary(), "gpu_launches": launches}
+        line.update(conv)
+        print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    world, rank, local, pg = dist_setup()
+    try:
+        if args.impl == "reference":
+            run_reference_arm(args, rank)
+        else:
+            run_ours(args, world, rank, local, pg)
+    finally:
+        if pg is not None:
+            pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

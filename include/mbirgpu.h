@@ -99,7 +99,8 @@ typedef struct {
     int32_t kmax;            /* most detector channels one voxel column hits per view */
     int32_t sv_size, cta_warps;
     int64_t masked_columns;  /* voxel columns inside the reconstruction circle, all frames */
-    int64_t nnz;             /* A-matrix nonzeros over all frames (x z_overlap per slice) */
+    int64_t nnz;             /* A-matrix nonzeros (view, channel) of the columns inside the circle,
+                                summed over frames; one voxel slice reads nnz*z_overlap entries */
     double delta_t;
     size_t device_bytes;     /* device memory the session holds */
 } mbirgpu_session_info;

@@ -83,4 +83,35 @@ void launch_build_amatrix(const Geom &g, const float *d_Hr, const double *d_cos,
                                                                d_view_frame, d_table, d_err);
 }
 
+// Sum of record counts over voxel columns inside the reconstruction circle:
+// the A-matrix nonzeros one sweep visits per voxel slice (before the
+// z_overlap factor).
+__global__ void count_masked_nnz_kernel(int n_records, int nxy, int rec_words, const int32_t *__restrict__ view_first,
+                                        const int32_t *__restrict__ view_frame, const uint8_t *__restrict__ mask,
+                                        const uint32_t *__restrict__ table, unsigned long long *__restrict__ out)
+{
+    unsigned long long acc = 0;
+    for (long long rec = blockIdx.x * (long long)blockDim.x + threadIdx.x; rec < (long long)n_records * nxy;
+         rec += (long long)gridDim.x * blockDim.x) {
+        const int f = view_frame[rec / nxy];
+        const int fv0 = view_first[f], nv = view_first[f + 1] - fv0;
+        const int c = (int)((rec - (long long)fv0 * nxy) / nv);
+        if (mask[c]) acc += table[rec * rec_words] >> 16;
+    }
+    for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+    if ((threadIdx.x & 31) == 0) atomicAdd(out, acc);
+}
+
+void launch_count_masked_nnz(const Geom &g, int n_assigned, const int32_t *d_view_first, const int32_t *d_view_frame,
+                             const uint8_t *d_mask, const uint32_t *d_table, unsigned long long *d_out,
+                             cudaStream_t st)
+{
+    const long long total = (long long)n_assigned * g.N_x * g.N_y;
+    long long blocks = (total + 255) / 256;
+    if (blocks > 148LL * 32) blocks = 148LL * 32;
+    if (blocks < 1) blocks = 1;
+    count_masked_nnz_kernel<<<(unsigned)blocks, 256, 0, st>>>(n_assigned, g.N_x * g.N_y, g.rec_words, d_view_first,
+                                                              d_view_frame, d_mask, d_table, d_out);
+}
+
 }  // namespace mbirgpu

@@ -65,6 +65,10 @@ void launch_build_amatrix(const Geom &g, const float *d_Hr, const double *d_cos,
                           const int32_t *d_views, const int32_t *d_view_first, const int32_t *d_view_frame,
                           uint32_t *d_table, int *d_err, cudaStream_t st);
 
+void launch_count_masked_nnz(const Geom &g, int n_assigned, const int32_t *d_view_first, const int32_t *d_view_frame,
+                             const uint8_t *d_mask, const uint32_t *d_table, unsigned long long *d_out,
+                             cudaStream_t st);
+
 // e = y - A x (FP64 accumulation); when d_y is null the result is A x itself.
 void launch_forward_project(const Geom &g, const uint32_t *d_table, const int32_t *d_view_first,
                             const int32_t *d_views, const int32_t *d_view_local, const int32_t *d_view_frame,

@@ -155,8 +155,14 @@ int Session::init(const mbirgpu_problem *pb, const mbirgpu_options *o, int mult_
     if (flag) return fail("A-matrix build: a voxel column hit %s detector channels.",
                           (flag & 2) ? "more than the record holds" : "non-contiguous");
 
-    // nonzero count (host side, from geometry-free table statistics would need a
-    // copy; count on the device lazily in info_get)
+    // A nonzeros over the columns a sweep visits (for the roofline's byte count)
+    CK(cudaMemsetAsync(d_stats, 0, sizeof(IcdStats), st));
+    if (n_assigned)
+        launch_count_masked_nnz(g, n_assigned, d_view_first, d_view_frame, d_mask, d_table, &d_stats->updates, st);
+    unsigned long long nnz = 0;
+    CK(cudaMemcpyAsync(&nnz, &d_stats->updates, sizeof(nnz), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    masked_nnz = (int64_t)nnz;
     CK(cudaMemsetAsync(d_x, 0, n_vox * sizeof(float), st));
     CK(cudaMemsetAsync(d_mag, 0, (size_t)g.N_time * nxy * sizeof(float), st));
     masked_columns = 0;
@@ -500,6 +506,7 @@ int mbirgpu_session_info_get(const mbirgpu_session *sp, mbirgpu_session_info *in
     info->sv_size = s->sv;
     info->cta_warps = s->warps;
     info->masked_columns = s->masked_columns;
+    info->nnz = s->masked_nnz;
     info->delta_t = g.delta_t;
     info->device_bytes = s->device_bytes;
     return 0;

@@ -18,6 +18,7 @@ struct Session {
     size_t n_sino = 0, n_vox = 0, device_bytes = 0;
     int n_assigned = 0;  // views that belong to some frame
     int64_t masked_columns = 0;
+    int64_t masked_nnz = 0;  // A nonzeros over masked columns, all frames, per voxel slice
     int sv = 8, warps = 4;
     bool timing = false;
 
