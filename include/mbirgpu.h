@@ -55,9 +55,11 @@ typedef struct {
     int32_t zero_skipping;   /* ZERO_SKIPPING (XT_Constants.h:47), default 1 */
     int32_t write_files;     /* reference side-effect files, default 1 */
     int32_t compute_cost;    /* FP64 MAP cost every iteration (cost.bin), default 1 */
-    int32_t refresh_every;   /* FP64 recomputation of e = y - Ax every n iterations, default 4 */
+    int32_t refresh_every;   /* FP64 recomputation of e = y - Ax every n iterations, default 8 */
     int32_t sv_size;         /* super-voxel edge in voxel columns; 0 = autotuned */
     int32_t cta_warps;       /* warps cooperating on one voxel column; 0 = autotuned */
+    int32_t icd_unroll;      /* views whose A records and sinogram entries one lane keeps in flight
+                                (1, 2 or 4); 0 = autotuned */
     uint64_t seed;           /* voxel-order seed */
 } mbirgpu_options;
 

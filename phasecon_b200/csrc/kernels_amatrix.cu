@@ -9,8 +9,9 @@
 // them), the records of column c are contiguous:
 //   record (f, c, v) at  view_first[f]*NXY + c*nv + v      (v = view in frame)
 // so the ICD kernel reads one column's views with unit stride.
-// Record = rec_words 32-bit words: word 0 = first | count << 16, then kmax
-// float weights, zero padded.
+// Record = rec_words 32-bit words: word 0 = row | count << 24, where row =
+// view * N_r + first channel is the record's first sinogram row (so kernels
+// need no view lookup), then kmax float weights, zero padded.
 #include "mbir_internal.h"
 
 namespace mbirgpu {
@@ -66,7 +67,7 @@ __global__ void build_amatrix_kernel(Geom g, const float *__restrict__ Hr, const
             }
         }
         if (count > g.kmax) count = g.kmax;
-        out[0] = (uint32_t)(first & 0xFFFF) | ((uint32_t)count << 16);
+        out[0] = (uint32_t)(view * g.N_r + first) | ((uint32_t)count << 24);
         for (int q = 0; q < g.rec_words - 1; q++) out[1 + q] = q < count ? __float_as_uint(vals[q]) : 0u;
     }
 }
@@ -96,7 +97,7 @@ __global__ void count_masked_nnz_kernel(int n_records, int nxy, int rec_words, c
         const int f = view_frame[rec / nxy];
         const int fv0 = view_first[f], nv = view_first[f + 1] - fv0;
         const int c = (int)((rec - (long long)fv0 * nxy) / nv);
-        if (mask[c]) acc += table[rec * rec_words] >> 16;
+        if (mask[c]) acc += table[rec * rec_words] >> 24;
     }
     for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
     if ((threadIdx.x & 31) == 0) atomicAdd(out, acc);

@@ -1,7 +1,8 @@
 // FP64 MAP cost (replaces computeCost, MBIR_4D/XT_ICD_update.c:185-318).
 //
 // Data term: 1/2 sum w e^2 where |e sqrt(w)| < T, else the generalised-Huber
-// branch 2 delta T |e sqrt(w)| + T^2 (1 - 2 delta) (XT_ICD_update.c:192-204).
+// branch 2 delta T |e sqrt(w)| + T^2 (1 - 2 delta) (XT_ICD_update.c:192-204);
+// the test is made as e^2 w < T^2.
 // Prior term: for every voxel the 13 causal spatial pairs (+x; the three +y
 // pairs of its slice; the nine pairs of the next slice) and the +t pair, each
 // filter weight times the qGGMRF potential |d|^q / sigma^q / (c + |d|^(q-p) /
@@ -22,11 +23,16 @@ constexpr int kCostBlocks = 148 * 8;
 
 int cost_partials_needed(const Geom &) { return 2 * kCostBlocks; }
 
-__device__ inline double qg_potential(double d, double q, double qmp, double sq, double sqp, double c)
+// qGGMRF potential |d|^q / sq / (c + |d|^(q-p) / sqp) in FP64, with the
+// reciprocals of the scale powers precomputed. |d|^(q-p) is exp((q-p) log|d|)
+// (relative error a few ulp of double); zero differences cost nothing.
+__device__ inline double qg_potential(float d, double q, double qmp, double inv_sq, double inv_sqp, double c)
 {
-    const double ad = fabs(d);
-    const double num = (q == 2.0 ? ad * ad : pow(ad, q)) / sq;
-    return num / (c + pow(ad, qmp) / sqp);
+    if (d == 0.0f) return 0.0;
+    const double ad = fabs((double)d);
+    const double lg = log(ad);
+    const double num = (q == 2.0 ? ad * ad : exp(q * lg)) * inv_sq;
+    return num / (c + exp(qmp * lg) * inv_sqp);
 }
 
 __device__ inline double block_sum(double v, double *sh)
@@ -53,12 +59,17 @@ __global__ void __launch_bounds__(kCostThreads) cost_partials_kernel(Geom g, con
     const long long stride = (long long)gridDim.x * blockDim.x;
     const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     double data = 0;
+    const double T2 = g.huber_T * g.huber_T;
     for (long long i = tid; i < nsino; i += stride) {
-        const double t = (double)err[i] * sqrt((double)w[i]);
-        if (fabs(t) < g.huber_T) data += t * t;
-        else data += 2.0 * g.huber_delta * g.huber_T * fabs(t) + g.huber_T * g.huber_T * (1.0 - 2.0 * g.huber_delta);
+        // |e sqrt(w)| < T  <=>  e^2 w < T^2; the square root is only needed on the Huber branch
+        const double e = (double)err[i], ww = (double)w[i];
+        const double t2 = e * e * ww;
+        if (t2 < T2) data += t2;
+        else data += 2.0 * g.huber_delta * g.huber_T * sqrt(t2) + T2 * (1.0 - 2.0 * g.huber_delta);
     }
     const double qmp = g.q - g.p;
+    const double inv_ssq = 1.0 / g.sigma_s_q, inv_ssqp = 1.0 / g.sigma_s_q_p;
+    const double inv_stq = 1.0 / g.sigma_t_q, inv_stqp = 1.0 / g.sigma_t_q_p;
     const int NX = g.N_x, NY = g.N_y, NZ = g.N_z, NT = g.N_time;
     const long long nvox = (long long)NT * NY * NX * NZ;
     double prior = 0;
@@ -74,7 +85,7 @@ __global__ void __launch_bounds__(kCostThreads) cost_partials_kernel(Geom g, con
             return x[(((size_t)ff * NY + jj) * NX + kk) * NZ + zz];
         };
         auto sf = [&](int dz, int dy, int dx) -> double { return g.spatial_filter[dz * 9 + dy * 3 + dx]; };
-        auto S = [&](float d) -> double { return qg_potential((double)d, g.q, qmp, g.sigma_s_q, g.sigma_s_q_p, g.c_s); };
+        auto S = [&](float d) -> double { return qg_potential(d, g.q, qmp, inv_ssq, inv_ssqp, g.c_s); };
         const bool jm = j - 1 >= 0, km = k - 1 >= 0, jp = j + 1 < NY, kp = k + 1 < NX, zp = z + 1 < NZ;
         double acc = 0;
         if (kp) acc += sf(1, 1, 2) * S(c - X(f, j, k + 1, z));
@@ -93,8 +104,7 @@ __global__ void __launch_bounds__(kCostThreads) cost_partials_kernel(Geom g, con
             }
         }
         if (f + 1 < NT)
-            acc += g.time_filter *
-                   qg_potential((double)(c - X(f + 1, j, k, z)), g.q, qmp, g.sigma_t_q, g.sigma_t_q_p, g.c_t);
+            acc += g.time_filter * qg_potential(c - X(f + 1, j, k, z), g.q, qmp, inv_stq, inv_stqp, g.c_t);
         prior += acc;
     }
     const double ds = block_sum(data, sh);

@@ -1,14 +1,11 @@
 // Layout conversions and the sparse forward / back projectors.
 //
 // Forward projection (replaces initErrorSinogam, MBIR_4D/XT_ICD_update.c:651-712,
-// and forward_project_voxel_AMat1D, XT_ForwardProject.c:44-61): one CTA per
-// (view, detector-channel chunk) keeps an FP64 accumulator for its chunk of the
-// view's sinogram row block in shared memory, streams every voxel column of
-// the view's frame (one warp per column, one lane per detector row), and adds
-// x * a into the channels the column's A record names. The A value is used
+// and forward_project_voxel_AMat1D, XT_ForwardProject.c:44-61): column-driven,
+// FP64 accumulation in an L2-resident FP64 image of the sinogram, rounded to
+// float once: e = y - A x (or A x when no y is given). The A value is used
 // unscaled, as the reference does here (the voxel update scales it by
-// delta_t, XT_VoxUpdate.c:61). The result is rounded to float once:
-// e = y - A x (or A x when no y is given).
+// delta_t, XT_VoxUpdate.c:61).
 //
 // Back projection (the adjoint, A^T s): one warp per (frame, voxel column),
 // lanes over detector rows, FP64 accumulation over the frame's views, then a
@@ -62,65 +59,56 @@ void launch_zfast_to_vol(const float *in, float *out, int N_time, int N_z, int N
     transpose_rows_cols<<<grid, block, 0, st>>>(in, out, nxy, N_z);
 }
 
-namespace {
-constexpr int kFwdThreads = 256;
-constexpr int kFwdSmemBytes = 96 * 1024;
-}  // namespace
-
-// grid: (channel chunks, N_p); dynamic smem: chunk * N_t doubles
-__global__ void __launch_bounds__(kFwdThreads) forward_project_kernel(
-    Geom g, const uint32_t *__restrict__ table, const int32_t *__restrict__ view_first,
-    const int32_t *__restrict__ views, const int32_t *__restrict__ view_frame, const float *__restrict__ x,
-    const float *__restrict__ y, float *__restrict__ out, int chunk)
+// One warp per (frame, voxel column), lane = detector row: every A entry of
+// the column adds a * x into an FP64 accumulator image of the sinogram with a
+// global FP64 reduction (red.global.add.f64, performed in L2). Columns whose
+// voxels are all zero are skipped.
+__global__ void __launch_bounds__(256) forward_project_kernel(Geom g, const uint32_t *__restrict__ table,
+                                                             const int32_t *__restrict__ view_first,
+                                                             const float *__restrict__ x, double *__restrict__ acc)
 {
-    extern __shared__ double acc[];
-    const int vi = blockIdx.y;  // position in views[]
-    const int f = view_frame[vi];
-    const int fv0 = view_first[f], nv = view_first[f + 1] - fv0, v = vi - fv0;
-    const int view = views[vi];
-    const int r0 = blockIdx.x * chunk, r1 = min(r0 + chunk, g.N_r);
-    const int NT = g.N_t, nxy = g.N_x * g.N_y;
-    for (int i = threadIdx.x; i < (r1 - r0) * NT; i += blockDim.x) acc[i] = 0.0;
-    __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-    const int z = lane / g.z_overlap;
-    const uint32_t *rec0 = table + ((size_t)fv0 * nxy + v) * g.rec_words;
-    const float *xf = x + (size_t)f * nxy * g.N_z;
-    for (int c = warp; c < nxy; c += nw) {
-        const uint32_t *rec = rec0 + (size_t)c * nv * g.rec_words;
-        const uint32_t hdr = __ldg(rec);
-        const int cnt = hdr >> 16, first = hdr & 0xFFFF;
-        if (cnt == 0 || first + cnt <= r0 || first >= r1) continue;
-        if (lane >= NT) continue;
-        const double xv = (double)__ldg(xf + (size_t)c * g.N_z + z);
-        if (xv == 0.0) continue;
-        for (int q = 0; q < cnt; q++) {
-            const int r = first + q;
-            if (r < r0 || r >= r1) continue;
-            const double a = (double)__uint_as_float(__ldg(rec + 1 + q));
-            atomicAdd(&acc[(r - r0) * NT + lane], xv * a);
+    const int nxy = g.N_x * g.N_y;
+    const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (gw >= (long long)g.N_time * nxy) return;
+    const int f = (int)(gw / nxy), c = (int)(gw - (long long)f * nxy);
+    const bool row_ok = lane < g.N_t;
+    const double xv = row_ok ? (double)__ldg(x + ((size_t)f * nxy + c) * g.N_z + lane / g.z_overlap) : 0.0;
+    if (__all_sync(0xffffffffu, xv == 0.0)) return;
+    const int fv0 = view_first[f], nv = view_first[f + 1] - fv0;
+    const uint32_t *rec = table + ((size_t)fv0 * nxy + (size_t)c * nv) * g.rec_words;
+    if (!row_ok) return;
+    constexpr int U = 4;
+    for (int v0 = 0; v0 < nv; v0 += U) {
+        uint32_t hdr[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) hdr[u] = v0 + u < nv ? __ldg(rec + (size_t)(v0 + u) * g.rec_words) : 0u;
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int cnt = hdr[u] >> 24, row = hdr[u] & 0xFFFFFF;
+            const uint32_t *r = rec + (size_t)(v0 + u) * g.rec_words + 1;
+            for (int q = 0; q < cnt; q++)
+                atomicAdd(acc + (size_t)(row + q) * g.N_t + lane, xv * (double)__uint_as_float(__ldg(r + q)));
         }
-    }
-    __syncthreads();
-    const size_t obase = ((size_t)view * g.N_r + r0) * NT;
-    for (int i = threadIdx.x; i < (r1 - r0) * NT; i += blockDim.x) {
-        const double s = acc[i];
-        out[obase + i] = y ? (float)((double)y[obase + i] - s) : (float)s;
     }
 }
 
-void launch_forward_project(const Geom &g, const uint32_t *d_table, const int32_t *d_view_first,
-                            const int32_t *d_views, const int32_t * /*d_view_local*/, const int32_t *d_view_frame,
-                            const float *d_x, const float *d_y, float *d_out, cudaStream_t st)
+__global__ void finish_projection_kernel(size_t n, const double *__restrict__ acc, const float *__restrict__ y,
+                                         float *__restrict__ out)
 {
-    int chunk = kFwdSmemBytes / (int)(sizeof(double) * g.N_t);
-    if (chunk > g.N_r) chunk = g.N_r;
-    const int nchunks = (g.N_r + chunk - 1) / chunk;
-    const size_t smem = (size_t)chunk * g.N_t * sizeof(double);
-    cudaFuncSetAttribute(forward_project_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kFwdSmemBytes);
-    dim3 grid(nchunks, g.N_p);
-    forward_project_kernel<<<grid, kFwdThreads, smem, st>>>(g, d_table, d_view_first, d_views, d_view_frame, d_x,
-                                                             d_y, d_out, chunk);
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        out[i] = y ? (float)((double)y[i] - acc[i]) : (float)acc[i];
+}
+
+void launch_forward_project(const Geom &g, const uint32_t *d_table, const int32_t *d_view_first,
+                            const float *d_x, const float *d_y, double *d_acc, float *d_out, cudaStream_t st)
+{
+    const size_t n = (size_t)g.N_p * g.N_r * g.N_t;
+    cudaMemsetAsync(d_acc, 0, n * sizeof(double), st);
+    const long long warps = (long long)g.N_time * g.N_x * g.N_y;
+    const long long blocks = (warps * 32 + 255) / 256;
+    forward_project_kernel<<<(unsigned)blocks, 256, 0, st>>>(g, d_table, d_view_first, d_x, d_acc);
+    finish_projection_kernel<<<148 * 8, 256, 0, st>>>(n, d_acc, d_y, d_out);
 }
 
 // One warp per (frame, column); out is [N_time][N_y][N_x][N_z].
@@ -139,11 +127,10 @@ __global__ void back_project_kernel(Geom g, const uint32_t *__restrict__ table,
     if (lane < g.N_t) {
         for (int v = 0; v < nv; v++, rec += g.rec_words) {
             const uint32_t hdr = __ldg(rec);
-            const int cnt = hdr >> 16, first = hdr & 0xFFFF;
-            const int view = views[fv0 + v];
+            const int cnt = hdr >> 24, row = hdr & 0xFFFFFF;
             for (int q = 0; q < cnt; q++) {
                 const double a = (double)__uint_as_float(__ldg(rec + 1 + q));
-                acc += a * (double)__ldg(sino + ((size_t)view * g.N_r + first + q) * g.N_t + lane);
+                acc += a * (double)__ldg(sino + ((size_t)row + q) * g.N_t + lane);
             }
         }
     }

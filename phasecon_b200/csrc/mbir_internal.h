@@ -69,10 +69,10 @@ void launch_count_masked_nnz(const Geom &g, int n_assigned, const int32_t *d_vie
                              const uint8_t *d_mask, const uint32_t *d_table, unsigned long long *d_out,
                              cudaStream_t st);
 
-// e = y - A x (FP64 accumulation); when d_y is null the result is A x itself.
+// e = y - A x (FP64 accumulation in d_acc, N_p*N_r*N_t doubles); when d_y is
+// null the result is A x itself. Rows of views outside every frame get y (or 0).
 void launch_forward_project(const Geom &g, const uint32_t *d_table, const int32_t *d_view_first,
-                            const int32_t *d_views, const int32_t *d_view_local, const int32_t *d_view_frame,
-                            const float *d_x, const float *d_y, float *d_out, cudaStream_t st);
+                            const float *d_x, const float *d_y, double *d_acc, float *d_out, cudaStream_t st);
 void launch_back_project(const Geom &g, const uint32_t *d_table, const int32_t *d_view_first,
                          const int32_t *d_views, const float *d_sino, float *d_x, cudaStream_t st);
 
@@ -89,14 +89,16 @@ struct IcdLaunch {
     int phase;            // 0..3
     int iter;             // 1-based iteration (zero-skipping starts at 2)
     int zero_skipping;
+    int unroll;           // views in flight per lane (1, 2, 4); the launcher caps it by record width
     uint64_t seed;
 };
 struct IcdStats {  // device accumulators
     unsigned long long updates, skipped;
     double sum_abs_dx, sum_abs_x;
 };
+// d_queue: one zeroed counter per launch (the persistent CTAs' work queue).
 void launch_icd_phase(const Geom &g, const IcdLaunch &L, const uint32_t *d_table, const int32_t *d_view_first,
-                      const int32_t *d_views, const uint8_t *d_mask, float *d_x, float *d_err, const float *d_w,
-                      float *d_mag, IcdStats *d_stats, cudaStream_t st);
+                      const uint8_t *d_mask, float *d_x, float *d_err, const float *d_w, float *d_mag,
+                      IcdStats *d_stats, unsigned int *d_queue, cudaStream_t st);
 
 }  // namespace mbirgpu

@@ -64,7 +64,7 @@ static int dalloc(T **p, size_t n, size_t *acc)
 Session::~Session()
 {
     void *ptrs[] = {d_y, d_w, d_err, d_x, d_tmp, d_table, d_Hr, d_cos, d_sin, d_views, d_view_first, d_view_frame,
-                    d_mask, d_mag, d_stats, d_cost_partials, d_cost_out, d_flag};
+                    d_mask, d_mag, d_stats, d_cost_partials, d_cost_out, d_flag, d_acc, d_queue};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     for (auto &ev : ev_pairs) {
@@ -115,7 +115,7 @@ int Session::init(const mbirgpu_problem *pb, const mbirgpu_options *o, int mult_
         dalloc(&d_view_frame, (size_t)g.N_p, &acc) || dalloc(&d_mask, nxy, &acc) ||
         dalloc(&d_mag, (size_t)g.N_time * nxy, &acc) || dalloc(&d_stats, 1, &acc) ||
         dalloc(&d_cost_partials, (size_t)cost_partials_needed(g), &acc) || dalloc(&d_cost_out, 2, &acc) ||
-        dalloc(&d_flag, 1, &acc))
+        dalloc(&d_flag, 1, &acc) || dalloc(&d_acc, n_sino, &acc) || dalloc(&d_queue, 4, &acc))
         return -1;
 
     // views not assigned to any frame keep no A records; frame map for the builder
@@ -201,13 +201,8 @@ void Session::choose_schedule()
 
 int Session::refresh_error()
 {
-    const Geom &g = hs.g;
-    Geom gb = g;
-    gb.N_p = n_assigned;
     // views outside every frame keep e = y (they never enter the problem)
-    CK(cudaMemcpyAsync(d_err, d_y, n_sino * sizeof(float), cudaMemcpyDeviceToDevice, st));
-    if (n_assigned)
-        launch_forward_project(gb, d_table, d_view_first, d_views, nullptr, d_view_frame, d_x, d_y, d_err, st);
+    launch_forward_project(hs.g, d_table, d_view_first, d_x, d_y, d_acc, d_err, st);
     CK(cudaGetLastError());
     return 0;
 }
@@ -249,6 +244,7 @@ int Session::icd_iteration(int iter, mbirgpu_iter_stats *out)
 {
     const Geom &g = hs.g;
     CK(cudaMemsetAsync(d_stats, 0, sizeof(IcdStats), st));
+    CK(cudaMemsetAsync(d_queue, 0, 4 * sizeof(unsigned int), st));
     IcdLaunch L{};
     L.sv = sv;
     L.n_sv_x = (g.N_x + sv - 1) / sv;
@@ -256,6 +252,7 @@ int Session::icd_iteration(int iter, mbirgpu_iter_stats *out)
     L.warps = warps;
     L.iter = iter;
     L.zero_skipping = opt.zero_skipping;
+    L.unroll = opt.icd_unroll > 0 ? opt.icd_unroll : 4;
     L.seed = opt.seed;
     Geom gb = g;
     gb.N_p = n_assigned;
@@ -270,7 +267,7 @@ int Session::icd_iteration(int iter, mbirgpu_iter_stats *out)
     for (int ph = 0; ph < 4; ph++) {
         L.phase = ph;
         if (timing) CK(cudaEventRecord(ev_pairs[ph].first, st));
-        launch_icd_phase(gb, L, d_table, d_view_first, d_views, d_mask, d_x, d_err, d_w, d_mag, d_stats, st);
+        launch_icd_phase(gb, L, d_table, d_view_first, d_mask, d_x, d_err, d_w, d_mag, d_stats, d_queue + ph, st);
         if (timing) CK(cudaEventRecord(ev_pairs[ph].second, st));
     }
     CK(cudaGetLastError());
@@ -354,8 +351,8 @@ int Session::amatrix(int32_t *first, int32_t *count, float *values)
                 const uint32_t *rec = tab.data() + (((size_t)fv0 * nxy) + c * nv + v) * g.rec_words;
                 const int view = hs.views[fv0 + v];
                 const size_t o = (size_t)view * nxy + c;
-                first[o] = rec[0] & 0xFFFF;
-                count[o] = rec[0] >> 16;
+                first[o] = (int32_t)(rec[0] & 0xFFFFFF) - view * g.N_r;
+                count[o] = rec[0] >> 24;
                 for (int q = 0; q < g.kmax; q++) std::memcpy(&values[o * g.kmax + q], &rec[1 + q], 4);
             }
     }
@@ -371,15 +368,11 @@ int Session::forward_project(const float *obj, float *sino)
         if (d_obj) cudaFree(d_obj);
         return -1;
     }
-    Geom gb = g;
-    gb.N_p = n_assigned;
     cudaError_t e = cudaMemcpyAsync(d_tmp, obj, n_vox * sizeof(float), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) {
         launch_vol_to_zfast(d_tmp, d_obj, g.N_time, g.N_z, g.N_y, g.N_x, st);
-        e = cudaMemsetAsync(d_out, 0, n_sino * sizeof(float), st);
+        launch_forward_project(g, d_table, d_view_first, d_obj, nullptr, d_acc, d_out, st);
     }
-    if (e == cudaSuccess && n_assigned)
-        launch_forward_project(gb, d_table, d_view_first, d_views, nullptr, d_view_frame, d_obj, nullptr, d_out, st);
     if (e == cudaSuccess) e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaMemcpyAsync(sino, d_out, n_sino * sizeof(float), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
@@ -431,9 +424,10 @@ void mbirgpu_default_options(mbirgpu_options *o)
     o->zero_skipping = 1;
     o->write_files = 1;
     o->compute_cost = 1;
-    o->refresh_every = 4;
+    o->refresh_every = 8;
     o->sv_size = 0;
     o->cta_warps = 0;
+    o->icd_unroll = 0;
     o->seed = 761521;  // the reference's srandom2 seed, XT_Engine.c:99
 }
 
@@ -444,6 +438,7 @@ int mbirgpu_set_options(const mbirgpu_options *o)
     if (o->max_iterations < 1) return fail("max_iterations must be positive");
     if (o->sv_size < 0 || o->sv_size > 16) return fail("sv_size must be 0 (auto) or 1..16");
     if (o->cta_warps < 0 || o->cta_warps > 8) return fail("cta_warps must be 0 (auto) or 1..8");
+    if (o->icd_unroll < 0 || o->icd_unroll > 4) return fail("icd_unroll must be 0 (auto) or 1..4");
     mbirgpu_options cur = mbirgpu::current_options();
     (void)cur;
     std::lock_guard<std::mutex> lk(mbirgpu::g_opt_mu);

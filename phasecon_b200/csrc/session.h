@@ -32,6 +32,8 @@ struct Session {
     IcdStats *d_stats = nullptr;
     double *d_cost_partials = nullptr, *d_cost_out = nullptr;
     int *d_flag = nullptr;
+    double *d_acc = nullptr;  // FP64 sinogram accumulator of the forward projector
+    unsigned int *d_queue = nullptr;  // super-voxel work-queue counters, one per colour phase
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pairs;
 
     ~Session();

@@ -40,7 +40,7 @@ class Options(C.Structure):
         ("mrf_p", C.c_double), ("mrf_q", C.c_double), ("alpha", C.c_double), ("max_iterations", C.c_int32),
         ("num_stages", C.c_int32), ("cost_rel_tol", C.c_double), ("zero_skipping", C.c_int32),
         ("write_files", C.c_int32), ("compute_cost", C.c_int32), ("refresh_every", C.c_int32),
-        ("sv_size", C.c_int32), ("cta_warps", C.c_int32), ("seed", C.c_uint64),
+        ("sv_size", C.c_int32), ("cta_warps", C.c_int32), ("icd_unroll", C.c_int32), ("seed", C.c_uint64),
     ]
 
 
