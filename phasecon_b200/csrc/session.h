@@ -39,6 +39,12 @@ struct Session {
     ~Session();
     int init(const mbirgpu_problem *pb, const mbirgpu_options *o, int mult_xy, int mult_z, void *stream);
     void choose_schedule();
+    int autotune();
+    struct TuneEntry {
+        int sv, warps;
+        double ms;
+    };
+    std::vector<TuneEntry> tune_log;
     int refresh_error();
     int set_object(const float *obj);
     int get_object(float *obj);

@@ -1,0 +1,49 @@
+"""Run a few ICD iterations of a synthetic workload (for profiling and quick checks).
+
+    python -m phasecon_b200.run_workload [--workload 4d|3d] [--iters N] [--sv S] [--warps W]
+                                         [--refresh] [--cost] [--ch-steps K]
+
+Builds the seeded workload (phasecon_b200/workloads.py), creates one session
+with the given schedule (autotuned when --sv/--warps are 0) and runs N ICD
+iterations from zero, then optionally one FP64 error-sinogram refresh and one
+FP64 cost evaluation. --ch-steps shortens the phantom simulation (same array
+sizes) to keep the number of unrelated kernel launches small under a profiler.
+"""
+from __future__ import annotations
+
+import argparse
+import time
+
+from . import Session, get_options
+from . import workloads as W
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--workload", default="4d", choices=["4d", "3d"])
+    ap.add_argument("--iters", type=int, default=2)
+    ap.add_argument("--sv", type=int, default=0)
+    ap.add_argument("--warps", type=int, default=0)
+    ap.add_argument("--refresh", action="store_true")
+    ap.add_argument("--cost", action="store_true")
+    ap.add_argument("--ch-steps", type=int, default=5000)
+    a = ap.parse_args(argv)
+    if a.workload == "4d":
+        pb, _, p = W.config_4d(ch_steps=a.ch_steps)
+    else:
+        pb, _, p = W.config_3d()
+    o = get_options()
+    o.mrf_p, o.refresh_every, o.sv_size, o.cta_warps = p, 0, a.sv, a.warps
+    s = Session(pb, options=o)
+    t0 = time.perf_counter()
+    for it in range(1, a.iters + 1):
+        st = s.icd_iteration(it)
+    if a.refresh:
+        s.refresh_error()
+    c = s.cost() if a.cost else None
+    print(f"workload {a.workload}: sv {s.info.sv_size} warps {s.info.cta_warps} iters {a.iters} "
+          f"updates/iter {st.voxel_updates} wall {time.perf_counter() - t0:.3f}s cost {c}")
+
+
+if __name__ == "__main__":
+    main()
