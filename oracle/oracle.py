@@ -345,3 +345,116 @@ def ref_reconstruct(pb: Problem, workdir: str, max_iter: int = 1000, num_stages:
     lib.ref_free(out)
     cost = np.fromfile(os.path.join(workdir, "cost.bin"), dtype=np.float64)
     return obj, cost, int(lib.ref_vox_updates())
+
+
+# --------------------------------------------------------------------------- PCMBIR reference (built from source)
+
+
+class PcParams(C.Structure):
+    """Mirror of PcParams in oracle/ref_pc_harness.c."""
+    _fields_ = [("rows", C.c_int32), ("cols", C.c_int32), ("delta_rows", C.c_double), ("delta_cols", C.c_double),
+                ("wavelength", C.c_double), ("distance", C.c_double), ("window_sigma", C.c_double),
+                ("mag_sig_s", C.c_double), ("mag_c_s", C.c_double), ("phase_sig_s", C.c_double),
+                ("phase_c_s", C.c_double), ("delta_over_beta", C.c_double), ("mrf_p", C.c_double)]
+
+
+_ref_pc = None
+
+
+def ref_pc_available() -> bool:
+    return os.path.exists(os.path.join(REF_DIR, "libref_pcmbir.so"))
+
+
+def ref_pc_lib() -> C.CDLL:
+    global _ref_pc
+    if _ref_pc is None:
+        lib = C.CDLL(os.path.join(REF_DIR, "libref_pcmbir.so"))
+        P = C.POINTER(PcParams)
+        lib.ref_pc_fresnel.argtypes = [P, _f64p, _f64p, C.c_int]
+        lib.ref_pc_sd_iter.argtypes = [P] + [_f64p] * 11 + [C.c_double]
+        lib.ref_pc_sd_iter.restype = C.c_double
+        lib.ref_pc_phase_projection.argtypes = [P] + [_f64p] * 8
+        lib.ref_pc_nms.argtypes = [P, C.c_int32, _f64p, _f64p, _f64p, _f64p, _f64p, _f64p, _u8p, C.c_double,
+                                   C.c_int32, C.c_double, _i32p]
+        lib.ref_pc_estimate.argtypes = [P] + [_f64p] * 15 + [C.c_int32, C.c_int32, C.c_int32, C.c_double,
+                                                              C.c_double]
+        lib.ref_pc_paganin.argtypes = [P, _f64p, _f64p, _f64p, C.c_double, _f64p, _f64p]
+        lib.ref_pc_filter.argtypes = [P, _f64p, _f64p]
+        _ref_pc = lib
+    return _ref_pc
+
+
+def pc_params(g) -> PcParams:
+    return PcParams(g.rows, g.cols, g.delta_rows, g.delta_cols, g.wavelength, g.distance, g.window_sigma,
+                    g.mag_sig_s, g.mag_c_s, g.phase_sig_s, g.phase_c_s, g.delta_over_beta, g.mrf_p)
+
+
+def _c(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def ref_pc_fresnel(g, x, herm=False):
+    xi = np.ascontiguousarray(np.stack([x.real, x.imag], -1), np.float64)
+    out = np.zeros_like(xi)
+    ref_pc_lib().ref_pc_fresnel(C.byref(pc_params(g)), xi, out, 1 if herm else 0)
+    return out[..., 0] + 1j * out[..., 1]
+
+
+def ref_pc_sd_iter(g, y, om, D, w, lam, buf):
+    arrs = [_c(y.real), _c(np.zeros_like(y.real)), _c(om.real), _c(om.imag), _c(D.real), _c(D.imag), _c(w.real),
+            _c(w.imag), _c(lam), _c(buf.real), _c(buf.imag)]
+    t = ref_pc_lib().ref_pc_sd_iter(C.byref(pc_params(g)), arrs[0], arrs[1], arrs[2], arrs[3], arrs[4], arrs[5],
+                                    arrs[6], arrs[7], arrs[8], arrs[9], arrs[10], g.nu)
+    return arrs[6] + 1j * arrs[7], arrs[2] + 1j * arrs[3], t
+
+
+def ref_pc_phase_projection(g, y, D, w):
+    om_r, om_i = np.zeros(y.shape), np.zeros(y.shape)
+    ref_pc_lib().ref_pc_phase_projection(C.byref(pc_params(g)), _c(y.real), _c(np.zeros(y.shape)), _c(D.real),
+                                         _c(D.imag), _c(w.real), _c(w.imag), om_r, om_i)
+    return om_r + 1j * om_i
+
+
+def ref_pc_nms(g, zr1, zi1, br, bi, nbr_r, nbr_i, flag, max_iter=50, thresh=0.005):
+    n = len(zr1)
+    zr = np.zeros((n, 4))
+    zi = np.zeros((n, 4))
+    zr[:, 1], zi[:, 1] = zr1, zi1
+    iters = np.zeros(n, np.int32)
+    ref_pc_lib().ref_pc_nms(C.byref(pc_params(g)), n, zr, zi, _c(br), _c(bi), _c(nbr_r), _c(nbr_i),
+                            np.ascontiguousarray(flag, np.uint8), g.nu, max_iter, thresh, iters)
+    return zr[:, 1].copy(), zi[:, 1].copy(), iters
+
+
+def ref_pc_estimate(g, y, om, D, zr, zi, lam, w, workdir, pret_iters=100, sd_iters=100, nms_iters=50):
+    R, Cc = y.shape
+    z_r = np.zeros((R, Cc, 4))
+    z_i = np.zeros((R, Cc, 4))
+    z_r[..., 1], z_i[..., 1] = zr, zi
+    om_r, om_i = _c(om.real), _c(om.imag)
+    w_r, w_i = _c(w.real), _c(w.imag)
+    v_r, v_i = np.zeros((R, Cc)), np.zeros((R, Cc))
+    cwd = os.getcwd()
+    os.makedirs(workdir, exist_ok=True)
+    os.chdir(workdir)
+    try:
+        ref_pc_lib().ref_pc_estimate(C.byref(pc_params(g)), _c(y.real), _c(np.zeros((R, Cc))), om_r, om_i, _c(D.real),
+                                     _c(D.imag), z_r, z_i, _c(lam), _c(zr), _c(zi), w_r, w_i, v_r, v_i, nms_iters,
+                                     sd_iters, pret_iters, g.mu, g.nu)
+        cost = np.fromfile("pret_cost_proj_0.bin", np.float64) if os.path.exists(
+            "pret_cost_proj_0.bin") else None
+    finally:
+        os.chdir(cwd)
+    return z_r[..., 1].copy(), z_i[..., 1].copy(), w_r + 1j * w_i, v_r + 1j * v_i, om_r + 1j * om_i, cost
+
+
+def ref_pc_paganin(g, meas, D):
+    zr, zi = np.zeros(meas.shape), np.zeros(meas.shape)
+    ref_pc_lib().ref_pc_paganin(C.byref(pc_params(g)), _c(meas), _c(D.real), _c(D.imag), g.wavenumber, zr, zi)
+    return zr, zi
+
+
+def ref_pc_filter(g):
+    f, d = np.zeros(27), np.zeros(4)
+    ref_pc_lib().ref_pc_filter(C.byref(pc_params(g)), f, d)
+    return f.reshape(3, 3, 3), d.reshape(2, 2)
