@@ -170,6 +170,96 @@ int mbirgpu_session_get_detector_response(mbirgpu_session *s, float *H_r);
 int mbirgpu_session_run(mbirgpu_session *s, int32_t max_iter, double *costs, int32_t *iters,
                         mbirgpu_iter_stats *total);
 
+/* --------------------------------------------------------------------------
+ * Phase-contrast tomography (PCMBIR_3D): per-view phase retrieval.
+ *
+ * Drop-in for phcontomo_reconstruct of PCMBIR_3D/XT_Engine.c:82-197
+ * (include/pcmbir4d.h:35). recon_type 1 runs single-material Paganin
+ * retrieval on every view and writes pag_mag_ret.bin / pag_phase_ret.bin
+ * (FP64, [proj_num][proj_cols][proj_rows] as the reference); recon_type 2
+ * reads them and runs the per-view phase-retrieval ADMM of
+ * estimate_complex_projection (PCMBIR_3D/XT_CmplxProjEst.c:91-229), writing
+ * mag_tomo_aux / phase_tomo_aux (the estimated complex projections),
+ * mag_pret_aux / phase_pret_aux, mag_pret_dual / phase_pret_dual,
+ * omega_real / omega_imag and the per-view pret_cost / pret_primal /
+ * pret_dual histories. Like the reference (XT_Engine.c:177-178) it returns
+ * *magobject = *phaseobject = NULL; results go to files. The tomographic
+ * ICD inside the ADMM is compiled out in the reference (ENABLE_TOMO_RECONS is
+ * never defined) and is not part of this entry point either.
+ * ------------------------------------------------------------------------ */
+int phcontomo_reconstruct(float **magobject, float **phaseobject, float *measurements, float *brights,
+                          float *proj_angles, float *proj_times, float *recon_times, int32_t proj_rows,
+                          int32_t proj_cols, int32_t proj_num, int32_t recon_num, float vox_wid, float rot_center,
+                          float mag_sig_s, float mag_sig_t, float mag_c_s, float mag_c_t, float phase_sig_s,
+                          float phase_sig_t, float phase_c_s, float phase_c_t, float convg_thresh,
+                          float obj2det_dist, float light_energy, float pag_regparam, uint8_t restart,
+                          uint8_t recon_type, FILE *debug_msg_ptr);
+
+typedef struct mbirgpu_pc_session mbirgpu_pc_session;
+
+typedef struct {
+    const float *measurements; /* [proj_num][proj_rows][proj_cols] intensities */
+    const float *brights;      /* [proj_rows][proj_cols] bright field */
+    int32_t proj_rows, proj_cols, proj_num;
+    float vox_wid;             /* detector pitch; delta_r = delta_t = vox_wid (XT_Init.c:278-279, 391-392) */
+    float mag_sig_s, mag_c_s, phase_sig_s, phase_c_s;
+    float obj2det_dist;        /* propagation distance, same unit as vox_wid (um) */
+    float light_energy;        /* keV; wavelength = hc / E (XT_Init.c:258) */
+    float pag_regparam;        /* delta / beta */
+} mbirgpu_pc_problem;
+
+typedef struct {
+    int32_t pret_max_iter;     /* PRet_MaxIter, XT_Init.c:517: 100 */
+    int32_t sd_max_iter;       /* SteepDes_MaxIter, :518: 100 */
+    int32_t nms_max_iter;      /* NMS_MaxIter, :515: 50 */
+    double pret_threshold;     /* PRet_threshold, :522: 1e-7 */
+    double sd_threshold;       /* SteepDes_threshold, :523: 5e-4 */
+    double nms_threshold;      /* NMS_threshold, :520: 5e-3 */
+    double mu, nu;             /* ADMM_mu, ADMM_nu for recon_type 2, :496-497: 0.5 */
+    double mrf_p, mrf_q;       /* MRF_P, MRF_Q of PCMBIR_3D/XT_Constants.h:146-147 */
+    int32_t nms_order;         /* proximal sweep order: 0 = the reference's raster order,
+                                  kept exactly by anti-diagonal wavefronts (default);
+                                  1 = four colour classes (more parallel, other order) */
+} mbirgpu_pc_options;
+
+typedef struct {
+    int64_t sd_steps;          /* steepest-descent steps run, summed over views */
+    int64_t fresnel_transforms;/* Fresnel transforms run, summed over views */
+    double kernel_ms;          /* device time of the run (CUDA events) */
+} mbirgpu_pc_stats;
+
+void mbirgpu_pc_default_options(mbirgpu_pc_options *opt);
+
+/* Replaces the phase-contrast part of initStructures (PCMBIR_3D/XT_Init.c:
+ * 251-549): measurements -> sqrt(I) / sqrt(mean bright), D = sqrt(bright) /
+ * sqrt(mean bright), transfer tables of the Fresnel and Hermitian transforms.
+ * Host images exchanged with a session are [proj_num][proj_cols][proj_rows]
+ * (the reference's [N_p][N_r][N_t]); complex images are interleaved
+ * (re, im) floats. */
+int mbirgpu_pc_session_create(mbirgpu_pc_session **out, const mbirgpu_pc_problem *pb,
+                              const mbirgpu_pc_options *opt, void *stream);
+int mbirgpu_pc_session_destroy(mbirgpu_pc_session *s);
+/* Batched Fresnel transform of every view (herm = 0: compute_FresnelTran,
+ * herm = 1: compute_HermFresnelTran). */
+int mbirgpu_pc_fresnel(mbirgpu_pc_session *s, const float *in, float *out, int32_t herm);
+/* Paganin retrieval of every view into the session's z (and, if not NULL, zr/zi). */
+int mbirgpu_pc_paganin(mbirgpu_pc_session *s, float *zr, float *zi);
+int mbirgpu_pc_set_z(mbirgpu_pc_session *s, const float *zr, const float *zi);
+/* ADMM start of initErrorSinogam (PCMBIR_3D/XT_ICD_update.c:680-799):
+ * w = e^{-z}, v = 0, Omega = phase of y / H(D w). */
+int mbirgpu_pc_init_admm(mbirgpu_pc_session *s);
+int mbirgpu_pc_set_state(mbirgpu_pc_session *s, const float *w, const float *v, const float *omega);
+int mbirgpu_pc_get_state(mbirgpu_pc_session *s, float *zr, float *zi, float *w, float *v, float *omega);
+/* One steepest-descent step of every view towards buf (steepest_descent_iter,
+ * PCMBIR_3D/XT_PhaseRet.c:205-270); thresh[proj_num] receives each view's statistic. */
+int mbirgpu_pc_sd_step(mbirgpu_pc_session *s, const float *buf, float *thresh);
+/* One Nelder-Mead proximal sweep over every pixel of every view with b = w - v. */
+int mbirgpu_pc_nms_sweep(mbirgpu_pc_session *s);
+/* The per-view ADMM: costs [proj_num][pret_max_iter + 1] (may be NULL, FP64
+ * phase-retrieval cost before and after each iteration, NaN after a view
+ * stops), iters [proj_num] (may be NULL). */
+int mbirgpu_pc_run(mbirgpu_pc_session *s, double *costs, int32_t *iters, mbirgpu_pc_stats *stats);
+
 #ifdef __cplusplus
 }
 #endif

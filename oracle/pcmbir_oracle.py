@@ -280,26 +280,39 @@ def paganin(g: PcGeom, meas, D):
     return t / 2, t * g.delta_over_beta / 2
 
 
+def pixel_order(R, Cc, order="raster"):
+    """Pixel visiting order of one proximal sweep: the reference's raster order
+    (XT_CmplxProjEst.c:117-160), or "color": the four (row parity, column
+    parity) classes one after the other, raster order inside each -- no two
+    8-neighbours share a class, so a class may be updated in parallel."""
+    if order == "raster":
+        return [(j, k) for j in range(R) for k in range(Cc)]
+    return [(j, k) for c in range(4) for j in range(c >> 1, R, 2) for k in range(c & 1, Cc, 2)]
+
+
+def nms_sweep(g: PcGeom, zr, zi, b, nms_iters=50, nms_thresh=0.005, order="raster"):
+    """One Nelder-Mead proximal sweep over every pixel of one view, in place."""
+    cost_fn = NmsCost(g)
+    for j, k in pixel_order(*zr.shape, order):
+        nr, ni, fl = neighbourhood(zr, zi, j, k)
+        zr[j, k], zi[j, k], _ = nelder_mead(cost_fn, zr[j, k], zi[j, k], b[j, k].real, b[j, k].imag,
+                                            nr, ni, fl, nms_iters, nms_thresh)
+
+
 def estimate_projection(g: PcGeom, y, om, D, zr, zi, lam, w, pret_iters=100, sd_iters=100, nms_iters=50,
-                        pret_thresh=1e-7, sd_thresh=5e-4, nms_thresh=0.005):
+                        pret_thresh=1e-7, sd_thresh=5e-4, nms_thresh=0.005, order="raster"):
     """Per-view phase-retrieval ADMM (estimate_complex_projection,
-    XT_CmplxProjEst.c:91-229, macro-off): per iteration a raster-order
-    Nelder-Mead proximal update of every pixel's z against b = w - v, up to
-    sd_iters steepest-descent steps on w towards e^{-z} + v, the dual update
+    XT_CmplxProjEst.c:91-229, macro-off): per iteration a Nelder-Mead
+    proximal update of every pixel's z against b = w - v (raster order as the
+    reference, or colour classes, see pixel_order), up to sd_iters
+    steepest-descent steps on w towards e^{-z} + v, the dual update
     v += e^{-z} - w, and a stop on the dual residual. The dual starts at zero
     (:108-109). Returns (zr, zi, w, v, Omega, cost history)."""
     zr, zi, w, om = zr.copy(), zi.copy(), w.copy(), om.copy()
     v = np.zeros_like(w)
-    cost_fn = NmsCost(g)
     costs = [pret_cost(g, y, D, zr, zi, lam)]
-    R, Cc = zr.shape
     for it in range(pret_iters):
-        b = w - v
-        for j in range(R):
-            for k in range(Cc):
-                nr, ni, fl = neighbourhood(zr, zi, j, k)
-                zr[j, k], zi[j, k], _ = nelder_mead(cost_fn, zr[j, k], zi[j, k], b[j, k].real, b[j, k].imag,
-                                                    nr, ni, fl, nms_iters, nms_thresh)
+        nms_sweep(g, zr, zi, w - v, nms_iters, nms_thresh, order)
         wold = w.copy()
         ez = np.exp(-zr) * (np.cos(-zi) + 1j * np.sin(-zi))
         buf = ez + v

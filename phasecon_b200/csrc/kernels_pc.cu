@@ -1,0 +1,515 @@
+// Phase-contrast (PCMBIR) kernels: batched Fresnel transforms and the
+// per-view phase-retrieval ADMM pieces, all views of a scan in each launch.
+//
+// Fresnel transform of one view (replaces compute_FresnelTran /
+// compute_HermFresnelTran, PCMBIR_3D/XT_FresnelTran.c:12-137):
+//   pass 1  rows:  prologue op forms the input, FFT along t (length N_t)
+//   pass 2  cols:  FFT along r (length N_r), multiply by the transfer table,
+//                  inverse FFT along r
+//   pass 3  rows:  inverse FFT along t, scale by 1/(N_r N_t), epilogue op
+// so every pass reads and writes the view once. FFTs are radix-2 Stockham
+// (self-sorting, ping-pong between two shared-memory buffers) with twiddles
+// exp(-2 pi i m / n_max) precomputed in double and rounded once to float.
+// Per-view sums needed by the steepest-descent step size and the stopping
+// tests are block-reduced and added in FP64. Views whose loop has stopped
+// (per-view flags) skip every launch.
+#include <cfloat>
+#include "pc_internal.h"
+
+namespace mbirgpu {
+
+namespace {
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) { return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+__device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+__device__ __forceinline__ float cabs2(float2 a) { return a.x * a.x + a.y * a.y; }
+
+// nseq sequences of length n (power of two) stored back to back in `a`;
+// radix-2 Stockham passes ping-pong between a and b. Returns the buffer
+// holding the result. tw[m] = exp(-2 pi i m / nmax), m < nmax / 2.
+__device__ float2 *fft_smem(float2 *a, float2 *b, int n, int log2n, int nseq, const float2 *tw, int nmax,
+                            bool inverse)
+{
+    const int half = n >> 1;
+    for (int L = 1, s = 0; L < n; L <<= 1, s++) {
+        const int tstride = nmax / (L << 1);
+        for (int idx = threadIdx.x; idx < nseq * half; idx += blockDim.x) {
+            const int q = idx >> (log2n - 1), j = idx & (half - 1);
+            const int k = j & (L - 1);
+            float2 w = tw[k * tstride];
+            if (inverse) w.y = -w.y;
+            const float2 x0 = a[q * n + j], x1 = a[q * n + j + half];
+            const float2 t = cmul(w, x1);
+            const int o = q * n + ((j - k) << 1) + k;
+            b[o] = cadd(x0, t);
+            b[o + L] = csub(x0, t);
+        }
+        __syncthreads();
+        float2 *tmp = a;
+        a = b;
+        b = tmp;
+    }
+    return a;
+}
+
+__device__ __forceinline__ void load_twiddles(float2 *s_tw, const float2 *tw, int nmax)
+{
+    for (int i = threadIdx.x; i < nmax / 2; i += blockDim.x) s_tw[i] = tw[i];
+}
+
+// FP64 block sum of per-thread values, one atomicAdd per CTA.
+__device__ void block_add(double v, double *dst, double *sh)
+{
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) sh[warp] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0;
+        for (int i = 0; i < (int)(blockDim.x >> 5); i++) s += sh[i];
+        atomicAdd(dst, s);
+    }
+    __syncthreads();
+}
+
+// e^{-z} for z = zr + i zi
+__device__ __forceinline__ float2 expz(float zr, float zi)
+{
+    const float e = expf(-zr);
+    float s, c;
+    sincosf(-zi, &s, &c);
+    return make_float2(e * c, e * s);
+}
+
+// the same with the hardware approximations, for the Nelder-Mead search whose
+// stop rule (a 0.005 % relative vertex movement) is far above their error
+__device__ __forceinline__ float2 expz_fast(float zr, float zi)
+{
+    const float e = __expf(-zr);
+    float s, c;
+    __sincosf(-zi, &s, &c);
+    return make_float2(e * c, e * s);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------- pass 1
+__global__ void pc_rows_forward(PcDims d, PcArgs A, int prologue)
+{
+    extern __shared__ float2 smem[];
+    const int v = blockIdx.y;
+    if (A.active && !A.active[v]) return;
+    const int C = d.C, rpc = d.rows_per_cta;
+    float2 *s_tw = smem, *a = smem + d.nmax / 2, *b = a + rpc * C;
+    load_twiddles(s_tw, A.tw, d.nmax);
+    const int r0 = blockIdx.x * rpc;
+    const size_t vb = (size_t)v * d.N;
+    for (int e = threadIdx.x; e < rpc * C; e += blockDim.x) {
+        const int r = r0 + e / C, c = e % C;
+        float2 x = make_float2(0.f, 0.f);
+        if (r < d.R) {
+            const size_t i = vb + (size_t)r * C + c, p = (size_t)r * C + c;
+            switch (prologue) {
+            case PC_IN_PLAIN: x = A.in[i]; break;
+            case PC_IN_DW: x = cscale(A.in[i], A.D[p]); break;
+            case PC_IN_DEZ: x = cscale(expz(A.zr[i], A.zi[i]), A.D[p]); break;
+            case PC_IN_PAG: {
+                const float m = A.y[i];
+                x = make_float2(m * m / (A.D[p] * A.D[p]), 0.f);
+            } break;
+            }
+        }
+        a[e] = x;
+    }
+    __syncthreads();
+    const int nrows = min(rpc, d.R - r0);
+    float2 *res = fft_smem(a, b, C, d.logC, nrows, s_tw, d.nmax, false);
+    for (int e = threadIdx.x; e < nrows * C; e += blockDim.x) A.work[vb + (size_t)r0 * C + e] = res[e];
+}
+
+// ---------------------------------------------------------------------------- pass 2
+__global__ void pc_cols_filter(PcDims d, PcArgs A, const float2 *__restrict__ transfer)
+{
+    extern __shared__ float2 smem[];
+    const int v = blockIdx.y;
+    if (A.active && !A.active[v]) return;
+    const int R = d.R, C = d.C, cb = d.cols_per_cta;
+    float2 *s_tw = smem, *a = smem + d.nmax / 2, *b = a + cb * R;
+    load_twiddles(s_tw, A.tw, d.nmax);
+    const int c0 = blockIdx.x * cb;
+    const size_t vb = (size_t)v * d.N;
+    for (int e = threadIdx.x; e < cb * R; e += blockDim.x) {
+        const int r = e / cb, q = e % cb;
+        a[q * R + r] = A.work[vb + (size_t)r * C + c0 + q];
+    }
+    __syncthreads();
+    float2 *res = fft_smem(a, b, R, d.logR, cb, s_tw, d.nmax, false);
+    float2 *other = res == a ? b : a;
+    for (int e = threadIdx.x; e < cb * R; e += blockDim.x) {
+        const int q = e / R, r = e % R;
+        res[e] = cmul(res[e], transfer[(size_t)r * C + c0 + q]);
+    }
+    __syncthreads();
+    res = fft_smem(res, other, R, d.logR, cb, s_tw, d.nmax, true);
+    for (int e = threadIdx.x; e < cb * R; e += blockDim.x) {
+        const int r = e / cb, q = e % cb;
+        A.work[vb + (size_t)r * C + c0 + q] = res[q * R + r];
+    }
+}
+
+// ---------------------------------------------------------------------------- pass 3
+__global__ void pc_rows_inverse(PcDims d, PcArgs A, int epilogue)
+{
+    extern __shared__ float2 smem[];
+    __shared__ double s_red[32];
+    const int v = blockIdx.y;
+    if (A.active && !A.active[v]) return;
+    const int C = d.C, rpc = d.rows_per_cta;
+    float2 *s_tw = smem, *a = smem + d.nmax / 2, *b = a + rpc * C;
+    load_twiddles(s_tw, A.tw, d.nmax);
+    const int r0 = blockIdx.x * rpc;
+    const int nrows = min(rpc, d.R - r0);
+    const size_t vb = (size_t)v * d.N;
+    for (int e = threadIdx.x; e < nrows * C; e += blockDim.x) a[e] = A.work[vb + (size_t)r0 * C + e];
+    __syncthreads();
+    float2 *res = fft_smem(a, b, C, d.logC, nrows, s_tw, d.nmax, true);
+    const float inv_n = 1.0f / (float)d.N;
+    double acc = 0.0;
+    for (int e = threadIdx.x; e < nrows * C; e += blockDim.x) {
+        const size_t i = vb + (size_t)r0 * C + e, p = (size_t)r0 * C + e;
+        const float2 t = cscale(res[e], inv_n);
+        switch (epilogue) {
+        case PC_OUT_PLAIN: A.out[i] = t; break;
+        case PC_OUT_GRES: {  // conj(Omega) Lambda (Omega t - y)
+            const float2 om = A.omega[i];
+            const float lam = A.lam ? A.lam[i] : 1.0f;
+            const float2 r = csub(cmul(om, t), make_float2(A.y[i], 0.f));
+            A.out[i] = cmul(cconj(om), cscale(r, lam));
+        } break;
+        case PC_OUT_GRAD: {  // g = D t + nu (w - buf); sum |g|^2
+            const float2 gw = csub(A.w[i], A.buf[i]);
+            const float2 g = cadd(cscale(t, A.D[p]), cscale(gw, d.nu));
+            A.g[i] = g;
+            acc += (double)cabs2(g);
+        } break;
+        case PC_OUT_SFWD: {  // conj(Omega) Lambda Omega t
+            const float2 om = A.omega[i];
+            const float lam = A.lam ? A.lam[i] : 1.0f;
+            A.out[i] = cmul(cconj(om), cscale(cmul(om, t), lam));
+        } break;
+        case PC_OUT_SDEN: {  // sum Re(conj(g) D t)
+            const float2 g = A.g[i];
+            const float2 dt = cscale(t, A.D[p]);
+            acc += (double)g.x * (double)dt.x + (double)g.y * (double)dt.y;
+        } break;
+        case PC_OUT_OMEGA: {  // Omega = (y / t) / |y / t|
+            const float yy = A.y[i];
+            const float den = cabs2(t) + FLT_MIN;
+            const float2 q = make_float2(yy * t.x / den, -yy * t.y / den);
+            const float m = sqrtf(cabs2(q)) + FLT_MIN;
+            A.omega[i] = make_float2(q.x / m, q.y / m);
+        } break;
+        case PC_OUT_PCOST: {  // sum Lambda (y - |t|)^2 / 2
+            const float lam = A.lam ? A.lam[i] : 1.0f;
+            const double rr = (double)A.y[i] - sqrt((double)cabs2(t));
+            acc += rr * rr * lam / 2.0;
+        } break;
+        case PC_OUT_PAG: {  // Paganin: thickness -log|Re t|
+            const float th = -logf(fabsf(t.x));
+            A.zr[i] = th / 2.0f;
+            A.zi[i] = th * d.delta_over_beta / 2.0f;
+        } break;
+        }
+    }
+    if (epilogue == PC_OUT_GRAD || epilogue == PC_OUT_SDEN || epilogue == PC_OUT_PCOST)
+        block_add(acc, A.acc + (size_t)v * kPcAccSlots + A.acc_slot, s_red);
+}
+
+// ---------------------------------------------------------------------------- pointwise steps
+// w -= alpha g with alpha = sum|g|^2 / (sum Re(conj g D^H H'^H ..) + nu sum|g|^2 + eps)
+// (compute_stepsize, PCMBIR_3D/XT_PhaseRet.c:126-165); sums |alpha g| and |w|.
+__global__ void pc_sd_update(PcDims d, PcArgs A)
+{
+    __shared__ double s_red[32];
+    const int v = blockIdx.y;
+    if (A.active && !A.active[v]) return;
+    double *acc = A.acc + (size_t)v * kPcAccSlots;
+    const double num = acc[PC_ACC_GG], den = acc[PC_ACC_DEN] + d.nu * num;
+    const double alpha = num / (den + DBL_MIN);
+    const float af = (float)alpha;
+    double up = 0, val = 0;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < d.N; e += gridDim.x * blockDim.x) {
+        const size_t i = (size_t)v * d.N + e;
+        const float2 g = A.g[i];
+        const float2 w = csub(A.w[i], cscale(g, af));
+        A.w[i] = w;
+        up += fabs(alpha) * sqrt((double)cabs2(g));
+        val += sqrt((double)cabs2(w));
+    }
+    block_add(up, acc + PC_ACC_UP, s_red);
+    block_add(val, acc + PC_ACC_VAL, s_red);
+}
+
+// per view: threshold 100 sum|alpha g| / sum|w|; stop after step j > 1 when below
+// the steepest-descent threshold (XT_CmplxProjEst.c:179-183)
+__global__ void pc_sd_finish(PcDims d, PcArgs A, int step, float sd_thresh)
+{
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= d.V) return;
+    if (A.active && !A.active[v]) return;
+    double *acc = A.acc + (size_t)v * kPcAccSlots;
+    const double th = 100.0 * acc[PC_ACC_UP] / acc[PC_ACC_VAL];
+    A.sd_thresh_out[v] = (float)th;
+    A.sd_steps[v] = step + 1;
+    if (th < sd_thresh && step > 1) A.active[v] = 0;
+    for (int s = 0; s < PC_ACC_PRIMAL; s++) acc[s] = 0.0;
+}
+
+// wold = w; buf = e^{-z} + v (XT_CmplxProjEst.c:170-177)
+__global__ void pc_pret_prepare(PcDims d, PcArgs A)
+{
+    const int v = blockIdx.y;
+    if (A.active && !A.active[v]) return;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < d.N; e += gridDim.x * blockDim.x) {
+        const size_t i = (size_t)v * d.N + e;
+        A.wold[i] = A.w[i];
+        A.buf[i] = cadd(expz(A.zr[i], A.zi[i]), A.vdual[i]);
+    }
+}
+
+// v += e^{-z} - w; sums for the primal / dual residuals (XT_CmplxProjEst.c:186-199)
+__global__ void pc_pret_dual(PcDims d, PcArgs A)
+{
+    __shared__ double s_red[32];
+    const int v = blockIdx.y;
+    if (A.active && !A.active[v]) return;
+    double pr = 0, du = 0, sm = 0;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < d.N; e += gridDim.x * blockDim.x) {
+        const size_t i = (size_t)v * d.N + e;
+        const float2 w = A.w[i];
+        const float2 dd = csub(expz(A.zr[i], A.zi[i]), w);
+        const float2 nv = cadd(A.vdual[i], dd);
+        A.vdual[i] = nv;
+        const float2 dw = csub(w, A.wold[i]);
+        pr += (double)cabs2(dd);
+        du += (double)cabs2(dw);
+        sm += (double)cabs2(nv);
+    }
+    double *acc = A.acc + (size_t)v * kPcAccSlots;
+    block_add(pr, acc + PC_ACC_PRIMAL, s_red);
+    block_add(du, acc + PC_ACC_DUALW, s_red);
+    block_add(sm, acc + PC_ACC_VSUM, s_red);
+}
+
+// the decorrelated qGGMRF prior over the causal pixel pairs (+col, +row,
+// +row+col, +row-col) of compute_pretcost (XT_CmplxProjEst.c:43-83), FP64
+__global__ void pc_prior_cost(PcDims d, PcArgs A, const __grid_constant__ PcPrior P)
+{
+    __shared__ double s_red[32];
+    const int v = blockIdx.y;
+    if (A.active && !A.active[v]) return;
+    double acc = 0;
+    const int R = d.R, C = d.C;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < d.N; e += gridDim.x * blockDim.x) {
+        const int j = e / C, k = e % C;
+        const size_t i = (size_t)v * d.N + e;
+        const double zr = A.zr[i], zi = A.zi[i];
+        const int dj[4] = {0, 1, 1, 1}, dk[4] = {1, 0, 1, -1};
+        for (int m = 0; m < 4; m++) {
+            const int jj = j + dj[m], kk = k + dk[m];
+            if (jj >= R || kk < 0 || kk >= C) continue;
+            const size_t n = (size_t)v * d.N + (size_t)jj * C + kk;
+            const double db = zr - (double)A.zr[n], dd = zi - (double)A.zi[n];
+            const double dph = P.T00 * dd + P.T01 * db, dmg = P.T10 * dd + P.T11 * db;
+            const double fw = P.f[(dj[m] + 1) * 3 + (dk[m] + 1)];
+            const double aph = fabs(dph), amg = fabs(dmg);
+            if (aph > 0)
+                acc += fw * (aph * aph / P.ph_sq) / (P.ph_c + exp(P.qmp * log(aph)) / P.ph_sqp);
+            if (amg > 0)
+                acc += fw * (amg * amg / P.mg_sq) / (P.mg_c + exp(P.qmp * log(amg)) / P.mg_sqp);
+        }
+    }
+    block_add(acc, A.acc + (size_t)v * kPcAccSlots + PC_ACC_PRIOR, s_red);
+}
+
+// per view: dual residual sqrt(sum|w - wold|^2 / sum|v|^2); stop when below the
+// phase-retrieval threshold after iteration 1 (XT_CmplxProjEst.c:198-214)
+__global__ void pc_pret_finish(PcDims d, PcArgs A, int iter, float pret_thresh, double *costs_out)
+{
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= d.V) return;
+    if (A.active && !A.active[v]) return;
+    double *acc = A.acc + (size_t)v * kPcAccSlots;
+    const double dual = sqrt(acc[PC_ACC_DUALW] / acc[PC_ACC_VSUM]);
+    const double primal = sqrt(acc[PC_ACC_PRIMAL] / (double)d.N);
+    A.dual_res[v] = dual;
+    A.primal_res[v] = primal;
+    if (costs_out) costs_out[v] = acc[PC_ACC_PCOST] + acc[PC_ACC_PRIOR];
+    A.pret_iters[v] = iter + 1;
+    if (dual < pret_thresh && iter > 1) A.active[v] = 0;
+    for (int s = 0; s < kPcAccSlots; s++) acc[s] = 0.0;
+}
+
+// ---------------------------------------------------------------------------- Nelder-Mead proximal
+// Per-pixel 2-D Nelder-Mead on z = (zr, zi) minimising nu/2 |e^{-z} - b|^2 +
+// decorrelated qGGMRF over the 3x3 neighbourhood (Cost_NMS and
+// Nelder_Mead_Simplex_2DSearch, PCMBIR_3D/XT_Search.c:8-215), b = w - v. The
+// reference sweeps pixels in raster order (XT_CmplxProjEst.c:117-160);
+// pc_nms_wavefront keeps that order exactly, pc_nms updates colour classes.
+namespace {
+struct NmsCtx {
+    float br, bi, nu;
+    float nr[9], ni[9];
+    unsigned flags;
+    const PcPrior *P;
+};
+
+__device__ float nms_cost(const NmsCtx &c, float zr, float zi)
+{
+    const float2 ez = expz_fast(zr, zi);
+    float cost = ((ez.x - c.br) * (ez.x - c.br) + (ez.y - c.bi) * (ez.y - c.bi)) * c.nu / 2;
+    const PcPrior &P = *c.P;
+#pragma unroll
+    for (int a = 0; a < 9; a++) {
+        if (c.flags & (1u << a)) {
+            const float db = zr - c.nr[a], dd = zi - c.ni[a];
+            const float dph = P.T00_f * dd + P.T01_f * db, dmg = P.T10_f * dd + P.T11_f * db;
+            const float aph = fabsf(dph), amg = fabsf(dmg);
+            const float fw = P.f_f[a];
+            if (aph > 0.f) cost += fw * (aph * aph * P.ph_isq_f) / (P.ph_c_f + __expf(P.qmp_f * __logf(aph)) * P.ph_isqp_f);
+            if (amg > 0.f) cost += fw * (amg * amg * P.mg_isq_f) / (P.mg_c_f + __expf(P.qmp_f * __logf(amg)) * P.mg_isqp_f);
+        }
+    }
+    return cost;
+}
+}  // namespace
+
+namespace {
+// The search of Nelder_Mead_Simplex_2DSearch for pixel (j, k) of view v,
+// written back to z. Neighbours are read from z as it stands (Gauss-Seidel).
+__device__ void nms_pixel(const PcDims &d, const PcArgs &A, const PcPrior &P, int v, int j, int k, int max_iter,
+                          float threshold)
+{
+    const int R = d.R, C = d.C;
+    const size_t i = (size_t)v * d.N + (size_t)j * C + k;
+    NmsCtx c;
+    c.P = &P;
+    c.nu = d.nu;
+    const float2 b = csub(A.w[i], A.vdual[i]);
+    c.br = b.x;
+    c.bi = b.y;
+    c.flags = 0;
+    for (int a = 0; a < 9; a++) {
+        const int jj = j + a / 3 - 1, kk = k + a % 3 - 1;
+        c.nr[a] = c.ni[a] = 0.f;
+        if (jj >= 0 && jj < R && kk >= 0 && kk < C) {
+            const size_t n = (size_t)v * d.N + (size_t)jj * C + kk;
+            c.nr[a] = A.zr[n];
+            c.ni[a] = A.zi[n];
+            if (a != 4) c.flags |= 1u << a;  // the centre's weight is zero
+        }
+    }
+    const float z0r = c.nr[4], z0i = c.ni[4];
+    float pr[3] = {z0r, 2 * z0r, z0r}, pi[3] = {z0i, z0i, 2 * z0i};
+    float cc[3] = {nms_cost(c, pr[0], pi[0]), nms_cost(c, pr[1], pi[1]), nms_cost(c, pr[2], pi[2])};
+    auto swap_pts = [&](int a2, int b2) {
+        float t = pr[a2]; pr[a2] = pr[b2]; pr[b2] = t;
+        t = pi[a2]; pi[a2] = pi[b2]; pi[b2] = t;
+        t = cc[a2]; cc[a2] = cc[b2]; cc[b2] = t;
+    };
+    auto sort3 = [&]() {
+        if (cc[2] < cc[1]) swap_pts(1, 2);
+        if (cc[1] < cc[0]) swap_pts(0, 1);
+        if (cc[2] < cc[1]) swap_pts(1, 2);
+    };
+    auto accept = [&](float ar, float ai, float ac) {
+        pr[2] = ar; pi[2] = ai; cc[2] = ac;
+        if (cc[2] < cc[1]) swap_pts(1, 2);
+        if (cc[1] < cc[0]) swap_pts(0, 1);
+    };
+    auto shrink = [&]() {
+        for (int q = 1; q < 3; q++) {
+            pr[q] = pr[0] + 0.5f * (pr[q] - pr[0]);
+            pi[q] = pi[0] + 0.5f * (pi[q] - pi[0]);
+            cc[q] = nms_cost(c, pr[q], pi[q]);
+        }
+        sort3();
+    };
+    sort3();
+    float cr0 = (pr[0] + pr[1]) / 2.0f, ci0 = (pi[0] + pi[1]) / 2.0f;
+    for (int it = 0; it < max_iter; it++) {
+        const float o_r[4] = {cr0, pr[0], pr[1], pr[2]}, o_i[4] = {ci0, pi[0], pi[1], pi[2]};
+        const float rr = cr0 + (cr0 - pr[2]), ri = ci0 + (ci0 - pi[2]);
+        const float crf = nms_cost(c, rr, ri);
+        if (crf < cc[1] && crf >= cc[0]) {
+            accept(rr, ri, crf);
+        } else if (crf < cc[0]) {
+            const float er = cr0 + 2.0f * (rr - cr0), ei = ci0 + 2.0f * (ri - ci0);
+            const float ce = nms_cost(c, er, ei);
+            if (ce < crf) accept(er, ei, ce);
+            else accept(rr, ri, crf);
+        } else if (crf >= cc[1] && crf < cc[2]) {
+            const float orr = cr0 + 0.5f * (rr - cr0), oi = ci0 + 0.5f * (ri - ci0);
+            const float co = nms_cost(c, orr, oi);
+            if (co <= crf) accept(orr, oi, co);
+            else shrink();
+        } else if (crf >= cc[2]) {
+            const float ir = cr0 - 0.5f * (cr0 - pr[2]), ii = ci0 - 0.5f * (ci0 - pi[2]);
+            const float ci = nms_cost(c, ir, ii);
+            if (ci < cc[2]) accept(ir, ii, ci);
+            else shrink();
+        }
+        cr0 = (pr[0] + pr[1]) / 2.0f;
+        ci0 = (pi[0] + pi[1]) / 2.0f;
+        const float n_r[4] = {cr0, pr[0], pr[1], pr[2]}, n_i[4] = {ci0, pi[0], pi[1], pi[2]};
+        float num = 0.f, den = 0.f;
+        for (int q = 0; q < 4; q++) {
+            num += fabsf(o_r[q] - n_r[q]) + fabsf(o_i[q] - n_i[q]);
+            den += fabsf(o_r[q]) + fabsf(o_i[q]);
+        }
+        if (num / den * 100.0f < threshold && it > 1) break;
+    }
+    A.zr[i] = pr[0];
+    A.zi[i] = pi[0];
+}
+}  // namespace
+
+// Colour-class sweep: pixels of one (row parity, column parity) class
+// together -- no two 8-neighbours share a class -- over four launches.
+__global__ void pc_nms(PcDims d, PcArgs A, const __grid_constant__ PcPrior P, int color, int max_iter,
+                       float threshold)
+{
+    const int v = blockIdx.y;
+    if (A.active && !A.active[v]) return;
+    const int cj = color >> 1, ck = color & 1;
+    const int hr = (d.R - cj + 1) / 2, hc = (d.C - ck + 1) / 2;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < hr * hc; e += gridDim.x * blockDim.x)
+        nms_pixel(d, A, P, v, 2 * (e / hc) + cj, 2 * (e % hc) + ck, max_iter, threshold);
+}
+
+// The reference's raster order, exactly: pixel (j, k) reads the updated
+// (j-1, k-1..k+1) and (j, k-1) and the not yet updated (j, k+1) and row j+1,
+// so every pixel of the anti-diagonal 2j + k = t depends only on pixels of
+// smaller t and none of larger t reads it first. One CTA per view walks the
+// 2(R-1) + C wavefronts with a block barrier between them (global-memory
+// writes of the block are visible to it after the barrier).
+__global__ void pc_nms_wavefront(PcDims d, PcArgs A, const __grid_constant__ PcPrior P, int max_iter,
+                                 float threshold)
+{
+    const int v = blockIdx.x;
+    if (A.active && !A.active[v]) return;
+    const int R = d.R, C = d.C;
+    const int T = 2 * (R - 1) + C;
+    for (int t = 0; t < T; t++) {
+        const int j_lo = t >= C ? (t - C + 2) / 2 : 0;  // smallest j with t - 2j <= C - 1
+        const int j_hi = min(R - 1, t / 2);
+        for (int j = j_lo + (int)threadIdx.x; j <= j_hi; j += blockDim.x)
+            nms_pixel(d, A, P, v, j, t - 2 * j, max_iter, threshold);
+        __syncthreads();
+    }
+}
+
+}  // namespace mbirgpu

@@ -28,6 +28,9 @@ EXPORTS = (
     "mbirgpu_session_cost", "mbirgpu_session_icd_iteration", "mbirgpu_session_forward_project",
     "mbirgpu_session_back_project", "mbirgpu_session_get_amatrix", "mbirgpu_session_get_detector_response",
     "mbirgpu_session_run",
+    "phcontomo_reconstruct", "mbirgpu_pc_default_options", "mbirgpu_pc_session_create", "mbirgpu_pc_session_destroy",
+    "mbirgpu_pc_fresnel", "mbirgpu_pc_paganin", "mbirgpu_pc_set_z", "mbirgpu_pc_init_admm", "mbirgpu_pc_set_state",
+    "mbirgpu_pc_get_state", "mbirgpu_pc_sd_step", "mbirgpu_pc_nms_sweep", "mbirgpu_pc_run",
 )
 
 

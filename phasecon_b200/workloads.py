@@ -9,6 +9,11 @@ detector, Poisson counts at I0 = 2e4, spatial + temporal qGGMRF with p = 1.2.
 I0 = 1e4, p = 1.1). Measurements are y = -log(N/I0), w = N, N ~ Poisson(I0
 e^{-Ax}) with A the reference's own system matrix (applied by the GPU forward
 projector, whose parity with the reference is tested).
+``config_pc`` is the phase-contrast scan: 40 random spheres (radius 5-40 um,
+refractive decrement delta in [1e-7, 5e-7], beta = delta / 100) in a 256 um
+cube at 1 um, 180 parallel-beam views over 180 deg on a 256x256 detector at
+20 keV, Fresnel propagation over 50 mm, intensities with Gaussian noise at a
+per-pixel SNR of 100.
 """
 from __future__ import annotations
 
@@ -47,3 +52,38 @@ def config_3d(seed: int = 0, n_xy: int = 128, n_z: int = 16, views: int = 180):
     pb = Problem(zeros, np.ones_like(zeros), angles, times, recon_times, n_z, n_xy, views, 1, vox_wid=1.0,
                  rot_center=n_xy / 2, sig_s=0.01, sig_t=1.0, c_s=1.0, c_t=1.0, convg_thresh=0.0)
     return _measure(pb, obj, 1e4, seed), obj, 1.1
+
+
+def config_pc(seed: int = 0, n: int = 256, views: int = 180, spheres: int = 40, energy_kev: float = 20.0,
+              distance_um: float = 5e4, snr: float = 100.0):
+    """Phase-contrast scan of random spheres. Returns (PcProblem, (zr, zi)
+    true [views][n][n] in the session layout [view][N_r][N_t])."""
+    from .pcmbir import PcProblem
+    rng = np.random.default_rng(seed)
+    lam = 4.135668e-19 * 299792458e+6 / energy_kev  # um
+    k = 2 * np.pi / lam
+    rad = rng.uniform(5.0, 40.0, spheres)
+    ctr = rng.uniform(-n / 2 + rad[:, None], n / 2 - rad[:, None], (spheres, 3))
+    delta = rng.uniform(1e-7, 5e-7, spheres)
+    beta = delta / 100.0
+    coords = np.arange(n) - n / 2 + 0.5
+    theta = np.arange(views) * np.pi / views
+    zr = np.zeros((views, n, n))
+    zi = np.zeros((views, n, n))
+    tt = coords[None, :]
+    for s in range(spheres):
+        r0 = ctr[s, 0] * np.cos(theta) + ctr[s, 1] * np.sin(theta)  # [views]
+        d2 = (coords[None, :, None] - r0[:, None, None]) ** 2 + (tt[:, None, :] * 0 + (coords[None, None, :] - ctr[s, 2]) ** 2)
+        th = 2 * np.sqrt(np.maximum(rad[s] ** 2 - d2, 0.0))
+        zr += k * beta[s] * th
+        zi += k * delta[s] * th
+    u = np.fft.fftfreq(n, 1.0)
+    H = np.exp(-1j * np.pi * lam * distance_um * (u[:, None] ** 2 + u[None, :] ** 2))
+    bright = np.full((n, n), 1.0e4, np.float32)
+    w = np.exp(-zr) * np.exp(-1j * zi)
+    inten = np.abs(np.fft.ifft2(np.fft.fft2(w, axes=(1, 2)) * H, axes=(1, 2))) ** 2 * 1.0e4
+    inten = inten + rng.normal(size=inten.shape) * inten / snr
+    meas = np.ascontiguousarray(np.maximum(inten, 1e-3).transpose(0, 2, 1), np.float32)
+    pb = PcProblem(measurements=meas, brights=bright, vox_wid=1.0, mag_sig_s=0.05, mag_c_s=1.0, phase_sig_s=0.05,
+                   phase_c_s=1.0, obj2det_dist=distance_um, light_energy=energy_kev, pag_regparam=100.0)
+    return pb, (zr, zi)
