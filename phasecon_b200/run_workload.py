@@ -1,13 +1,16 @@
-"""Run a few ICD iterations of a synthetic workload (for profiling and quick checks).
+"""Run a few iterations of a synthetic workload (for profiling and quick checks).
 
     python -m phasecon_b200.run_workload [--workload 4d|3d] [--iters N] [--sv S] [--warps W]
                                          [--refresh] [--cost] [--ch-steps K]
+    python -m phasecon_b200.run_workload --workload pc [--iters N] [--views V] [--nms-order 0|1]
 
-Builds the seeded workload (phasecon_b200/workloads.py), creates one session
-with the given schedule (autotuned when --sv/--warps are 0) and runs N ICD
+Builds the seeded workload (phasecon_b200/workloads.py). For 4d / 3d: one
+session with the given schedule (autotuned when --sv/--warps are 0), N ICD
 iterations from zero, then optionally one FP64 error-sinogram refresh and one
-FP64 cost evaluation. --ch-steps shortens the phantom simulation (same array
-sizes) to keep the number of unrelated kernel launches small under a profiler.
+FP64 cost evaluation; --ch-steps shortens the phantom simulation (same array
+sizes) to keep the number of unrelated kernel launches small under a
+profiler. For pc: the phase-contrast scan, Paganin retrieval, the ADMM start
+and N phase-retrieval iterations of every view.
 """
 from __future__ import annotations
 
@@ -20,7 +23,9 @@ from . import workloads as W
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("--workload", default="4d", choices=["4d", "3d"])
+    ap.add_argument("--workload", default="4d", choices=["4d", "3d", "pc"])
+    ap.add_argument("--views", type=int, default=180)
+    ap.add_argument("--nms-order", type=int, default=0)
     ap.add_argument("--iters", type=int, default=2)
     ap.add_argument("--sv", type=int, default=0)
     ap.add_argument("--warps", type=int, default=0)
@@ -28,6 +33,8 @@ def main(argv=None):
     ap.add_argument("--cost", action="store_true")
     ap.add_argument("--ch-steps", type=int, default=5000)
     a = ap.parse_args(argv)
+    if a.workload == "pc":
+        return run_pc(a)
     if a.workload == "4d":
         pb, _, p = W.config_4d(ch_steps=a.ch_steps)
     else:
@@ -43,6 +50,19 @@ def main(argv=None):
     c = s.cost() if a.cost else None
     print(f"workload {a.workload}: sv {s.info.sv_size} warps {s.info.cta_warps} iters {a.iters} "
           f"updates/iter {st.voxel_updates} wall {time.perf_counter() - t0:.3f}s cost {c}")
+
+
+def run_pc(a):
+    from .pcmbir import PcSession, default_options
+    pb, _ = W.config_pc(views=a.views)
+    s = PcSession(pb, default_options(pret_max_iter=a.iters, nms_order=a.nms_order))
+    s.paganin()
+    s.init_admm()
+    t0 = time.perf_counter()
+    costs, iters, st = s.run()
+    print(f"workload pc: views {a.views} iters {a.iters} sd_steps {st.sd_steps} transforms "
+          f"{st.fresnel_transforms} device {st.kernel_ms:.1f} ms wall {time.perf_counter() - t0:.3f}s "
+          f"cost[0] {costs[0, :a.iters + 1]}")
 
 
 if __name__ == "__main__":
