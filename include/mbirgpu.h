@@ -154,6 +154,19 @@ int mbirgpu_session_icd_iteration(mbirgpu_session *s, int32_t iter, mbirgpu_iter
 int mbirgpu_session_forward_project(mbirgpu_session *s, const float *object, float *sino);
 int mbirgpu_session_back_project(mbirgpu_session *s, const float *sino, float *object);
 
+/* No counterpart in the reference. The forward projection of
+ * mbirgpu_session_forward_project for callers that may not allocate device
+ * memory (a framework allocator or a fixed budget owns it; cudaMalloc would
+ * synchronise a latency-critical loop): object_dev [N_time][N_z][N_y][N_x]
+ * and sino_dev [N_p][N_r][N_t] are device pointers, and the FP64 scratch is
+ * a fixed 16 MiB array in the library (N_p * N_r * N_t <= 2,097,152, larger
+ * sessions are rejected). Enqueued on the session's stream, not waited for.
+ * Make the first call on each device before any stream capture (it looks the
+ * scratch up). The call clears the scratch it uses itself. The scratch is
+ * shared by every call on a device: calls in flight at the same time on one
+ * device race, so order them. */
+int mbirgpu_session_forward_project_noalloc(mbirgpu_session *s, const float *object_dev, float *sino_dev);
+
 /* The device A-matrix table, for inspection: per (frame view, voxel column)
  * the first detector channel, the count and kmax FP32 values.
  * first/count: [N_p][N_y][N_x]; values: [N_p][N_y][N_x][kmax]. */

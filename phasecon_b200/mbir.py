@@ -27,7 +27,7 @@ EXPORTS = (
     "mbirgpu_session_object_device", "mbirgpu_session_refresh_error", "mbirgpu_session_get_error",
     "mbirgpu_session_cost", "mbirgpu_session_icd_iteration", "mbirgpu_session_forward_project",
     "mbirgpu_session_back_project", "mbirgpu_session_get_amatrix", "mbirgpu_session_get_detector_response",
-    "mbirgpu_session_run",
+    "mbirgpu_session_run", "mbirgpu_session_forward_project_noalloc",
     "phcontomo_reconstruct", "mbirgpu_pc_default_options", "mbirgpu_pc_session_create", "mbirgpu_pc_session_destroy",
     "mbirgpu_pc_fresnel", "mbirgpu_pc_paganin", "mbirgpu_pc_set_z", "mbirgpu_pc_init_admm", "mbirgpu_pc_set_state",
     "mbirgpu_pc_get_state", "mbirgpu_pc_sd_step", "mbirgpu_pc_nms_sweep", "mbirgpu_pc_run",
@@ -111,6 +111,7 @@ def lib() -> C.CDLL:
         L.mbirgpu_session_icd_iteration.argtypes = [C.c_void_p, C.c_int32, C.POINTER(IterStats)]
         L.mbirgpu_session_forward_project.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         L.mbirgpu_session_back_project.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.mbirgpu_session_forward_project_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         L.mbirgpu_session_get_amatrix.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.mbirgpu_session_get_detector_response.argtypes = [C.c_void_p, C.c_void_p]
         L.mbirgpu_session_run.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.POINTER(C.c_int32),
@@ -295,6 +296,12 @@ class Session:
         out = np.zeros(self.sino_shape, np.float32)
         _check(lib().mbirgpu_session_forward_project(self.h, a.ctypes.data, out.ctypes.data))
         return out
+
+    def forward_project_noalloc(self, object_dev: int, sino_dev: int) -> None:
+        """A x from a device object [N_time][N_z][N_y][N_x] into a device
+        sinogram [N_p][N_r][N_t] (raw device addresses), allocating nothing;
+        enqueued on the session's stream, not waited for."""
+        _check(lib().mbirgpu_session_forward_project_noalloc(self.h, C.c_void_p(object_dev), C.c_void_p(sino_dev)))
 
     def back_project(self, sino: np.ndarray) -> np.ndarray:
         a = np.ascontiguousarray(sino, np.float32).reshape(self.sino_shape)
