@@ -56,6 +56,8 @@ def parse():
     ap.add_argument("--no-converge", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--max-converge-iters", type=int, default=400)
+    ap.add_argument("--workload", default="4d", choices=["4d", "batch"],
+                    help="4d: the 4-D benchmark (default); batch: 48 uneven 3-D problems, batched vs sequential")
     return ap.parse_args()
 
 
@@ -278,19 +280,24 @@ def run_ours(args, world, rank, local, pg):
     total_updates = sum_over_ranks(pg, float(updates))
     value = total_updates / (ms_max / 1e3)
 
-    # roofline of the ICD sweep kernel (4 launches per iteration)
-    n_launch = 4 * args.steps
+    # roofline of the ICD sweep kernel: every ICD launch of the timed iterations
+    # (K^2 colour phases of the full sweep + K^2 per non-homogeneous pass from
+    # iteration 2), algorithmic bytes 12 nnz_v + 8 per voxel update
+    nh = opt.nhicd_passes
+    phases = info.sv_colors ** 2
+    icd_launches = sum(phases * (1 + (nh if it > 1 else 0))
+                       for it in range(args.warmup + 1, args.warmup + args.steps + 1))
     entries = info.nnz * info.N_t  # (e, w) entries one full sweep reads: nnz_v summed over voxel slices
-    upd_per_iter = updates / args.steps
     full = info.masked_columns * info.N_z
-    bytes_iter = (12.0 * entries + 8.0 * full) * (upd_per_iter / full if full else 1.0)
-    bytes_launch = bytes_iter / 4
-    avg_launch_s = kernel_ms / n_launch / 1e3
+    bytes_per_update = (12.0 * entries + 8.0 * full) / full
+    bytes_total = bytes_per_update * updates
+    avg_launch_s = kernel_ms / icd_launches / 1e3
     peak, peak_kind = measured_peaks()
-    achieved = bytes_launch / avg_launch_s / 1e9
+    achieved = bytes_total / (kernel_ms / 1e3) / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": profiled_traffic(), "peak_source": peak_kind, "kernel": "icd_phase_kernel",
-                "algorithmic_bytes_per_launch": bytes_launch, "avg_launch_ms": avg_launch_s * 1e3}
+                "algorithmic_bytes_per_launch": bytes_total / icd_launches, "avg_launch_ms": avg_launch_s * 1e3,
+                "bytes_per_voxel_update": bytes_per_update, "icd_launches": icd_launches}
 
     # time to converged cost from zero (plain GPU ICD), FP64 cost every iteration
     conv = {}
@@ -371,7 +378,9 @@ def run_ours(args, world, rank, local, pg):
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                 "config": {"workload": WORKLOAD, "voxels": [info.N_time, info.N_z, info.N_y, info.N_x],
                            "views": info.N_p, "detector": [info.N_t, info.N_r], "sv_size": info.sv_size,
-                           "cta_warps": info.cta_warps, "parallelism": f"replicas{world}",
+                           "cta_warps": info.cta_warps, "sv_colors": info.sv_colors,
+                           "nhicd_passes": opt.nhicd_passes,
+                           "parallelism": f"replicas{world}",
                            "l2": "inputs larger than L2: A table %.2f GB, y/w/e %.0f MB, x %.0f MB" % (
                                info.device_bytes / 1e9, 3 * info.N_p * info.N_r * info.N_t * 4 / 1e6,
                                info.N_time * info.N_z * info.N_y * info.N_x * 4 / 1e6)},
@@ -381,12 +390,76 @@ def run_ours(args, world, rank, local, pg):
         print(json.dumps(line))
 
 
+def run_batch(args, world, rank, local, pg):
+    """48 independent uneven 3-D problems: K iterations of the batched persistent
+    launch (CUDA graph per iteration) against K iterations of each problem in
+    its own session, one after another; plain SV-ICD in both (no NH passes)."""
+    import torch
+
+    import phasecon_b200 as pc
+    from phasecon_b200 import workloads as W
+
+    torch.cuda.set_device(local)
+    probs = W.config_batch(seed=rank)
+    opt = pc.get_options()
+    opt.nhicd_passes = 0
+    # batched: creation (H2D, A tables, autotune, graph capture), warm-up, timed run
+    t0 = time.perf_counter()
+    b = pc.Batch(probs, options=opt)
+    t_create = time.perf_counter() - t0
+    b.run(args.warmup)
+    before = b.run(0).voxel_updates
+    with ClockSampler(local) as clk:
+        st = b.run(args.steps)
+    upd = st.voxel_updates - before
+    ms = max_over_ranks(pg, st.device_ms)
+    value = sum_over_ranks(pg, float(upd)) / (ms / 1e3)
+    costs = [b.cost(i) for i in range(len(probs))]
+    b.close()
+    # sequential: each problem alone (its own autotuned session), same iterations
+    seq_ms, seq_upd = 0.0, 0
+    for p in probs:
+        s = pc.Session(p, options=opt)
+        s.set_timing(True)
+        for it in range(1, args.warmup + 1):
+            s.icd_iteration(it)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for it in range(args.warmup + 1, args.warmup + args.steps + 1):
+            seq_upd += s.icd_iteration(it).voxel_updates
+        e1.record()
+        torch.cuda.synchronize()
+        seq_ms += e0.elapsed_time(e1)
+        s.close()
+    seq_value = sum_over_ranks(pg, float(seq_upd)) / (max_over_ranks(pg, seq_ms) / 1e3)
+    if rank == 0:
+        print(json.dumps({
+            "metric": "aggregate voxel-updates/s, batched persistent launch vs sequential per-problem solves",
+            "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "batch_48_uneven_3d", "problems": len(probs),
+                       "edges": sorted({p.proj_cols for p in probs}), "depths": [min(p.proj_rows for p in probs),
+                                                                                 max(p.proj_rows for p in probs)],
+                       "views": [min(p.proj_num for p in probs), max(p.proj_num for p in probs)],
+                       "sv_size": st.sv_size, "cta_warps": st.cta_warps, "sv_colors": st.sv_colors,
+                       "kernel_launches_per_iteration": st.kernel_launches_per_iteration,
+                       "graph_launches": st.graph_launches, "parallelism": f"replicas{world}"},
+            "sequential": {"value": seq_value, "unit": UNIT, "ms_per_step": seq_ms / args.steps},
+            "speedup_vs_sequential": value / seq_value if seq_value else None,
+            "batch_create_s": t_create, "mean_final_cost": float(np.mean(costs)),
+            "clocks": clk.summary()}))
+
+
 def main():
     args = parse()
     world, rank, local, pg = dist_setup()
     try:
         if args.impl == "reference":
             run_reference_arm(args, rank)
+        elif args.workload == "batch":
+            run_batch(args, world, rank, local, pg)
         else:
             run_ours(args, world, rank, local, pg)
     finally:

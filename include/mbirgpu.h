@@ -61,6 +61,15 @@ typedef struct {
     int32_t icd_unroll;      /* views whose A records and sinogram entries one lane keeps in flight
                                 (1, 2 or 4); 0 = autotuned */
     uint64_t seed;           /* voxel-order seed */
+    int32_t nhicd_passes;    /* non-homogeneous ICD (XT_ICD_update.c:1007-1047, XT_NHICD.c:164-216):
+                                from iteration 2, after the full sweep, n passes each re-update the
+                                voxel columns with the largest 5x5-Hamming-filtered update magnitude
+                                (1/NHICD_Iterations of the masked columns per frame, as the
+                                reference); 0 = off, up to 16. Default 10 (the reference's
+                                NHICD_Iterations, XT_Init.c:406; NO_NHICD is 0) */
+    int32_t sv_colors;       /* super-voxel colouring: K x K colour classes, K = 2 (4 phases per
+                                sweep) or 4 (16 phases: same-colour super-voxels twice as far
+                                apart); 0 = autotuned */
 } mbirgpu_options;
 
 /* Defaults as listed above. */
@@ -105,6 +114,7 @@ typedef struct {
                                 summed over frames; one voxel slice reads nnz*z_overlap entries */
     double delta_t;
     size_t device_bytes;     /* device memory the session holds */
+    int32_t sv_colors;       /* K of the K x K super-voxel colouring in use */
 } mbirgpu_session_info;
 
 typedef struct {
@@ -154,6 +164,14 @@ int mbirgpu_session_icd_iteration(mbirgpu_session *s, int32_t iter, mbirgpu_iter
 int mbirgpu_session_forward_project(mbirgpu_session *s, const float *object, float *sino);
 int mbirgpu_session_back_project(mbirgpu_session *s, const float *sino, float *object);
 
+/* The NH-ICD voxel-line selection for a given update-magnitude map (for
+ * inspection): mag [N_time][N_y][N_x] (sum over z of |update| of each voxel
+ * column's latest visit, MagUpdateMap), sel [N_time][N_y][N_x] receives 1
+ * for the columns an NH pass would visit -- the masked columns among the
+ * masked/NHICD_Iterations largest 5x5-Hamming-filtered values of the frame
+ * (VSC_based_Voxel_Line_Select, MBIR_4D/XT_NHICD.c:164-216). */
+int mbirgpu_session_nh_select(mbirgpu_session *s, const float *mag, uint8_t *sel);
+
 /* No counterpart in the reference. The forward projection of
  * mbirgpu_session_forward_project for callers that may not allocate device
  * memory (a framework allocator or a fixed budget owns it; cudaMalloc would
@@ -182,6 +200,46 @@ int mbirgpu_session_get_detector_response(mbirgpu_session *s, float *H_r);
  * iteration count in *iters. */
 int mbirgpu_session_run(mbirgpu_session *s, int32_t max_iter, double *costs, int32_t *iters,
                         mbirgpu_iter_stats *total);
+
+/* --------------------------------------------------------------------------
+ * Batched reconstruction of many independent problems (no counterpart in the
+ * reference, which solves one problem per process).
+ *
+ * All problems stay resident; one ICD iteration of all of them is one
+ * persistent launch per colour phase (and per detector-row class) whose CTAs
+ * drain a queue over every problem's super-voxels, captured once as a CUDA
+ * graph. Each problem is a single stage at voxel scale 1 (mult_xy = mult_z =
+ * 1, the finest stage of reconstruct()), starts from zero and stops on its own
+ * convergence test (100 sum|dx| / sum|x| < convg_thresh after the first
+ * iteration, MBIR_4D/XT_ICD_update.c:1083-1090). The super-voxel size and
+ * CTA width are autotuned for the whole batch unless fixed in the options.
+ * ------------------------------------------------------------------------ */
+typedef struct mbirgpu_batch mbirgpu_batch;
+
+typedef struct {
+    int64_t voxel_updates;     /* updates that ran in all problems since creation */
+    double device_ms;          /* device time of this run (CUDA events) */
+    int32_t graph_launches;    /* CUDA graph launches of this run (one per iteration) */
+    int32_t kernel_launches_per_iteration;
+    int32_t problems_converged;
+    int32_t sv_size, cta_warps, sv_colors;
+} mbirgpu_batch_stats;
+
+int mbirgpu_batch_create(mbirgpu_batch **out, const mbirgpu_problem *problems, int32_t n,
+                         const mbirgpu_options *opt, void *stream);
+int mbirgpu_batch_destroy(mbirgpu_batch *b);
+/* Run `iterations` more iterations of every problem that has not converged. */
+int mbirgpu_batch_run(mbirgpu_batch *b, int32_t iterations, mbirgpu_batch_stats *stats);
+int mbirgpu_batch_problem_info(mbirgpu_batch *b, int32_t i, mbirgpu_session_info *info, int32_t *iterations,
+                               int32_t *converged);
+/* Object of problem i, [N_time][N_z][N_y][N_x] without halo. */
+int mbirgpu_batch_get_object(mbirgpu_batch *b, int32_t i, float *object);
+/* FP64 MAP cost of problem i (MBIR_4D/XT_ICD_update.c:185-318). */
+int mbirgpu_batch_cost(mbirgpu_batch *b, int32_t i, double *total);
+/* Drop-in style: reconstruct n problems together with the current options,
+ * up to `iterations` iterations each; objects[i] receives a malloc'ed buffer in
+ * reconstruct()'s layout [recon_num][proj_rows+2][proj_cols][proj_cols]. */
+int mbirgpu_reconstruct_batch(float **objects, const mbirgpu_problem *problems, int32_t n, int32_t iterations);
 
 /* --------------------------------------------------------------------------
  * Phase-contrast tomography (PCMBIR_3D): per-view phase retrieval.

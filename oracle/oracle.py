@@ -160,6 +160,8 @@ def ref_lib() -> C.CDLL:
         lib.ref_functional_substitution.argtypes = [P, C.c_int32, _f64p, _f64p, _f64p, _f64p, _u8p, _f64p, _u8p,
                                                     _f64p]
         lib.ref_random2_sequence.argtypes = [C.c_uint32, C.c_int32, _f64p]
+        lib.ref_vsc_select.argtypes = [C.c_int32, C.c_int32, _f32p, C.c_int32, _u8p]
+        lib.ref_vsc_select.restype = C.c_int32
         lib.ref_reconstruct.argtypes = [P, C.c_int32, C.POINTER(C.POINTER(C.c_float))]
         lib.ref_reconstruct.restype = C.c_int
         lib.ref_free.argtypes = [C.c_void_p]
@@ -246,6 +248,45 @@ class Oracle:
                                                      np.ascontiguousarray(nflag, np.uint8),
                                                      np.ascontiguousarray(tnhood, np.float64),
                                                      np.ascontiguousarray(tflag, np.uint8))
+
+
+HAMMING_5X5 = np.array([[0.0064, 0.0432, 0.0800, 0.0432, 0.0064],
+                        [0.0432, 0.2916, 0.5400, 0.2916, 0.0432],
+                        [0.0800, 0.5400, 1.0000, 0.5400, 0.0800],
+                        [0.0432, 0.2916, 0.5400, 0.2916, 0.0432],
+                        [0.0064, 0.0432, 0.0800, 0.0432, 0.0064]])  # XT_NHICD.c:132-136
+NHICD_ITERATIONS = 10  # XT_Init.c:406
+
+
+def vsc_select(mag: np.ndarray, n_lines: int, nhicd_iterations: int = NHICD_ITERATIONS) -> np.ndarray:
+    """NH-ICD voxel-line selection of one frame / z block
+    (VSC_based_Voxel_Line_Select, XT_NHICD.c:164-216): the update-magnitude map
+    filtered by the 5x5 Hamming window in FP64 in the reference's (p, q) order,
+    stored as float (ComputeVSC, :128-161); threshold = the (N - k)-th smallest
+    filtered value, N = ny nx, k = floor(n_lines / NHICD_Iterations)
+    (RandomizedSelect's order statistic, :177-178); selected = filtered > threshold.
+    Returns a bool [ny][nx] map (unmasked lines included, as the reference)."""
+    mag = np.asarray(mag, np.float32)
+    ny, nx = mag.shape
+    acc = np.zeros((ny, nx), np.float64)
+    pad = np.zeros((ny + 4, nx + 4), np.float64)
+    pad[2:-2, 2:-2] = mag
+    for p in range(5):
+        for q in range(5):
+            acc = acc + HAMMING_5X5[p, q] * pad[p:p + ny, q:q + nx]
+    filt = acc.astype(np.float32)
+    k = n_lines // nhicd_iterations
+    N = ny * nx
+    thresh = np.sort(filt.ravel())[N - k - 1]
+    return filt > thresh
+
+
+def ref_vsc_select(mag: np.ndarray, n_lines: int) -> np.ndarray:
+    """The reference's own VSC_based_Voxel_Line_Select on one frame (oracle/_ref)."""
+    mag = np.ascontiguousarray(mag, np.float32)
+    out = np.zeros(mag.shape, np.uint8)
+    ref_lib().ref_vsc_select(mag.shape[0], mag.shape[1], mag, n_lines, out)
+    return out.astype(bool)
 
 
 def random2_sequence(seed: int, n: int) -> np.ndarray:

@@ -27,6 +27,7 @@
 #include "XT_ICD_update.h"
 #include "allocate.h"
 #include "randlib.h"
+#include "XT_NHICD.h"
 
 /* Globals read by the patched reference (see the sed recipe in the Makefile). */
 double oracle_ref_mrf_p = 1.2;
@@ -218,6 +219,46 @@ int ref_functional_substitution(const RefProblem *pb, int32_t n, const double *V
     }
     ref_fini(&st, 0);
     return 0;
+}
+
+/*
+ * The reference's NH-ICD voxel-line selection (VSC_based_Voxel_Line_Select,
+ * XT_NHICD.c:164-216) for one frame and one z block: mag is the update-
+ * magnitude map [ny][nx], n_lines the number of voxel lines of the block
+ * (UpdateSelectNum). sel[ny][nx] receives 1 for every selected line; the
+ * return value is the number selected. RandomizedSelect draws from random2,
+ * seeded here so the call is repeatable (its result does not depend on it).
+ */
+int32_t ref_vsc_select(int32_t ny, int32_t nx, const float *mag, int32_t n_lines, uint8_t *sel)
+{
+    ScannedObject O;
+    TomoInputs T;
+    int32_t i, n;
+    memset(&O, 0, sizeof(O));
+    memset(&T, 0, sizeof(T));
+    O.N_time = 1;
+    O.N_y = ny;
+    O.N_x = nx;
+    O.NHICD_Iterations = 10; /* XT_Init.c:406 */
+    T.num_z_blocks = 1;
+    T.UpdateSelectNum = (int32_t **)multialloc(sizeof(int32_t), 2, 1, 1);
+    T.NHICDSelectNum = (int32_t **)multialloc(sizeof(int32_t), 2, 1, 1);
+    T.x_NHICD_select = (int32_t ***)multialloc(sizeof(int32_t), 3, 1, 1, ny * nx);
+    T.y_NHICD_select = (int32_t ***)multialloc(sizeof(int32_t), 3, 1, 1, ny * nx);
+    Real_arr_t ****map = (Real_arr_t ****)multialloc(sizeof(Real_arr_t), 4, 1, 1, ny, nx);
+    for (i = 0; i < ny * nx; i++) (&map[0][0][0][0])[i] = mag[i];
+    T.UpdateSelectNum[0][0] = n_lines;
+    srandom2(761521);
+    VSC_based_Voxel_Line_Select(&O, &T, map);
+    n = T.NHICDSelectNum[0][0];
+    memset(sel, 0, (size_t)ny * nx);
+    for (i = 0; i < n; i++) sel[T.y_NHICD_select[0][0][i] * nx + T.x_NHICD_select[0][0][i]] = 1;
+    multifree(map, 4);
+    multifree(T.x_NHICD_select, 3);
+    multifree(T.y_NHICD_select, 3);
+    multifree(T.UpdateSelectNum, 2);
+    multifree(T.NHICDSelectNum, 2);
+    return n;
 }
 
 /* The reference's Park-Miller generator (randlib.c:119-172). */

@@ -6,17 +6,20 @@
 // (XT_ICD_update.c:133-182).
 //
 // Schedule. The image plane is tiled into super-voxels (SVs) of sv x sv voxel
-// columns; an SV's colour is (sv_y & 1, sv_x & 1). Phase p updates, in frame
-// f, the SVs of colour p ^ (f & 1): no two SVs updated at once share a prior
-// neighbour, and a voxel and its temporal neighbours (same column, frames
-// f +- 1) are never updated at once -- the GPU counterpart of the
-// reference's z-block / frame checkerboard (XT_ICD_update.c:964-1046). Frames
-// use disjoint views, so different frames never share sinogram entries;
-// concurrent SVs of one frame can share entries along a ray, and their error
-// sinogram updates are atomic adds.
+// columns; with K x K colours (K = 2 or 4) an SV's colour is
+// (sv_y mod K) K + (sv_x mod K). Phase p updates, in frame f, the SVs of
+// colour (p + f) mod K^2: no two SVs updated at once share a prior neighbour,
+// and a voxel and its temporal neighbours (same column, frames f +- 1) are
+// never updated at once -- the GPU counterpart of the reference's z-block /
+// frame checkerboard (XT_ICD_update.c:964-1046). Frames use disjoint views,
+// so different frames never share sinogram entries; concurrent SVs of one
+// frame can share entries along a ray, and their error sinogram updates are
+// atomic adds (how many may run at once is bounded by sv_max_concurrent).
 //
 // A grid of persistent CTAs (as many as fit on the GPU) drains a queue of the
-// phase's SVs; a CTA owns one SV at a time and visits its voxel columns one
+// phase's SVs, frames fastest and SV slots in a spread order (queue index x
+// perm mod slots), so the SVs in flight are far apart; a CTA owns one SV at a
+// time and visits its voxel columns one
 // after another in a seeded random order (the counterpart of
 // randomly_select_x_y, XT_ICD_update.c:499-531). For one column all warps
 // cooperate, with three CTA barriers per column:
@@ -43,14 +46,6 @@ namespace {
 
 constexpr int kMaxWarps = 8;
 constexpr int kMaxSvCols = 256;  // sv <= 16
-
-struct IcdConst {
-    float sf[27];
-    float tf;
-    float q, qmp, ssq, ssqp, stq, stqp, cs, ct, bs0, bt0, alpha, dt;
-    float huber_T, huber_delta;
-    int huber;
-};
 
 __device__ __forceinline__ uint64_t mix64(uint64_t z)
 {
@@ -124,30 +119,59 @@ __device__ __forceinline__ void red_add(float *p, const float (&d)[2])
     asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(p), "f"(d[0]), "f"(d[1]) : "memory");
 }
 
-}  // namespace
 
+struct IcdSmem {
+    float num[kMaxWarps][32], den[kMaxWarps][32];
+    float th1[kMaxWarps][32], th2[kMaxWarps][32];
+    int pos[kMaxWarps][32];
+    float dx[32];
+    int order[kMaxSvCols];
+    int ncols, item;
+};
+
+struct IcdCount {
+    unsigned long long upd, skip;
+    float sum_dx, sum_x;
+};
+
+// Warp 0 adds the CTA's counters to the problem's statistics and clears them.
+__device__ __forceinline__ void flush_counts(IcdCount &cnt, IcdStats *stats)
+{
+    if ((threadIdx.x >> 5) == 0) {
+        for (int off = 16; off > 0; off >>= 1) {
+            cnt.upd += __shfl_xor_sync(0xffffffffu, cnt.upd, off);
+            cnt.skip += __shfl_xor_sync(0xffffffffu, cnt.skip, off);
+            cnt.sum_dx += __shfl_xor_sync(0xffffffffu, cnt.sum_dx, off);
+            cnt.sum_x += __shfl_xor_sync(0xffffffffu, cnt.sum_x, off);
+        }
+        if ((threadIdx.x & 31) == 0 && (cnt.upd || cnt.skip)) {
+            atomicAdd(&stats->updates, cnt.upd);
+            atomicAdd(&stats->skipped, cnt.skip);
+            atomicAdd(&stats->sum_abs_dx, (double)cnt.sum_dx);
+            atomicAdd(&stats->sum_abs_x, (double)cnt.sum_x);
+        }
+    }
+    cnt = IcdCount{};
+}
+
+// Update the voxel columns of super-voxel (sx, sy) of frame f; the whole CTA
+// cooperates (see the file comment for the four passes per column).
 // KW: 16-byte words per A record (1, 2, 3 for voxel scale 1, 2, 4);
 // kUnroll: views whose records and sinogram entries are in flight together;
 // VEC: consecutive detector rows one lane owns (4 when N_t % 4 == 0, else 2).
 template <int KW, int kUnroll, int VEC>
-__global__ void __launch_bounds__(kMaxWarps * 32, 4) icd_phase_kernel(
-    Geom g, IcdLaunch L, IcdConst K, const uint32_t *__restrict__ table, const int32_t *__restrict__ view_first,
-    const uint8_t *__restrict__ mask, float *__restrict__ x, float *__restrict__ err, const float *__restrict__ wgt,
-    float *__restrict__ mag, IcdStats *__restrict__ stats, unsigned int *__restrict__ queue)
+__device__ __forceinline__ void icd_update_sv(const Geom &g, const IcdLaunch &L, const IcdConst &K,
+                                              const uint32_t *__restrict__ table,
+                                              const int32_t *__restrict__ view_first,
+                                              const uint8_t *__restrict__ mask, float *__restrict__ x,
+                                              float *__restrict__ err, const float *__restrict__ wgt,
+                                              float *__restrict__ mag, int f, int sx, int sy, IcdSmem &S,
+                                              IcdCount &cnt)
 {
-    __shared__ float s_num[kMaxWarps][32], s_den[kMaxWarps][32];
-    __shared__ float s_th1[kMaxWarps][32], s_th2[kMaxWarps][32];
-    __shared__ int s_pos[kMaxWarps][32];
-    __shared__ float s_dx[32];
-    __shared__ int s_order[kMaxSvCols];
-    __shared__ int s_ncols, s_item;
-
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, W = blockDim.x >> 5;
     const int NX = g.N_x, NY = g.N_y, NZ = g.N_z, NT = g.N_t, MZ = g.z_overlap;
     const int nxy = NX * NY;
     const int RW = g.rec_words;
-    const int half_x = (L.n_sv_x + 1) / 2, half_y = (L.n_sv_y + 1) / 2;
-    const int n_items = g.N_time * half_x * half_y;
 
     // lane -> (view group, run of VEC detector rows) for the theta / apply passes
     using VT = typename VecF<VEC>::T;
@@ -161,283 +185,265 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 4) icd_phase_kernel(
     const int gstride = W * G;
     const int gfirst = warp * G + grp;
     const bool zl = lane < NZ;
+    const int fv0 = view_first[f], nv = view_first[f + 1] - fv0;
 
-    unsigned long long n_upd = 0, n_skip = 0;
-    float sum_dx = 0.0f, sum_x = 0.0f;
-
-    // persistent CTA: take super-voxels of this phase's colour from the queue
-    for (;;) {
-        __syncthreads();  // s_item / s_order of the previous SV are no longer read
-        if (threadIdx.x == 0) s_item = (int)atomicAdd(queue, 1u);
-        __syncthreads();
-        const int item = s_item;
-        if (item >= n_items) break;
-        const int f = item / (half_x * half_y);
-        const int rem = item - f * half_x * half_y;
-        const int color = L.phase ^ (f & 1);
-        const int sx = 2 * (rem % half_x) + (color & 1);
-        const int sy = 2 * (rem / half_x) + (color >> 1);
-        if (sx >= L.n_sv_x || sy >= L.n_sv_y) continue;  // uniform
-        const int fv0 = view_first[f], nv = view_first[f + 1] - fv0;
-
-        // ---- the SV's columns inside the reconstruction circle, shuffled ----------
-        if (warp == 0) {
-            const int ncand = L.sv * L.sv;
-            int n = 0;
-            for (int base = 0; base < ncand; base += 32) {
-                const int i = base + lane;
-                int ok = 0, c = 0;
-                if (i < ncand) {
-                    const int j = sy * L.sv + i / L.sv, k = sx * L.sv + i % L.sv;
-                    if (j < NY && k < NX) {
-                        c = j * NX + k;
-                        ok = mask[c];
-                    }
+    // ---- the SV's columns inside the reconstruction circle, shuffled ----------
+    if (warp == 0) {
+        const int ncand = L.sv * L.sv;
+        int n = 0;
+        for (int base = 0; base < ncand; base += 32) {
+            const int i = base + lane;
+            int ok = 0, c = 0;
+            if (i < ncand) {
+                const int j = sy * L.sv + i / L.sv, k = sx * L.sv + i % L.sv;
+                if (j < NY && k < NX) {
+                    c = j * NX + k;
+                    ok = mask[c] && (!L.sel || L.sel[(size_t)f * nxy + c]);
                 }
-                const unsigned m = __ballot_sync(0xffffffffu, ok);
-                if (ok) s_order[n + __popc(m & ((1u << lane) - 1))] = c;
-                n += __popc(m);
             }
-            __syncwarp();
-            if (lane == 0) {
-                uint64_t h = mix64(L.seed ^ mix64(((uint64_t)L.iter << 40) ^ ((uint64_t)f << 20) ^
-                                                 (uint64_t)(sy * L.n_sv_x + sx)));
-                for (int i = n - 1; i > 0; i--) {  // Fisher-Yates
-                    h = mix64(h);
-                    const int r = (int)(h % (uint64_t)(i + 1));
-                    const int t = s_order[i];
-                    s_order[i] = s_order[r];
-                    s_order[r] = t;
-                }
-                s_ncols = n;
-            }
+            const unsigned m = __ballot_sync(0xffffffffu, ok);
+            if (ok) S.order[n + __popc(m & ((1u << lane) - 1))] = c;
+            n += __popc(m);
         }
-        __syncthreads();
-        const int ncols = s_ncols;
+        __syncwarp();
+        if (lane == 0) {
+            uint64_t h = mix64(L.seed ^ mix64(((uint64_t)L.iter << 40) ^ ((uint64_t)f << 20) ^
+                                             (uint64_t)(sy * L.n_sv_x + sx)));
+            for (int i = n - 1; i > 0; i--) {  // Fisher-Yates
+                h = mix64(h);
+                const int r = (int)(h % (uint64_t)(i + 1));
+                const int t = S.order[i];
+                S.order[i] = S.order[r];
+                S.order[r] = t;
+            }
+            S.ncols = n;
+        }
+    }
+    __syncthreads();
+    const int ncols = S.ncols;
 
-        for (int ci = 0; ci < ncols; ci++) {
-            const int c = s_order[ci];
-            const int j = c / NX, k = c - j * NX;
-            const size_t col_off = ((size_t)f * nxy + c) * NZ;
-            const uint32_t *col_rec = table + ((size_t)fv0 * nxy + (size_t)c * nv) * RW;
+    for (int ci = 0; ci < ncols; ci++) {
+        const int c = S.order[ci];
+        const int j = c / NX, k = c - j * NX;
+        const size_t col_off = ((size_t)f * nxy + c) * NZ;
+        const uint32_t *col_rec = table + ((size_t)fv0 * nxy + (size_t)c * nv) * RW;
 
-            // ---- 1. neighbourhood (sources split over warps) + column activity ------
-            int active_pred;
-            {
-                const float V = zl ? x[col_off + lane] : 0.0f;
-                float num = 0.0f, den = 0.0f;
-                int pos = 0;
-                for (int s = warp; s < 10; s += W) {
-                    if (s < 8) {
-                        const int o = s < 4 ? s : s + 1;  // skip the centre of the 3x3
-                        const int dy = o / 3 - 1, dx = o % 3 - 1;
-                        const int jj = j + dy, kk = k + dx;
-                        const bool valid = jj >= 0 && jj < NY && kk >= 0 && kk < NX;
-                        const float nz0 = (valid && zl) ? x[((size_t)f * nxy + jj * NX + kk) * NZ + lane] : 0.0f;
-                        const float nzm = __shfl_up_sync(0xffffffffu, nz0, 1);
-                        const float nzp = __shfl_down_sync(0xffffffffu, nz0, 1);
-                        if (valid && zl) {
-                            const float nb[3] = {nzm, nz0, nzp};
+        // ---- 1. neighbourhood (sources split over warps) + column activity ------
+        int active_pred;
+        {
+            const float V = zl ? x[col_off + lane] : 0.0f;
+            float num = 0.0f, den = 0.0f;
+            int pos = 0;
+            for (int s = warp; s < 10; s += W) {
+                if (s < 8) {
+                    const int o = s < 4 ? s : s + 1;  // skip the centre of the 3x3
+                    const int dy = o / 3 - 1, dx = o % 3 - 1;
+                    const int jj = j + dy, kk = k + dx;
+                    const bool valid = jj >= 0 && jj < NY && kk >= 0 && kk < NX;
+                    const float nz0 = (valid && zl) ? x[((size_t)f * nxy + jj * NX + kk) * NZ + lane] : 0.0f;
+                    const float nzm = __shfl_up_sync(0xffffffffu, nz0, 1);
+                    const float nzp = __shfl_down_sync(0xffffffffu, nz0, 1);
+                    if (valid && zl) {
+                        const float nb[3] = {nzm, nz0, nzp};
 #pragma unroll
-                            for (int dz = -1; dz <= 1; dz++) {
-                                const int zz = lane + dz;
-                                if (zz < 0 || zz >= NZ) continue;
-                                const float n = nb[dz + 1];
-                                const float b = qg_weight(V - n, K.q, K.qmp, K.ssq, K.ssqp, K.cs, K.bs0);
-                                const float cf = K.sf[(dz + 1) * 9 + (dy + 1) * 3 + (dx + 1)] * b;
-                                num += cf * n;
-                                den += cf;
-                                pos |= n > 0.0f;
-                            }
-                        }
-                    } else {
-                        const int ff = f + (s == 8 ? -1 : 1);
-                        if (ff >= 0 && ff < g.N_time && zl) {
-                            const float n = x[((size_t)ff * nxy + c) * NZ + lane];
-                            const float b = qg_weight(V - n, K.q, K.qmp, K.stq, K.stqp, K.ct, K.bt0);
-                            const float cf = K.tf * b;
+                        for (int dz = -1; dz <= 1; dz++) {
+                            const int zz = lane + dz;
+                            if (zz < 0 || zz >= NZ) continue;
+                            const float n = nb[dz + 1];
+                            const float b = qg_weight(V - n, K.q, K.qmp, K.ssq, K.ssqp, K.cs, K.bs0);
+                            const float cf = K.sf[(dz + 1) * 9 + (dy + 1) * 3 + (dx + 1)] * b;
                             num += cf * n;
                             den += cf;
                             pos |= n > 0.0f;
                         }
                     }
+                } else {
+                    const int ff = f + (s == 8 ? -1 : 1);
+                    if (ff >= 0 && ff < g.N_time && zl) {
+                        const float n = x[((size_t)ff * nxy + c) * NZ + lane];
+                        const float b = qg_weight(V - n, K.q, K.qmp, K.stq, K.stqp, K.ct, K.bt0);
+                        const float cf = K.tf * b;
+                        num += cf * n;
+                        den += cf;
+                        pos |= n > 0.0f;
+                    }
                 }
-                s_num[warp][lane] = num;
-                s_den[warp][lane] = den;
-                s_pos[warp][lane] = pos;
-                // a column is skipped only if every slice is zero with no positive
-                // neighbour (in-column neighbours are the column's own values)
-                active_pred = !L.zero_skipping || L.iter <= 1 || (zl && V != 0.0f) || pos;
             }
-            if (!__syncthreads_or(active_pred)) {
-                if (warp == 0 && zl) n_skip++;
-                if (warp == 0 && lane == 0) mag[(size_t)f * nxy + c] = 0.0f;
-                continue;  // uniform across the CTA
-            }
+            S.num[warp][lane] = num;
+            S.den[warp][lane] = den;
+            S.pos[warp][lane] = pos;
+            // a column is skipped only if every slice is zero with no positive
+            // neighbour (in-column neighbours are the column's own values)
+            active_pred = !L.zero_skipping || L.iter <= 1 || (zl && V != 0.0f) || pos;
+        }
+        if (!__syncthreads_or(active_pred)) {
+            if (warp == 0 && zl) cnt.skip++;
+            if (warp == 0 && lane == 0) mag[(size_t)f * nxy + c] = 0.0f;
+            continue;  // uniform across the CTA
+        }
 
-            // ---- 2. theta over the column's views -----------------------------------
-            {
-                float th1[VEC], th2[VEC];
+        // ---- 2. theta over the column's views -----------------------------------
+        {
+            float th1[VEC], th2[VEC];
 #pragma unroll
-                for (int i = 0; i < VEC; i++) th1[i] = th2[i] = 0.0f;
-                if (row_ok) {
-                    for (int v0 = gfirst; v0 < nv; v0 += kUnroll * gstride) {
-                        Rec<KW> R[kUnroll];
+            for (int i = 0; i < VEC; i++) th1[i] = th2[i] = 0.0f;
+            if (row_ok) {
+                for (int v0 = gfirst; v0 < nv; v0 += kUnroll * gstride) {
+                    Rec<KW> R[kUnroll];
 #pragma unroll
-                        for (int u = 0; u < kUnroll; u++) {
-                            const int v = v0 + u * gstride;
-                            if (v < nv) R[u] = load_rec<KW>(col_rec + (size_t)v * RW);
-                            else R[u].w[0].x = 0u;
-                        }
+                    for (int u = 0; u < kUnroll; u++) {
+                        const int v = v0 + u * gstride;
+                        if (v < nv) R[u] = load_rec<KW>(col_rec + (size_t)v * RW);
+                        else R[u].w[0].x = 0u;
+                    }
 #pragma unroll
-                        for (int u = 0; u < kUnroll; u++) {
-                            const uint32_t hdr = R[u].w[0].x;
-                            const int cnt = hdr >> 24;
-                            const size_t sb = (size_t)(hdr & 0xFFFFFF) * NT + t0;
+                    for (int u = 0; u < kUnroll; u++) {
+                        const uint32_t hdr = R[u].w[0].x;
+                        const int cnt_q = hdr >> 24;
+                        const size_t sb = (size_t)(hdr & 0xFFFFFF) * NT + t0;
 #pragma unroll
-                            for (int q = 0; q < 4 * KW - 1; q++) {
-                                if (q < cnt) {
-                                    float ev[VEC], wv[VEC];
-                                    VecF<VEC>::get(__ldcg(reinterpret_cast<const VT *>(err + sb + (size_t)q * NT)), ev);
-                                    VecF<VEC>::get(__ldg(reinterpret_cast<const VT *>(wgt + sb + (size_t)q * NT)), wv);
-                                    const float a = rec_val<KW>(R[u], q) * K.dt;
+                        for (int q = 0; q < 4 * KW - 1; q++) {
+                            if (q < cnt_q) {
+                                float ev[VEC], wv[VEC];
+                                VecF<VEC>::get(__ldcg(reinterpret_cast<const VT *>(err + sb + (size_t)q * NT)), ev);
+                                VecF<VEC>::get(__ldg(reinterpret_cast<const VT *>(wgt + sb + (size_t)q * NT)), wv);
+                                const float a = rec_val<KW>(R[u], q) * K.dt;
 #pragma unroll
-                                    for (int i = 0; i < VEC; i++) {
-                                        float ww = wv[i];
-                                        if (K.huber) {
-                                            const float sw = sqrtf(ww);
-                                            if (!(fabsf(ev[i] * sw) < K.huber_T)) ww = K.huber_T * K.huber_delta * sw / fabsf(ev[i]);
-                                        }
-                                        const float aw = a * ww;
-                                        th2[i] += a * aw;
-                                        th1[i] -= ev[i] * aw;
+                                for (int i = 0; i < VEC; i++) {
+                                    float ww = wv[i];
+                                    if (K.huber) {
+                                        const float sw = sqrtf(ww);
+                                        if (!(fabsf(ev[i] * sw) < K.huber_T)) ww = K.huber_T * K.huber_delta * sw / fabsf(ev[i]);
                                     }
+                                    const float aw = a * ww;
+                                    th2[i] += a * aw;
+                                    th1[i] -= ev[i] * aw;
                                 }
                             }
                         }
                     }
                 }
-                // fold the view groups of the warp onto group 0
-                for (int off = lprp; off < 32; off <<= 1) {
-#pragma unroll
-                    for (int i = 0; i < VEC; i++) {
-                        th1[i] += __shfl_xor_sync(0xffffffffu, th1[i], off);
-                        th2[i] += __shfl_xor_sync(0xffffffffu, th2[i], off);
-                    }
-                }
-                if (grp == 0 && row_ok) {
-#pragma unroll
-                    for (int i = 0; i < VEC; i++) {
-                        s_th1[warp][t0 + i] = th1[i];
-                        s_th2[warp][t0 + i] = th2[i];
-                    }
-                }
             }
-            __syncthreads();
-
-            // ---- 3. zero-skipping and solve (warp 0, lane = slice) -------------------
-            if (warp == 0) {
-                const float V0 = zl ? x[col_off + lane] : 0.0f;
-                float numA = 0.0f, denA = 0.0f, t1 = 0.0f, t2 = 0.0f;
-                int pos = 0;
-                for (int w = 0; w < W; w++) {
-                    numA += s_num[w][lane];
-                    denA += s_den[w][lane];
-                    pos |= s_pos[w][lane];
-                    if (lane < NT) {
-                        t1 += s_th1[w][lane];
-                        t2 += s_th2[w][lane];
-                    }
-                }
-                {
-                    const float vm = __shfl_up_sync(0xffffffffu, V0, 1);
-                    const float vp = __shfl_down_sync(0xffffffffu, V0, 1);
-                    if (lane >= 1 && vm > 0.0f) pos = 1;
-                    if (lane + 1 < NZ && vp > 0.0f) pos = 1;
-                }
-                const bool skip = !zl || (L.zero_skipping && L.iter > 1 && V0 == 0.0f && !pos);
-                __syncwarp();
-                s_th1[0][lane] = t1;
-                s_th2[0][lane] = t2;
-                __syncwarp();
-                float th1 = 0.0f, th2 = 0.0f;
-                if (zl)
-                    for (int r = 0; r < MZ; r++) {
-                        th1 += s_th1[0][lane * MZ + r];
-                        th2 += s_th2[0][lane * MZ + r];
-                    }
-                float cur = V0;
-#pragma unroll
-                for (int parity = 0; parity < 2; parity++) {
-                    const float vm = __shfl_up_sync(0xffffffffu, cur, 1);
-                    const float vp = __shfl_down_sync(0xffffffffu, cur, 1);
-                    if (!skip && (lane & 1) == parity) {
-                        float num = numA, den = denA;
-                        if (lane >= 1) {
-                            const float cf = K.sf[0 * 9 + 4] * qg_weight(V0 - vm, K.q, K.qmp, K.ssq, K.ssqp, K.cs, K.bs0);
-                            num += cf * vm;
-                            den += cf;
-                        }
-                        if (lane + 1 < NZ) {
-                            const float cf = K.sf[2 * 9 + 4] * qg_weight(V0 - vp, K.q, K.qmp, K.ssq, K.ssqp, K.cs, K.bs0);
-                            num += cf * vp;
-                            den += cf;
-                        }
-                        const float u = (num + th2 * V0 - th1) / (den + th2);
-                        cur = V0 + K.alpha * (u - V0);
-                    }
-                }
-                const float dx = skip ? 0.0f : cur - V0;
-                s_dx[lane] = dx;
-                if (zl) {
-                    if (!skip) {
-                        x[col_off + lane] = cur;
-                        n_upd++;
-                        sum_dx += fabsf(dx);
-                        sum_x += fabsf(cur);
-                    } else {
-                        n_skip++;
-                    }
-                }
-                float m = fabsf(dx);
-                for (int off = 16; off > 0; off >>= 1) m += __shfl_xor_sync(0xffffffffu, m, off);
-                if (lane == 0) mag[(size_t)f * nxy + c] = m;
-            }
-            __syncthreads();
-
-            // ---- 4. apply e -= a dx (the next column's barrier orders these
-            //         reductions before its theta loads) --------------------------------
-            {
-                float dxv[VEC];
-                bool any = false;
+            // fold the view groups of the warp onto group 0
+            for (int off = lprp; off < 32; off <<= 1) {
 #pragma unroll
                 for (int i = 0; i < VEC; i++) {
-                    dxv[i] = row_ok ? s_dx[(t0 + i) / MZ] : 0.0f;
-                    any |= dxv[i] != 0.0f;
+                    th1[i] += __shfl_xor_sync(0xffffffffu, th1[i], off);
+                    th2[i] += __shfl_xor_sync(0xffffffffu, th2[i], off);
                 }
-                if (any) {
-                    for (int v0 = gfirst; v0 < nv; v0 += kUnroll * gstride) {
-                        Rec<KW> R[kUnroll];
+            }
+            if (grp == 0 && row_ok) {
 #pragma unroll
-                        for (int u = 0; u < kUnroll; u++) {
-                            const int v = v0 + u * gstride;
-                            if (v < nv) R[u] = load_rec<KW>(col_rec + (size_t)v * RW);
-                            else R[u].w[0].x = 0u;
-                        }
+                for (int i = 0; i < VEC; i++) {
+                    S.th1[warp][t0 + i] = th1[i];
+                    S.th2[warp][t0 + i] = th2[i];
+                }
+            }
+        }
+        __syncthreads();
+
+        // ---- 3. zero-skipping and solve (warp 0, lane = slice) -------------------
+        if (warp == 0) {
+            const float V0 = zl ? x[col_off + lane] : 0.0f;
+            float numA = 0.0f, denA = 0.0f, t1 = 0.0f, t2 = 0.0f;
+            int pos = 0;
+            for (int w = 0; w < W; w++) {
+                numA += S.num[w][lane];
+                denA += S.den[w][lane];
+                pos |= S.pos[w][lane];
+                if (lane < NT) {
+                    t1 += S.th1[w][lane];
+                    t2 += S.th2[w][lane];
+                }
+            }
+            {
+                const float vm = __shfl_up_sync(0xffffffffu, V0, 1);
+                const float vp = __shfl_down_sync(0xffffffffu, V0, 1);
+                if (lane >= 1 && vm > 0.0f) pos = 1;
+                if (lane + 1 < NZ && vp > 0.0f) pos = 1;
+            }
+            const bool skip = !zl || (L.zero_skipping && L.iter > 1 && V0 == 0.0f && !pos);
+            __syncwarp();
+            S.th1[0][lane] = t1;
+            S.th2[0][lane] = t2;
+            __syncwarp();
+            float th1 = 0.0f, th2 = 0.0f;
+            if (zl)
+                for (int r = 0; r < MZ; r++) {
+                    th1 += S.th1[0][lane * MZ + r];
+                    th2 += S.th2[0][lane * MZ + r];
+                }
+            float cur = V0;
 #pragma unroll
-                        for (int u = 0; u < kUnroll; u++) {
-                            const uint32_t hdr = R[u].w[0].x;
-                            const int cnt = hdr >> 24;
-                            const size_t sb = (size_t)(hdr & 0xFFFFFF) * NT + t0;
+            for (int parity = 0; parity < 2; parity++) {
+                const float vm = __shfl_up_sync(0xffffffffu, cur, 1);
+                const float vp = __shfl_down_sync(0xffffffffu, cur, 1);
+                if (!skip && (lane & 1) == parity) {
+                    float num = numA, den = denA;
+                    if (lane >= 1) {
+                        const float cf = K.sf[0 * 9 + 4] * qg_weight(V0 - vm, K.q, K.qmp, K.ssq, K.ssqp, K.cs, K.bs0);
+                        num += cf * vm;
+                        den += cf;
+                    }
+                    if (lane + 1 < NZ) {
+                        const float cf = K.sf[2 * 9 + 4] * qg_weight(V0 - vp, K.q, K.qmp, K.ssq, K.ssqp, K.cs, K.bs0);
+                        num += cf * vp;
+                        den += cf;
+                    }
+                    const float u = (num + th2 * V0 - th1) / (den + th2);
+                    cur = V0 + K.alpha * (u - V0);
+                }
+            }
+            const float dx = skip ? 0.0f : cur - V0;
+            S.dx[lane] = dx;
+            if (zl) {
+                if (!skip) {
+                    x[col_off + lane] = cur;
+                    cnt.upd++;
+                    cnt.sum_dx += fabsf(dx);
+                    cnt.sum_x += fabsf(cur);
+                } else {
+                    cnt.skip++;
+                }
+            }
+            float m = fabsf(dx);
+            for (int off = 16; off > 0; off >>= 1) m += __shfl_xor_sync(0xffffffffu, m, off);
+            if (lane == 0) mag[(size_t)f * nxy + c] = m;
+        }
+        __syncthreads();
+
+        // ---- 4. apply e -= a dx (the next column's barrier orders these
+        //         reductions before its theta loads) --------------------------------
+        {
+            float dxv[VEC];
+            bool any = false;
 #pragma unroll
-                            for (int q = 0; q < 4 * KW - 1; q++) {
-                                if (q < cnt) {
-                                    const float a = -(rec_val<KW>(R[u], q) * K.dt);
-                                    float d[VEC];
+            for (int i = 0; i < VEC; i++) {
+                dxv[i] = row_ok ? S.dx[(t0 + i) / MZ] : 0.0f;
+                any |= dxv[i] != 0.0f;
+            }
+            if (any) {
+                for (int v0 = gfirst; v0 < nv; v0 += kUnroll * gstride) {
+                    Rec<KW> R[kUnroll];
 #pragma unroll
-                                    for (int i = 0; i < VEC; i++) d[i] = a * dxv[i];
-                                    red_add(err + sb + (size_t)q * NT, d);
-                                }
+                    for (int u = 0; u < kUnroll; u++) {
+                        const int v = v0 + u * gstride;
+                        if (v < nv) R[u] = load_rec<KW>(col_rec + (size_t)v * RW);
+                        else R[u].w[0].x = 0u;
+                    }
+#pragma unroll
+                    for (int u = 0; u < kUnroll; u++) {
+                        const uint32_t hdr = R[u].w[0].x;
+                        const int cnt_q = hdr >> 24;
+                        const size_t sb = (size_t)(hdr & 0xFFFFFF) * NT + t0;
+#pragma unroll
+                        for (int q = 0; q < 4 * KW - 1; q++) {
+                            if (q < cnt_q) {
+                                const float a = -(rec_val<KW>(R[u], q) * K.dt);
+                                float d[VEC];
+#pragma unroll
+                                for (int i = 0; i < VEC; i++) d[i] = a * dxv[i];
+                                red_add(err + sb + (size_t)q * NT, d);
                             }
                         }
                     }
@@ -445,22 +451,37 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 4) icd_phase_kernel(
             }
         }
     }
+}
 
-    // ---- per-CTA statistics -------------------------------------------------------------
-    if (warp == 0) {
-        for (int off = 16; off > 0; off >>= 1) {
-            n_upd += __shfl_xor_sync(0xffffffffu, n_upd, off);
-            n_skip += __shfl_xor_sync(0xffffffffu, n_skip, off);
-            sum_dx += __shfl_xor_sync(0xffffffffu, sum_dx, off);
-            sum_x += __shfl_xor_sync(0xffffffffu, sum_x, off);
-        }
-        if (lane == 0) {
-            atomicAdd(&stats->updates, n_upd);
-            atomicAdd(&stats->skipped, n_skip);
-            atomicAdd(&stats->sum_abs_dx, (double)sum_dx);
-            atomicAdd(&stats->sum_abs_x, (double)sum_x);
-        }
+}  // namespace
+
+// One colour phase of one problem: persistent CTAs drain the phase's SV queue.
+template <int KW, int kUnroll, int VEC>
+__global__ void __launch_bounds__(kMaxWarps * 32, 4) icd_phase_kernel(
+    Geom g, IcdLaunch L, IcdConst K, const uint32_t *__restrict__ table, const int32_t *__restrict__ view_first,
+    const uint8_t *__restrict__ mask, float *__restrict__ x, float *__restrict__ err, const float *__restrict__ wgt,
+    float *__restrict__ mag, IcdStats *__restrict__ stats, unsigned int *__restrict__ queue)
+{
+    __shared__ IcdSmem S;
+    const int KC = L.colors_k;
+    const int hx = (L.n_sv_x + KC - 1) / KC, slots = hx * ((L.n_sv_y + KC - 1) / KC);
+    const int n_items = g.N_time * slots;
+    IcdCount cnt{};
+    for (;;) {
+        __syncthreads();  // S.item / S.order of the previous SV are no longer read
+        if (threadIdx.x == 0) S.item = (int)atomicAdd(queue, 1u);
+        __syncthreads();
+        const int item = S.item;
+        if (item >= n_items) break;
+        const int f = item % g.N_time;  // frames fastest: concurrent SVs spread over the frames
+        const int rem = (int)((long long)(item / g.N_time) * L.perm % slots);
+        const int color = (L.phase + f) % (KC * KC);  // frame f +- 1 is never on the same colour
+        const int sx = KC * (rem % hx) + color % KC;
+        const int sy = KC * (rem / hx) + color / KC;
+        if (sx >= L.n_sv_x || sy >= L.n_sv_y) continue;  // uniform
+        icd_update_sv<KW, kUnroll, VEC>(g, L, K, table, view_first, mask, x, err, wgt, mag, f, sx, sy, S, cnt);
     }
+    flush_counts(cnt, stats);
 }
 
 template <int KW, int U, int VEC>
@@ -473,17 +494,15 @@ static void launch_kw(const Geom &g, const IcdLaunch &L, const IcdConst &K, cons
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, icd_phase_kernel<KW, U, VEC>, threads, 0);
-    const int half_x = (L.n_sv_x + 1) / 2, half_y = (L.n_sv_y + 1) / 2;
-    const long long items = (long long)g.N_time * half_x * half_y;
+    const long long items = (long long)g.N_time * sv_slots(g.N_x, g.N_y, L.sv, L.colors_k);
     long long grid = (long long)sms * (per_sm > 0 ? per_sm : 1);
     if (grid > items) grid = items;
+    if (L.max_ctas > 0 && grid > L.max_ctas) grid = L.max_ctas;
     icd_phase_kernel<KW, U, VEC><<<(unsigned)grid, threads, 0, st>>>(g, L, K, d_table, d_view_first, d_mask, d_x,
                                                                      d_err, d_w, d_mag, d_stats, d_queue);
 }
 
-void launch_icd_phase(const Geom &g, const IcdLaunch &L, const uint32_t *d_table, const int32_t *d_view_first,
-                      const uint8_t *d_mask, float *d_x, float *d_err, const float *d_w, float *d_mag,
-                      IcdStats *d_stats, unsigned int *d_queue, cudaStream_t st)
+IcdConst make_icd_const(const Geom &g)
 {
     IcdConst K;
     for (int i = 0; i < 27; i++) K.sf[i] = (float)g.spatial_filter[i];
@@ -503,6 +522,14 @@ void launch_icd_phase(const Geom &g, const IcdLaunch &L, const uint32_t *d_table
     K.huber_T = (float)g.huber_T;
     K.huber_delta = (float)g.huber_delta;
     K.huber = g.huber;
+    return K;
+}
+
+void launch_icd_phase(const Geom &g, const IcdLaunch &L, const uint32_t *d_table, const int32_t *d_view_first,
+                      const uint8_t *d_mask, float *d_x, float *d_err, const float *d_w, float *d_mag,
+                      IcdStats *d_stats, unsigned int *d_queue, cudaStream_t st)
+{
+    const IcdConst K = make_icd_const(g);
 #define MBIR_LAUNCH(KW, U, VEC) \
     launch_kw<KW, U, VEC>(g, L, K, d_table, d_view_first, d_mask, d_x, d_err, d_w, d_mag, d_stats, d_queue, st)
     const int kw = g.rec_words / 4;
@@ -523,6 +550,115 @@ void launch_icd_phase(const Geom &g, const IcdLaunch &L, const uint32_t *d_table
         else MBIR_LAUNCH(3, 1, 2);
     }
 #undef MBIR_LAUNCH
+}
+
+// ---------------------------------------------------------------------------------------------
+// Many independent problems in one persistent launch per colour phase. The
+// queue runs over the SV items of every problem of the launch, interleaved in
+// proportion to each problem's item count (item_map[] gives the problem and
+// its item), so the CTAs working at any moment spread over the problems; a
+// CTA keeps the descriptor of its current problem in shared memory and
+// reloads it when its next item belongs to another problem. Problems of one
+// launch share the record width and the detector-row vector width (template
+// parameters).
+template <int KW, int kUnroll, int VEC>
+__global__ void __launch_bounds__(kMaxWarps * 32, 4) icd_batch_kernel(const BatchDesc *__restrict__ descs,
+                                                                      const int2 *__restrict__ item_map, int total,
+                                                                      int phase, unsigned int *__restrict__ queue)
+{
+    __shared__ IcdSmem S;
+    __shared__ __align__(16) BatchDesc P;
+    int cur = -1;
+    IcdCount cnt{};
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0) S.item = (int)atomicAdd(queue, 1u);
+        __syncthreads();
+        const int item = S.item;
+        if (item >= total) break;
+        const int2 pm = item_map[item];  // (problem, item of that problem)
+        if (pm.x != cur) {                // uniform
+            if (cur >= 0) flush_counts(cnt, P.stats);
+            __syncthreads();
+            const int4 *src = reinterpret_cast<const int4 *>(descs + pm.x);
+            int4 *dst = reinterpret_cast<int4 *>(&P);
+            for (int i = threadIdx.x; i < (int)(sizeof(BatchDesc) / sizeof(int4)); i += blockDim.x) dst[i] = src[i];
+            __syncthreads();
+            cur = pm.x;
+        }
+        if (!P.active) continue;
+        const int K = P.L.colors_k;
+        const int hx = (P.L.n_sv_x + K - 1) / K, slots = hx * ((P.L.n_sv_y + K - 1) / K);
+        const int f = pm.y % P.g.N_time;
+        const int rem = (int)((long long)(pm.y / P.g.N_time) * P.L.perm % slots);
+        const int color = (phase + f) % (K * K);
+        const int sx = K * (rem % hx) + color % K;
+        const int sy = K * (rem / hx) + color / K;
+        if (sx >= P.L.n_sv_x || sy >= P.L.n_sv_y) continue;
+        icd_update_sv<KW, kUnroll, VEC>(P.g, P.L, P.K, P.table, P.view_first, P.mask, P.x, P.err, P.w, P.mag, f, sx,
+                                        sy, S, cnt);
+    }
+    if (cur >= 0) flush_counts(cnt, P.stats);
+}
+
+// Before an iteration: advance every problem's iteration number and clear its counters.
+__global__ void batch_begin_iteration(BatchDesc *descs, int n)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    descs[i].L.iter += 1;
+    *descs[i].stats = IcdStats{};
+}
+
+// After an iteration: accumulate the updates and stop problems whose
+// convergence statistic 100 sum|dx| / sum|x| fell below their threshold after
+// the first iteration (XT_ICD_update.c:1083-1090).
+__global__ void batch_end_iteration(BatchDesc *descs, int n)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || !descs[i].active) return;
+    const IcdStats s = *descs[i].stats;
+    descs[i].total_updates += s.updates;
+    descs[i].iters_done = descs[i].L.iter;
+    const double pct = s.sum_abs_x > 0 ? 100.0 * s.sum_abs_dx / s.sum_abs_x : 0.0;
+    descs[i].last_pct = pct;
+    if (descs[i].L.iter > 1 && pct < descs[i].convg_thresh) descs[i].active = 0;
+}
+
+int batch_grid(int vec, int warps)
+{
+    int dev = 0, sms = 148, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (vec == 4) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, icd_batch_kernel<1, 2, 4>, warps * 32, 0);
+    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, icd_batch_kernel<1, 2, 2>, warps * 32, 0);
+    return sms * (per_sm > 0 ? per_sm : 1);
+}
+
+void launch_icd_batch(int vec, int warps, int grid, const BatchDesc *d_descs, const int2 *d_item_map, int total,
+                      int phase, unsigned int *d_queue, cudaStream_t st)
+{
+    if (vec == 4) icd_batch_kernel<1, 2, 4><<<grid, warps * 32, 0, st>>>(d_descs, d_item_map, total, phase, d_queue);
+    else icd_batch_kernel<1, 2, 2><<<grid, warps * 32, 0, st>>>(d_descs, d_item_map, total, phase, d_queue);
+}
+
+int icd_grid(int warps)
+{
+    int dev = 0, sms = 148, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, icd_phase_kernel<1, 2, 4>, warps * 32, 0);
+    return sms * (per_sm > 0 ? per_sm : 1);
+}
+
+void launch_batch_begin(BatchDesc *d_descs, int n, cudaStream_t st)
+{
+    batch_begin_iteration<<<(n + 127) / 128, 128, 0, st>>>(d_descs, n);
+}
+
+void launch_batch_end(BatchDesc *d_descs, int n, cudaStream_t st)
+{
+    batch_end_iteration<<<(n + 127) / 128, 128, 0, st>>>(d_descs, n);
 }
 
 }  // namespace mbirgpu

@@ -1,6 +1,7 @@
 // Internal declarations shared by the host code and the CUDA kernels of
 // libmbirgpu. Not part of the public ABI (include/mbirgpu.h is).
 #pragma once
+#include <algorithm>
 #include <cstdint>
 #include <cstddef>
 #include <string>
@@ -91,14 +92,116 @@ struct IcdLaunch {
     int zero_skipping;
     int unroll;           // views in flight per lane (1, 2, 4); the launcher caps it by record width
     uint64_t seed;
+    const uint8_t *sel;   // [N_time][N_y][N_x] columns this sweep may visit (with the mask); null = all
+    int perm;             // queue order inside a frame: SV slot = (queue index * perm) mod slots
+    int colors_k;         // K x K colour classes; phase p updates colour (p + frame) mod K^2
+    long long max_ctas;   // cap on the persistent grid (sv_max_concurrent); 0 = none
 };
+
+// SV slots of one colour per frame and the items (all frames) of one phase.
+inline int sv_slots(int N_x, int N_y, int sv, int K)
+{
+    const int nx = (N_x + sv - 1) / sv, ny = (N_y + sv - 1) / sv;
+    return ((nx + K - 1) / K) * ((ny + K - 1) / K);
+}
+
+// Multiplier of the SV queue order: coprime with n and near n / golden ratio,
+// so consecutive queue positions -- the SVs CTAs work on at the same time --
+// land far apart in the image instead of in one band of SV rows.
+inline int spread_multiplier(int n)
+{
+    if (n <= 2) return 1;
+    auto gcd = [](long long a, long long b) {
+        while (b) {
+            const long long t = a % b;
+            a = b;
+            b = t;
+        }
+        return a;
+    };
+    long long p = (long long)(0.6180339887498949 * n);
+    if (p < 1) p = 1;
+    while (gcd(p, n) != 1) p++;
+    return (int)p;
+}
 struct IcdStats {  // device accumulators
     unsigned long long updates, skipped;
     double sum_abs_dx, sum_abs_x;
 };
+// Per-problem constants of the voxel update, in FP32.
+struct IcdConst {
+    float sf[27];
+    float tf;
+    float q, qmp, ssq, ssqp, stq, stqp, cs, ct, bs0, bt0, alpha, dt;
+    float huber_T, huber_delta;
+    int huber;
+};
+IcdConst make_icd_const(const Geom &g);
+
 // d_queue: one zeroed counter per launch (the persistent CTAs' work queue).
 void launch_icd_phase(const Geom &g, const IcdLaunch &L, const uint32_t *d_table, const int32_t *d_view_first,
                       const uint8_t *d_mask, float *d_x, float *d_err, const float *d_w, float *d_mag,
                       IcdStats *d_stats, unsigned int *d_queue, cudaStream_t st);
+
+// One problem of a batched launch (device-resident descriptor).
+constexpr int kMaxBatch = 256;
+struct __align__(16) BatchDesc {
+    Geom g;
+    IcdLaunch L;
+    IcdConst K;
+    const uint32_t *table;
+    const int32_t *view_first;
+    const uint8_t *mask;
+    float *x, *err;
+    const float *w;
+    float *mag;
+    IcdStats *stats;
+    unsigned long long total_updates;  // voxel updates of all iterations run
+    double last_pct;                   // last convergence statistic 100 sum|dx| / sum|x|
+    float convg_thresh;                // the problem's convg_thresh (percent)
+    int active;                        // 0 once converged: its items are skipped
+    int iters_done;
+};
+int batch_grid(int vec, int warps);
+void launch_icd_batch(int vec, int warps, int grid, const BatchDesc *d_descs, const int2 *d_item_map, int total,
+                      int phase, unsigned int *d_queue, cudaStream_t st);
+// persistent grid of the one-problem sweep kernel at `warps` warps per CTA
+int icd_grid(int warps);
+// Stability of concurrent super-voxel updates: CTAs update different columns
+// at the same time, and columns of one frame on a common ray couple like a
+// Jacobi step, more strongly the closer they are. Same-colour SVs are K sv
+// columns apart; with C columns of a frame in flight, spread over the image
+// (spread_multiplier), the over-relaxed updates stay convergent for
+// 32 C <= N_y (K sv / 2)^2. Measured on 256 x 256 single-frame problems
+// (90-360 views, no temporal prior): sv 4 with K = 2 converges at C <= 256
+// and diverges at C = 512 (one problem already at 256); sv 8 with K = 2
+// converges at C = 256, all its SVs of a colour. Launches cap their
+// persistent grid at this many CTAs (frames are interleaved in the queue,
+// so each frame gets its share).
+inline long long sv_max_concurrent(int N_x, int N_y, int frames, int sv, int K)
+{
+    const long long spacing = (long long)K * sv / 2;
+    (void)N_x;
+    return std::max(1LL, (long long)std::max(1, frames) * ((long long)N_y * spacing * spacing / 32));
+}
+
+// Relative iterations to convergence by same-colour spacing K sv / 2
+// (4: 1, 8: 51/56, 16: 38/56, measured on the 4-D workload with K = 2).
+inline double sv_convergence_factor(int sv, int K)
+{
+    const int spacing = K * sv / 2;
+    return spacing >= 16 ? 38.0 / 56.0 : spacing >= 8 ? 51.0 / 56.0 : 1.0;
+}
+void launch_batch_begin(BatchDesc *d_descs, int n, cudaStream_t st);
+void launch_batch_end(BatchDesc *d_descs, int n, cudaStream_t st);
+
+// Non-homogeneous ICD selection (VSC_based_Voxel_Line_Select, XT_NHICD.c:164-216):
+// per frame, the 5x5 Hamming-filtered update-magnitude map (ComputeVSC,
+// :128-161) and sel = mask && filtered > the (N - k)-th smallest filtered
+// value, N = N_x N_y (RandomizedSelect's threshold), i.e. the k largest.
+constexpr int kMaxNhPasses = 16;
+constexpr int kNhicdIterations = 10;  // NHICD_Iterations, XT_Init.c:406
+void launch_nh_select(int n_frames, int N_y, int N_x, const float *d_mag, const uint8_t *d_mask, int k,
+                      float *d_filt, uint8_t *d_sel, cudaStream_t st);
 
 }  // namespace mbirgpu

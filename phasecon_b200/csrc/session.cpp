@@ -64,7 +64,7 @@ static int dalloc(T **p, size_t n, size_t *acc)
 Session::~Session()
 {
     void *ptrs[] = {d_y, d_w, d_err, d_x, d_tmp, d_table, d_Hr, d_cos, d_sin, d_views, d_view_first, d_view_frame,
-                    d_mask, d_mag, d_stats, d_cost_partials, d_cost_out, d_flag, d_acc, d_queue};
+                    d_mask, d_mag, d_stats, d_cost_partials, d_cost_out, d_flag, d_acc, d_queue, d_filt, d_sel};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     for (auto &ev : ev_pairs) {
@@ -115,7 +115,10 @@ int Session::init(const mbirgpu_problem *pb, const mbirgpu_options *o, int mult_
         dalloc(&d_view_frame, (size_t)g.N_p, &acc) || dalloc(&d_mask, nxy, &acc) ||
         dalloc(&d_mag, (size_t)g.N_time * nxy, &acc) || dalloc(&d_stats, 1, &acc) ||
         dalloc(&d_cost_partials, (size_t)cost_partials_needed(g), &acc) || dalloc(&d_cost_out, 2, &acc) ||
-        dalloc(&d_flag, 1, &acc) || dalloc(&d_acc, n_sino, &acc) || dalloc(&d_queue, 4, &acc))
+        dalloc(&d_flag, 1, &acc) || dalloc(&d_acc, n_sino, &acc) || dalloc(&d_queue, kQueueCounters, &acc))
+        return -1;
+    if (opt.nhicd_passes > 0 &&
+        (dalloc(&d_filt, (size_t)g.N_time * nxy, &acc) || dalloc(&d_sel, (size_t)g.N_time * nxy, &acc)))
         return -1;
 
     // views not assigned to any frame keep no A records; frame map for the builder
@@ -172,57 +175,66 @@ int Session::init(const mbirgpu_problem *pb, const mbirgpu_options *o, int mult_
     if (refresh_error()) return -1;
     return autotune();
 }
-
-// Schedule autotuner. Candidates: super-voxel edge sv in {4, 8, 16} and
-// warps per CTA in {2, 4}. Each candidate runs one ICD sweep on the current
-// state (snapshotted and restored afterwards); its time is scaled by the
-// relative number of iterations that SV size needs to reach a relative cost
-// change of 1e-4 (larger SVs update fewer neighbouring columns at once and
-// converge in fewer iterations; measured on the 4-D workload from zero:
-// 56 / 51 / 38 iterations for sv = 4 / 8 / 16). The smallest estimated
-// time to convergence wins. User-fixed sv_size / cta_warps bypass the search.
+// Schedule autotuner. Candidates: (super-voxel edge sv, colours K) in
+// {(4, 2), (4, 4), (8, 2), (8, 4), (16, 2)} and warps per CTA in {2, 4}, each
+// with its grid capped at sv_max_concurrent CTAs. Each candidate runs one
+// iteration as the run will (the second one when non-homogeneous passes are
+// on) on the current state (snapshotted and restored afterwards);
+// its time is scaled by the relative number of iterations its same-colour
+// spacing needs to converge (sv_convergence_factor). The smallest estimated
+// time to convergence wins. User-fixed sv_size / cta_warps / sv_colors
+// restrict the search; with all three fixed there is none.
 void Session::choose_schedule()
 {
     const Geom &g = hs.g;
     int ntp = 4;
     while (ntp < g.N_t) ntp <<= 1;
     sv = opt.sv_size > 0 ? std::min(opt.sv_size, 16) : 8;
+    colors = opt.sv_colors > 0 ? opt.sv_colors : 2;
     warps = opt.cta_warps > 0 ? std::min(opt.cta_warps, 8) : std::max(2, std::min(8, g.max_views / (16 * (32 / ntp))));
 }
 
 int Session::autotune()
 {
-    if (opt.sv_size > 0 && opt.cta_warps > 0) return 0;
+    if (opt.sv_size > 0 && opt.cta_warps > 0 && opt.sv_colors > 0) return 0;
     const Geom &g = hs.g;
     // snapshot x and e into the scratch buffers (d_tmp holds a volume, d_acc a sinogram)
     CK(cudaMemcpyAsync(d_tmp, d_x, n_vox * sizeof(float), cudaMemcpyDeviceToDevice, st));
     CK(cudaMemcpyAsync(d_acc, d_err, n_sino * sizeof(float), cudaMemcpyDeviceToDevice, st));
     const bool save_timing = timing;
     timing = true;
-    const int svs[3] = {4, 8, 16};
-    const double conv[3] = {1.0, 51.0 / 56.0, 38.0 / 56.0};
+    const int cand[5][2] = {{4, 2}, {4, 4}, {8, 2}, {8, 4}, {16, 2}};
     const int ws[2] = {2, 4};
+    auto allowed = [&](int a, int b) {
+        if (opt.sv_size > 0 && cand[a][0] != opt.sv_size) return false;
+        if (opt.sv_colors > 0 && cand[a][1] != opt.sv_colors) return false;
+        if (opt.cta_warps > 0 && ws[b] != opt.cta_warps) return false;
+        return cand[a][0] <= std::max(g.N_x, g.N_y);
+    };
     double best = 1e300;
-    int best_sv = sv, best_w = warps;
-    for (int a = 0; a < 3; a++) {
-        if (opt.sv_size > 0 && svs[a] != opt.sv_size) continue;
-        if (svs[a] > std::max(g.N_x, g.N_y)) continue;
+    int best_sv = sv, best_w = warps, best_k = colors;
+    for (int a = 0; a < 5; a++) {
         for (int b = 0; b < 2; b++) {
-            if (opt.cta_warps > 0 && ws[b] != opt.cta_warps) continue;
-            sv = svs[a];
+            if (!allowed(a, b)) continue;
+            sv = cand[a][0];
+            colors = cand[a][1];
             warps = ws[b];
+            // time a full iteration as the run will do it: with non-homogeneous
+            // passes that is iteration 2 (they start there), after iteration 1
             mbirgpu_iter_stats st_;
             const int saved_refresh = opt.refresh_every;
             opt.refresh_every = 0;
             int rc = icd_iteration(1, &st_);
+            if (!rc && opt.nhicd_passes > 0 && d_sel) rc = icd_iteration(2, &st_);
             opt.refresh_every = saved_refresh;
             if (rc) return -1;
-            const double est = st_.kernel_ms * conv[a];
+            const double est = st_.kernel_ms * sv_convergence_factor(sv, colors);
             tune_log.push_back({sv, warps, st_.kernel_ms});
             if (est < best) {
                 best = est;
                 best_sv = sv;
                 best_w = warps;
+                best_k = colors;
             }
             CK(cudaMemcpyAsync(d_x, d_tmp, n_vox * sizeof(float), cudaMemcpyDeviceToDevice, st));
             CK(cudaMemcpyAsync(d_err, d_acc, n_sino * sizeof(float), cudaMemcpyDeviceToDevice, st));
@@ -231,6 +243,7 @@ int Session::autotune()
     timing = save_timing;
     sv = best_sv;
     warps = best_w;
+    colors = best_k;
     CK(cudaMemsetAsync(d_mag, 0, (size_t)g.N_time * g.N_x * g.N_y * sizeof(float), st));
     CK(cudaStreamSynchronize(st));
     return 0;
@@ -281,7 +294,7 @@ int Session::icd_iteration(int iter, mbirgpu_iter_stats *out)
 {
     const Geom &g = hs.g;
     CK(cudaMemsetAsync(d_stats, 0, sizeof(IcdStats), st));
-    CK(cudaMemsetAsync(d_queue, 0, 4 * sizeof(unsigned int), st));
+    CK(cudaMemsetAsync(d_queue, 0, kQueueCounters * sizeof(unsigned int), st));
     IcdLaunch L{};
     L.sv = sv;
     L.n_sv_x = (g.N_x + sv - 1) / sv;
@@ -291,22 +304,46 @@ int Session::icd_iteration(int iter, mbirgpu_iter_stats *out)
     L.zero_skipping = opt.zero_skipping;
     L.unroll = opt.icd_unroll > 0 ? opt.icd_unroll : 4;
     L.seed = opt.seed;
+    L.colors_k = colors;
+    L.perm = spread_multiplier(sv_slots(g.N_x, g.N_y, sv, colors));
+    L.max_ctas = sv_max_concurrent(g.N_x, g.N_y, g.N_time, sv, colors);
+    const int phases = colors * colors;
     Geom gb = g;
     gb.N_p = n_assigned;
-    if (timing && ev_pairs.size() < 4) {
-        while (ev_pairs.size() < 4) {
+    if (timing && ev_pairs.size() < 2) {
+        while (ev_pairs.size() < 2) {
             cudaEvent_t a, b;
             CK(cudaEventCreate(&a));
             CK(cudaEventCreate(&b));
             ev_pairs.push_back({a, b});
         }
     }
-    for (int ph = 0; ph < 4; ph++) {
+    if (timing) CK(cudaEventRecord(ev_pairs[0].first, st));
+    for (int ph = 0; ph < phases; ph++) {
         L.phase = ph;
-        if (timing) CK(cudaEventRecord(ev_pairs[ph].first, st));
         launch_icd_phase(gb, L, d_table, d_view_first, d_mask, d_x, d_err, d_w, d_mag, d_stats, d_queue + ph, st);
-        if (timing) CK(cudaEventRecord(ev_pairs[ph].second, st));
     }
+    if (timing) CK(cudaEventRecord(ev_pairs[0].second, st));
+    int launches = phases;
+    // non-homogeneous passes (the reference's NH-ICD, from iteration 2): each
+    // re-updates the k columns per frame with the largest filtered update
+    // magnitude, k = masked columns / NHICD_Iterations (XT_NHICD.c:176)
+    const int nh = (d_sel && iter > 1) ? std::min(opt.nhicd_passes, kMaxNhPasses) : 0;
+    if (nh > 0 && timing) CK(cudaEventRecord(ev_pairs[1].first, st));
+    for (int pass = 0; pass < nh; pass++) {
+        const int k = (int)(masked_columns / std::max(1, g.N_time)) / kNhicdIterations;
+        launch_nh_select(g.N_time, g.N_y, g.N_x, d_mag, d_mask, k, d_filt, d_sel, st);
+        IcdLaunch Ln = L;
+        Ln.sel = d_sel;
+        Ln.seed = L.seed ^ (0x9E3779B97F4A7C15ull * (uint64_t)(pass + 1));
+        for (int ph = 0; ph < phases; ph++) {
+            Ln.phase = ph;
+            launch_icd_phase(gb, Ln, d_table, d_view_first, d_mask, d_x, d_err, d_w, d_mag, d_stats,
+                             d_queue + kMaxPhases * (pass + 1) + ph, st);
+        }
+        launches += phases + 2;
+    }
+    if (nh > 0 && timing) CK(cudaEventRecord(ev_pairs[1].second, st));
     CK(cudaGetLastError());
     if (opt.refresh_every > 0 && iter % opt.refresh_every == 0)
         if (refresh_error()) return -1;
@@ -319,12 +356,13 @@ int Session::icd_iteration(int iter, mbirgpu_iter_stats *out)
         out->zero_skipped = (int64_t)hst.skipped;
         out->sum_abs_update = hst.sum_abs_dx;
         out->sum_abs_value = hst.sum_abs_x;
-        out->kernel_launches = 4;
+        out->kernel_launches = launches;
         if (timing) {
-            double ms = 0;
-            for (int ph = 0; ph < 4; ph++) {
-                float m = 0;
-                CK(cudaEventElapsedTime(&m, ev_pairs[ph].first, ev_pairs[ph].second));
+            float m = 0;
+            CK(cudaEventElapsedTime(&m, ev_pairs[0].first, ev_pairs[0].second));
+            double ms = m;
+            if (nh > 0) {
+                CK(cudaEventElapsedTime(&m, ev_pairs[1].first, ev_pairs[1].second));
                 ms += m;
             }
             out->kernel_ms = ms;
@@ -466,6 +504,8 @@ void mbirgpu_default_options(mbirgpu_options *o)
     o->cta_warps = 0;
     o->icd_unroll = 0;
     o->seed = 761521;  // the reference's srandom2 seed, XT_Engine.c:99
+    o->nhicd_passes = mbirgpu::kNhicdIterations;  // the reference runs NH-ICD by default (NO_NHICD 0)
+    o->sv_colors = 0;
 }
 
 int mbirgpu_set_options(const mbirgpu_options *o)
@@ -476,6 +516,9 @@ int mbirgpu_set_options(const mbirgpu_options *o)
     if (o->sv_size < 0 || o->sv_size > 16) return fail("sv_size must be 0 (auto) or 1..16");
     if (o->cta_warps < 0 || o->cta_warps > 8) return fail("cta_warps must be 0 (auto) or 1..8");
     if (o->icd_unroll < 0 || o->icd_unroll > 4) return fail("icd_unroll must be 0 (auto) or 1..4");
+    if (o->nhicd_passes < 0 || o->nhicd_passes > mbirgpu::kMaxNhPasses)
+        return fail("nhicd_passes must be 0 (off) .. %d", mbirgpu::kMaxNhPasses);
+    if (o->sv_colors != 0 && o->sv_colors != 2 && o->sv_colors != 4) return fail("sv_colors must be 0 (auto), 2 or 4");
     mbirgpu_options cur = mbirgpu::current_options();
     (void)cur;
     std::lock_guard<std::mutex> lk(mbirgpu::g_opt_mu);
@@ -537,6 +580,7 @@ int mbirgpu_session_info_get(const mbirgpu_session *sp, mbirgpu_session_info *in
     info->kmax = g.kmax;
     info->sv_size = s->sv;
     info->cta_warps = s->warps;
+    info->sv_colors = s->colors;
     info->masked_columns = s->masked_columns;
     info->nnz = s->masked_nnz;
     info->delta_t = g.delta_t;
@@ -611,6 +655,32 @@ int mbirgpu_session_icd_iteration(mbirgpu_session *sp, int32_t iter, mbirgpu_ite
     SESSION(sp);
     if (iter < 1) return fail("iterations are numbered from 1");
     return s->icd_iteration(iter, stats);
+}
+
+int mbirgpu_session_nh_select(mbirgpu_session *sp, const float *mag, uint8_t *sel)
+{
+    SESSION(sp);
+    if (!mag || !sel) return fail("NULL argument");
+    const mbirgpu::Geom &g = s->hs.g;
+    const size_t n = (size_t)g.N_time * g.N_y * g.N_x;
+    float *d_m = nullptr, *d_f = nullptr;
+    uint8_t *d_s = nullptr;
+    cudaError_t e = cudaMalloc((void **)&d_m, n * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc((void **)&d_f, n * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc((void **)&d_s, n);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_m, mag, n * sizeof(float), cudaMemcpyHostToDevice, s->st);
+    if (e == cudaSuccess) {
+        const int k = (int)(s->masked_columns / std::max(1, g.N_time)) / mbirgpu::kNhicdIterations;
+        mbirgpu::launch_nh_select(g.N_time, g.N_y, g.N_x, d_m, s->d_mask, k, d_f, d_s, s->st);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(sel, d_s, n, cudaMemcpyDeviceToHost, s->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
+    cudaFree(d_m);
+    cudaFree(d_f);
+    cudaFree(d_s);
+    if (e != cudaSuccess) return fail("NH-ICD selection failed: %s", cudaGetErrorString(e));
+    return 0;
 }
 
 int mbirgpu_session_forward_project(mbirgpu_session *sp, const float *object, float *sino)

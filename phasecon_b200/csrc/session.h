@@ -19,7 +19,7 @@ struct Session {
     int n_assigned = 0;  // views that belong to some frame
     int64_t masked_columns = 0;
     int64_t masked_nnz = 0;  // A nonzeros over masked columns, all frames, per voxel slice
-    int sv = 8, warps = 4;
+    int sv = 8, warps = 4, colors = 2;
     bool timing = false;
 
     float *d_y = nullptr, *d_w = nullptr, *d_err = nullptr, *d_x = nullptr, *d_tmp = nullptr;
@@ -33,7 +33,11 @@ struct Session {
     double *d_cost_partials = nullptr, *d_cost_out = nullptr;
     int *d_flag = nullptr;
     double *d_acc = nullptr;  // FP64 sinogram accumulator of the forward projector
-    unsigned int *d_queue = nullptr;  // super-voxel work-queue counters, one per colour phase
+    unsigned int *d_queue = nullptr;  // super-voxel work-queue counters, one per ICD launch of an iteration
+    static constexpr int kMaxPhases = 16;  // K x K colours, K <= 4
+    static constexpr int kQueueCounters = kMaxPhases * (1 + kMaxNhPasses);
+    float *d_filt = nullptr;          // NH-ICD filtered update magnitudes [N_time][N_y][N_x]
+    uint8_t *d_sel = nullptr;         // NH-ICD selected columns [N_time][N_y][N_x]
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pairs;
 
     ~Session();

@@ -27,7 +27,9 @@ EXPORTS = (
     "mbirgpu_session_object_device", "mbirgpu_session_refresh_error", "mbirgpu_session_get_error",
     "mbirgpu_session_cost", "mbirgpu_session_icd_iteration", "mbirgpu_session_forward_project",
     "mbirgpu_session_back_project", "mbirgpu_session_get_amatrix", "mbirgpu_session_get_detector_response",
-    "mbirgpu_session_run", "mbirgpu_session_forward_project_noalloc",
+    "mbirgpu_session_run", "mbirgpu_session_forward_project_noalloc", "mbirgpu_session_nh_select",
+    "mbirgpu_batch_create", "mbirgpu_batch_destroy", "mbirgpu_batch_run", "mbirgpu_batch_problem_info",
+    "mbirgpu_batch_get_object", "mbirgpu_batch_cost", "mbirgpu_reconstruct_batch",
     "phcontomo_reconstruct", "mbirgpu_pc_default_options", "mbirgpu_pc_session_create", "mbirgpu_pc_session_destroy",
     "mbirgpu_pc_fresnel", "mbirgpu_pc_paganin", "mbirgpu_pc_set_z", "mbirgpu_pc_init_admm", "mbirgpu_pc_set_state",
     "mbirgpu_pc_get_state", "mbirgpu_pc_sd_step", "mbirgpu_pc_nms_sweep", "mbirgpu_pc_run",
@@ -44,6 +46,7 @@ class Options(C.Structure):
         ("num_stages", C.c_int32), ("cost_rel_tol", C.c_double), ("zero_skipping", C.c_int32),
         ("write_files", C.c_int32), ("compute_cost", C.c_int32), ("refresh_every", C.c_int32),
         ("sv_size", C.c_int32), ("cta_warps", C.c_int32), ("icd_unroll", C.c_int32), ("seed", C.c_uint64),
+        ("nhicd_passes", C.c_int32), ("sv_colors", C.c_int32),
     ]
 
 
@@ -64,6 +67,7 @@ class SessionInfo(C.Structure):
         ("N_y", C.c_int32), ("N_z", C.c_int32), ("mult_xy", C.c_int32), ("mult_z", C.c_int32),
         ("max_views", C.c_int32), ("kmax", C.c_int32), ("sv_size", C.c_int32), ("cta_warps", C.c_int32),
         ("masked_columns", C.c_int64), ("nnz", C.c_int64), ("delta_t", C.c_double), ("device_bytes", C.c_size_t),
+        ("sv_colors", C.c_int32),
     ]
 
 
@@ -71,6 +75,14 @@ class IterStats(C.Structure):
     _fields_ = [
         ("voxel_updates", C.c_int64), ("zero_skipped", C.c_int64), ("sum_abs_update", C.c_double),
         ("sum_abs_value", C.c_double), ("kernel_ms", C.c_double), ("kernel_launches", C.c_int32),
+    ]
+
+
+class BatchStats(C.Structure):
+    _fields_ = [
+        ("voxel_updates", C.c_int64), ("device_ms", C.c_double), ("graph_launches", C.c_int32),
+        ("kernel_launches_per_iteration", C.c_int32), ("problems_converged", C.c_int32), ("sv_size", C.c_int32),
+        ("cta_warps", C.c_int32), ("sv_colors", C.c_int32),
     ]
 
 
@@ -112,6 +124,16 @@ def lib() -> C.CDLL:
         L.mbirgpu_session_forward_project.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         L.mbirgpu_session_back_project.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         L.mbirgpu_session_forward_project_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.mbirgpu_session_nh_select.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.mbirgpu_batch_create.argtypes = [C.POINTER(C.c_void_p), C.c_void_p, C.c_int32, C.POINTER(Options),
+                                           C.c_void_p]
+        L.mbirgpu_batch_destroy.argtypes = [C.c_void_p]
+        L.mbirgpu_batch_run.argtypes = [C.c_void_p, C.c_int32, C.POINTER(BatchStats)]
+        L.mbirgpu_batch_problem_info.argtypes = [C.c_void_p, C.c_int32, C.POINTER(SessionInfo),
+                                                 C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
+        L.mbirgpu_batch_get_object.argtypes = [C.c_void_p, C.c_int32, C.c_void_p]
+        L.mbirgpu_batch_cost.argtypes = [C.c_void_p, C.c_int32, C.POINTER(C.c_double)]
+        L.mbirgpu_reconstruct_batch.argtypes = [C.POINTER(C.POINTER(C.c_float)), C.c_void_p, C.c_int32, C.c_int32]
         L.mbirgpu_session_get_amatrix.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.mbirgpu_session_get_detector_response.argtypes = [C.c_void_p, C.c_void_p]
         L.mbirgpu_session_run.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.POINTER(C.c_int32),
@@ -303,6 +325,15 @@ class Session:
         enqueued on the session's stream, not waited for."""
         _check(lib().mbirgpu_session_forward_project_noalloc(self.h, C.c_void_p(object_dev), C.c_void_p(sino_dev)))
 
+    def nh_select(self, mag: np.ndarray) -> np.ndarray:
+        """NH-ICD voxel-line selection [N_time][N_y][N_x] (uint8) for an
+        update-magnitude map [N_time][N_y][N_x]."""
+        i = self.info
+        m = np.ascontiguousarray(mag, np.float32).reshape(i.N_time, i.N_y, i.N_x)
+        out = np.zeros((i.N_time, i.N_y, i.N_x), np.uint8)
+        _check(lib().mbirgpu_session_nh_select(self.h, m.ctypes.data, out.ctypes.data))
+        return out
+
     def back_project(self, sino: np.ndarray) -> np.ndarray:
         a = np.ascontiguousarray(sino, np.float32).reshape(self.sino_shape)
         out = np.zeros(self.shape, np.float32)
@@ -321,3 +352,76 @@ class Session:
         out = np.zeros((self.info.N_p, 65), np.float32)
         _check(lib().mbirgpu_session_get_detector_response(self.h, out.ctypes.data))
         return out
+
+
+def _problem_structs(problems):
+    keep = [pb.arrays() for pb in problems]
+    arr = (ProblemStruct * len(problems))()
+    for i, (pb, a) in enumerate(zip(problems, keep)):
+        arr[i] = ProblemStruct(*(x.ctypes.data for x in a), pb.proj_rows, pb.proj_cols, pb.proj_num, pb.recon_num,
+                               pb.vox_wid, pb.rot_center, pb.sig_s, pb.sig_t, pb.c_s, pb.c_t, pb.convg_thresh,
+                               pb.quad_convex, pb.huber_delta, pb.huber_T)
+    return arr, keep
+
+
+class Batch:
+    """Many independent problems resident together, iterated by one persistent
+    launch per colour phase captured as a CUDA graph (mbirgpu_batch_*)."""
+
+    def __init__(self, problems, options: Options | None = None, stream: int | None = None):
+        self._arr, self._keep = _problem_structs(problems)
+        self.problems = list(problems)
+        self.h = C.c_void_p()
+        opt = options if options is not None else get_options()
+        _check(lib().mbirgpu_batch_create(C.byref(self.h), C.cast(self._arr, C.c_void_p), len(problems),
+                                          C.byref(opt), C.c_void_p(stream or 0)))
+
+    def close(self):
+        if self.h:
+            lib().mbirgpu_batch_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def run(self, iterations: int) -> BatchStats:
+        st = BatchStats()
+        _check(lib().mbirgpu_batch_run(self.h, iterations, C.byref(st)))
+        return st
+
+    def info(self, i: int):
+        inf = SessionInfo()
+        it, conv = C.c_int32(), C.c_int32()
+        _check(lib().mbirgpu_batch_problem_info(self.h, i, C.byref(inf), C.byref(it), C.byref(conv)))
+        return inf, it.value, bool(conv.value)
+
+    def get_object(self, i: int) -> np.ndarray:
+        inf, _, _ = self.info(i)
+        a = np.zeros((inf.N_time, inf.N_z, inf.N_y, inf.N_x), np.float32)
+        _check(lib().mbirgpu_batch_get_object(self.h, i, a.ctypes.data))
+        return a
+
+    def cost(self, i: int) -> float:
+        c = C.c_double()
+        _check(lib().mbirgpu_batch_cost(self.h, i, C.byref(c)))
+        return c.value
+
+
+def reconstruct_batch(problems, iterations: int):
+    """mbirgpu_reconstruct_batch: every object in reconstruct()'s layout
+    [recon_num][proj_rows+2][proj_cols][proj_cols]."""
+    arr, keep = _problem_structs(problems)
+    outs = (C.POINTER(C.c_float) * len(problems))()
+    _check(lib().mbirgpu_reconstruct_batch(outs, C.cast(arr, C.c_void_p), len(problems), iterations))
+    libc = C.CDLL(None)
+    libc.free.argtypes = [C.c_void_p]
+    res = []
+    for pb, o in zip(problems, outs):
+        n = pb.recon_num * (pb.proj_rows + 2) * pb.proj_cols * pb.proj_cols
+        res.append(np.ctypeslib.as_array(o, shape=(n,)).copy().reshape(pb.recon_num, pb.proj_rows + 2, pb.proj_cols,
+                                                                        pb.proj_cols))
+        libc.free(C.cast(o, C.c_void_p))
+    return res

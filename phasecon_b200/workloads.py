@@ -9,6 +9,9 @@ detector, Poisson counts at I0 = 2e4, spatial + temporal qGGMRF with p = 1.2.
 I0 = 1e4, p = 1.1). Measurements are y = -log(N/I0), w = N, N ~ Poisson(I0
 e^{-Ax}) with A the reference's own system matrix (applied by the GPU forward
 projector, whose parity with the reference is tested).
+``config_batch`` is the batch of independent uneven 3-D problems: edges from
+{64, 96, 128, 192, 256}, slab depths 8-32 (even), 90-360 views, seeded random
+ellipsoid sets (0-0.02 per mm), Poisson I0 in [5e3, 5e4].
 ``config_pc`` is the phase-contrast scan: 40 random spheres (radius 5-40 um,
 refractive decrement delta in [1e-7, 5e-7], beta = delta / 100) in a 256 um
 cube at 1 um, 180 parallel-beam views over 180 deg on a 256x256 detector at
@@ -52,6 +55,24 @@ def config_3d(seed: int = 0, n_xy: int = 128, n_z: int = 16, views: int = 180):
     pb = Problem(zeros, np.ones_like(zeros), angles, times, recon_times, n_z, n_xy, views, 1, vox_wid=1.0,
                  rot_center=n_xy / 2, sig_s=0.01, sig_t=1.0, c_s=1.0, c_t=1.0, convg_thresh=0.0)
     return _measure(pb, obj, 1e4, seed), obj, 1.1
+
+
+def config_batch(seed: int = 0, n: int = 48, edges=(64, 96, 128, 192, 256), depth=(8, 32), views=(90, 360)):
+    """n independent 3-D problems of uneven size. Returns a list of Problem."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        n_xy = int(rng.choice(edges))
+        n_z = int(rng.integers(depth[0] // 2, depth[1] // 2 + 1)) * 2
+        nv = int(rng.integers(views[0], views[1] + 1))
+        I0 = float(rng.uniform(5e3, 5e4))
+        angles, times, recon_times = P.uniform_views(nv)
+        obj = P.random_ellipsoids(n_xy, n_z, seed * 1000 + i)[None]
+        zeros = np.zeros((nv, n_z, n_xy), np.float32)
+        pb = Problem(zeros, np.ones_like(zeros), angles, times, recon_times, n_z, n_xy, nv, 1, vox_wid=1.0,
+                     rot_center=n_xy / 2, sig_s=0.01, sig_t=1.0, c_s=1.0, c_t=1.0, convg_thresh=0.0)
+        out.append(_measure(pb, obj, I0, seed * 1000 + i))
+    return out
 
 
 def config_pc(seed: int = 0, n: int = 256, views: int = 180, spheres: int = 40, energy_kev: float = 20.0,

@@ -130,3 +130,21 @@ def test_live_reference_matches_fixture():
     geo = O.ref_geometry(pb)
     assert np.array_equal(geo["H_r"], GOLD["quad_H_r"])
     assert np.array_equal(O.ref_random2_sequence(1, 20) * 2147483647, GOLD["randlib_seed1"].astype(np.float64))
+
+
+NH_GOLD = np.load(os.path.join(os.path.dirname(__file__), "golden", "nhicd_reference.npz"))
+
+
+def test_vsc_selection_matches_reference_fixture():
+    """NH-ICD voxel-line selection (XT_NHICD.c:164-216): dense, sparse (ties at
+    zero) and quantised (ties) magnitude maps, square and non-square."""
+    for i in range(int(NH_GOLD["n"])):
+        got = O.vsc_select(NH_GOLD[f"mag{i}"], int(NH_GOLD[f"lines{i}"]))
+        assert np.array_equal(got, NH_GOLD[f"sel{i}"].astype(bool)), i
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference build not present")
+def test_live_reference_vsc_selection():
+    rng = np.random.default_rng(9)
+    m = rng.exponential(1.0, (48, 48)).astype(np.float32)
+    assert np.array_equal(O.vsc_select(m, 1500), O.ref_vsc_select(m, 1500))
