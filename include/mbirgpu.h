@@ -164,6 +164,16 @@ int mbirgpu_session_icd_iteration(mbirgpu_session *s, int32_t iter, mbirgpu_iter
 int mbirgpu_session_forward_project(mbirgpu_session *s, const float *object, float *sino);
 int mbirgpu_session_back_project(mbirgpu_session *s, const float *sino, float *object);
 
+/* Filtered back-projection of the measurements (Ram-Lak ramp filter, then
+ * the adjoint of the A matrix per frame, scaled by pi / views of the frame):
+ * the classical initial image. _fbp returns it ([N_time][N_z][N_y][N_x]);
+ * _set_object_fbp makes it the current object, zero outside the
+ * reconstruction circle like every object ICD works on (and recomputes e).
+ * The reference starts from zero or a restart file (initObject,
+ * MBIR_4D/XT_ICD_update.c:540-647); FBP has no counterpart there. */
+int mbirgpu_session_fbp(mbirgpu_session *s, float *object);
+int mbirgpu_session_set_object_fbp(mbirgpu_session *s);
+
 /* The NH-ICD voxel-line selection for a given update-magnitude map (for
  * inspection): mag [N_time][N_y][N_x] (sum over z of |update| of each voxel
  * column's latest visit, MagUpdateMap), sel [N_time][N_y][N_x] receives 1
@@ -240,6 +250,43 @@ int mbirgpu_batch_cost(mbirgpu_batch *b, int32_t i, double *total);
  * up to `iterations` iterations each; objects[i] receives a malloc'ed buffer in
  * reconstruct()'s layout [recon_num][proj_rows+2][proj_cols][proj_cols]. */
 int mbirgpu_reconstruct_batch(float **objects, const mbirgpu_problem *problems, int32_t n, int32_t iterations);
+
+/* --------------------------------------------------------------------------
+ * Learned warm start (no counterpart in the reference, which starts from zero
+ * or a restart file). A 3-D U-Net -- four levels of c, 2c, 4c, 8c channels,
+ * 3x3x3 convolutions with ReLU, 2x2x2 max-pooling, nearest upsampling with
+ * skip concatenation, a 1x1x1 head added to the input -- trained and run by
+ * the library's own BF16 tensor-core kernels (FP32 accumulation, FP32 master
+ * weights, Adam). It maps a filtered back-projection frame to a converged
+ * MBIR frame; ICD then runs to its usual convergence test from that image,
+ * so the network changes the starting point only, never the solution.
+ * Volumes are FP32 device arrays [D][H][W] with D, H, W multiples of 8.
+ * ------------------------------------------------------------------------ */
+typedef struct mbirgpu_unet mbirgpu_unet;
+
+int mbirgpu_unet_create(mbirgpu_unet **out, int32_t base_channels, uint64_t seed, void *stream);
+int mbirgpu_unet_destroy(mbirgpu_unet *u);
+int64_t mbirgpu_unet_num_params(const mbirgpu_unet *u);
+/* The network sees scale x input (values of order one) and returns
+ * input + correction / scale; default 1. */
+int mbirgpu_unet_set_input_scale(mbirgpu_unet *u, float scale);
+float mbirgpu_unet_get_input_scale(const mbirgpu_unet *u);
+/* Parameters (FP32 master copy), in layer order: per convolution the weights
+ * [27][C_in][C_out] then the biases [C_out]; the head's weights [c] and bias. */
+int mbirgpu_unet_get_params(mbirgpu_unet *u, float *params);
+int mbirgpu_unet_set_params(mbirgpu_unet *u, const float *params);
+int mbirgpu_unet_forward(mbirgpu_unet *u, const float *d_input, float *d_output, int32_t D, int32_t H, int32_t W);
+/* Loss mean((net(input) - target)^2) and its gradient w.r.t. every parameter
+ * (host, layer order as above; may be NULL). */
+int mbirgpu_unet_gradients(mbirgpu_unet *u, const float *d_input, const float *d_target, int32_t D, int32_t H,
+                           int32_t W, double *loss, float *grads);
+/* One Adam step (beta 0.9 / 0.999) on one (input, target) pair. */
+int mbirgpu_unet_train_step(mbirgpu_unet *u, const float *d_input, const float *d_target, int32_t D, int32_t H,
+                            int32_t W, float lr, double *loss);
+/* The session's object becomes the network applied to each frame of the
+ * filtered back-projection, zero outside the reconstruction circle; e = y - A x
+ * is recomputed. */
+int mbirgpu_session_set_object_unet(mbirgpu_session *s, mbirgpu_unet *u);
 
 /* --------------------------------------------------------------------------
  * Phase-contrast tomography (PCMBIR_3D): per-view phase retrieval.

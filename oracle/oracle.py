@@ -107,6 +107,7 @@ def build(with_reference: bool | None = None) -> None:
         with_reference = os.path.isdir("/root/reference/Source_Code/MBIR_4D")
     if with_reference:
         subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+        subprocess.run(["make", "-s", "-C", HERE, "ref_pc"], check=True)
 
 
 _orc = None

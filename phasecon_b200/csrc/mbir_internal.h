@@ -77,6 +77,16 @@ void launch_forward_project(const Geom &g, const uint32_t *d_table, const int32_
 void launch_back_project(const Geom &g, const uint32_t *d_table, const int32_t *d_view_first,
                          const int32_t *d_views, const float *d_sino, float *d_x, cudaStream_t st);
 
+// Filtered back-projection of d_y into d_x ([N_time][N_y][N_x][N_z]); d_q is a
+// sinogram-sized scratch for the ramp-filtered data. The ramp filter keeps one
+// view ([N_r][N_t] floats) in shared memory.
+void launch_fbp(const Geom &g, const uint32_t *d_table, const int32_t *d_view_first, const int32_t *d_views,
+                const float *d_y, float *d_q, float *d_x, cudaStream_t st);
+// Zero the voxel columns of d_x ([N_time][N_y][N_x][N_z]) outside the
+// reconstruction circle: ICD never updates them, and the reference keeps them 0.
+void launch_mask_object(const Geom &g, const uint8_t *d_mask, float *d_x, cudaStream_t st);
+inline bool fbp_supported(const Geom &g) { return ((size_t)g.N_r * g.N_t + 2 * (size_t)g.N_r) * 4 <= 200 * 1024; }
+
 // FP64 MAP cost: out[0] = data term, out[1] = prior term (device doubles).
 void launch_cost(const Geom &g, const float *d_err, const float *d_w, const float *d_x, double *d_partials,
                  int n_partials, double *d_out, cudaStream_t st);

@@ -480,6 +480,57 @@ int Session::back_project(const float *sino, float *obj)
     return 0;
 }
 
+int Session::fbp(float *obj)
+{
+    const Geom &g = hs.g;
+    if (!fbp_supported(g)) return fail("FBP: %d channels x %d rows per view exceed the filter's shared memory", g.N_r, g.N_t);
+    float *d_o = nullptr;
+    size_t acc = 0;
+    if (dalloc(&d_o, n_vox, &acc)) return -1;
+    launch_fbp(g, d_table, d_view_first, d_views, d_y, d_tmp, d_o, st);
+    launch_zfast_to_vol(d_o, d_tmp, g.N_time, g.N_z, g.N_y, g.N_x, st);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(obj, d_tmp, n_vox * sizeof(float), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(d_o);
+    if (e != cudaSuccess) return fail("filtered back-projection failed: %s", cudaGetErrorString(e));
+    return 0;
+}
+
+int Session::set_object_fbp()
+{
+    const Geom &g = hs.g;
+    if (!fbp_supported(g)) return fail("FBP: %d channels x %d rows per view exceed the filter's shared memory", g.N_r, g.N_t);
+    launch_fbp(g, d_table, d_view_first, d_views, d_y, d_tmp, d_x, st);
+    launch_mask_object(g, d_mask, d_x, st);
+    CK(cudaGetLastError());
+    return refresh_error();
+}
+
+int unet_apply_frames(UNet *u, float *d_vol, int N_time, int N_z, int N_y, int N_x);
+
+int Session::set_object_unet(UNet *u)
+{
+    const Geom &g = hs.g;
+    if (!fbp_supported(g)) return fail("FBP: %d channels x %d rows per view exceed the filter's shared memory", g.N_r, g.N_t);
+    float *d_v = nullptr;
+    size_t acc = 0;
+    if (dalloc(&d_v, n_vox, &acc)) return -1;
+    launch_fbp(g, d_table, d_view_first, d_views, d_y, d_tmp, d_x, st);
+    launch_zfast_to_vol(d_x, d_v, g.N_time, g.N_z, g.N_y, g.N_x, st);
+    cudaError_t e = cudaStreamSynchronize(st);  // the network runs on its own stream
+    int rc = e == cudaSuccess ? unet_apply_frames(u, d_v, g.N_time, g.N_z, g.N_y, g.N_x) : -1;
+    if (!rc) {
+        launch_vol_to_zfast(d_v, d_x, g.N_time, g.N_z, g.N_y, g.N_x, st);
+        launch_mask_object(g, d_mask, d_x, st);
+        rc = refresh_error();
+        e = cudaStreamSynchronize(st);
+    }
+    cudaFree(d_v);
+    if (e != cudaSuccess) return fail("warm start failed: %s", cudaGetErrorString(e));
+    return rc;
+}
+
 }  // namespace mbirgpu
 
 using mbirgpu::fail;
@@ -655,6 +706,26 @@ int mbirgpu_session_icd_iteration(mbirgpu_session *sp, int32_t iter, mbirgpu_ite
     SESSION(sp);
     if (iter < 1) return fail("iterations are numbered from 1");
     return s->icd_iteration(iter, stats);
+}
+
+int mbirgpu_session_fbp(mbirgpu_session *sp, float *object)
+{
+    SESSION(sp);
+    if (!object) return fail("NULL object");
+    return s->fbp(object);
+}
+
+int mbirgpu_session_set_object_fbp(mbirgpu_session *sp)
+{
+    SESSION(sp);
+    return s->set_object_fbp();
+}
+
+int mbirgpu_session_set_object_unet(mbirgpu_session *sp, mbirgpu_unet *u)
+{
+    SESSION(sp);
+    if (!u) return fail("U-Net pointer is NULL");
+    return s->set_object_unet(reinterpret_cast<mbirgpu::UNet *>(u));
 }
 
 int mbirgpu_session_nh_select(mbirgpu_session *sp, const float *mag, uint8_t *sel)

@@ -9,6 +9,7 @@ namespace mbirgpu {
 
 int fail(const char *fmt, ...);
 mbirgpu_options current_options();
+struct UNet;
 
 struct Session {
     HostSetup hs;
@@ -58,6 +59,9 @@ struct Session {
     int amatrix(int32_t *first, int32_t *count, float *values);
     int forward_project(const float *obj, float *sino);
     int back_project(const float *sino, float *obj);
+    int fbp(float *obj);              // host [N_time][N_z][N_y][N_x]
+    int set_object_fbp();             // x = FBP, then e = y - A x
+    int set_object_unet(UNet *u);     // x = U-Net(FBP) per frame, then e = y - A x
 };
 
 }  // namespace mbirgpu

@@ -1,0 +1,794 @@
+// Learned warm start: a 3-D U-Net trained and run by this library's own
+// kernels, mapping a filtered back-projection frame to a converged MBIR frame.
+//
+// Network (base width c, default 16): four levels of c, 2c, 4c, 8c channels;
+// each encoder level two 3x3x3 convolutions with ReLU, 2x2x2 max-pooling
+// between levels; each decoder level nearest 2x upsampling, a 3x3x3
+// convolution to the level's width, concatenation with the encoder skip, and
+// two 3x3x3 convolutions; a 1x1x1 head to one channel added to the input
+// (the network predicts the correction to the FBP image). Activations and
+// weights are BF16 ([voxel][channel], channels fastest), accumulation FP32,
+// master weights and Adam state FP32.
+//
+// Convolutions are implicit GEMMs on the tensor cores (mma.sync m16n8k16
+// BF16 -> FP32):
+//   forward   out[v][co] = sum_{tap, ci} in[v + off(tap)][ci] w[tap][ci][co]
+//             (M = voxels, N = co, K = 27 ci; zero padding);
+//   data grad the same kernel on the output gradient with the weights
+//             flipped in space and transposed in channels;
+//   weight grad dw[tap][ci][co] = sum_v in[v + off(tap)][ci] g[v][co]
+//             (M = ci, N = co, K = voxels, split over voxel chunks, FP32 atomics).
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <random>
+#include <string>
+#include <vector>
+
+#include "../../include/mbirgpu.h"
+#include "mbir_internal.h"
+
+namespace mbirgpu {
+
+int fail(const char *fmt, ...);
+
+namespace {
+
+using bf16 = __nv_bfloat16;
+
+__device__ __forceinline__ void mma_bf16(float (&c)[4], const uint32_t (&a)[4], const uint32_t (&b)[2])
+{
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+        "{%0, %1, %2, %3};"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+__device__ __forceinline__ uint32_t ld_pair(const bf16 *p) { return *reinterpret_cast<const uint32_t *>(p); }
+
+// voxel v of a D x H x W grid shifted by tap (dz, dy, dx in -1..1); -1 outside
+__device__ __forceinline__ long long shifted(long long v, int tap, int D, int H, int W)
+{
+    const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
+    const int x = (int)(v % W), y = (int)((v / W) % H), z = (int)(v / ((long long)W * H));
+    const int xx = x + dx, yy = y + dy, zz = z + dz;
+    if (xx < 0 || xx >= W || yy < 0 || yy >= H || zz < 0 || zz >= D) return -1;
+    return ((long long)zz * H + yy) * W + xx;
+}
+
+constexpr int kConvM = 128;  // voxels per CTA
+constexpr int kConvN = 64;   // output channels per CTA
+constexpr int kPadK = 24;    // shared-memory row stride (16 + 8) in bf16
+
+// out = act(conv3x3x3(in, w) + b); w is [27][Cin][Cout].
+__global__ void __launch_bounds__(128) conv_fwd_kernel(const bf16 *__restrict__ in, int Cin,
+                                                       const bf16 *__restrict__ w, const float *__restrict__ bias,
+                                                       bf16 *__restrict__ out, int Cout, int D, int H, int W,
+                                                       int relu)
+{
+    __shared__ __align__(16) bf16 As[kConvM][kPadK];
+    __shared__ __align__(16) bf16 Bs[kConvN][kPadK];
+    const long long V = (long long)D * H * W;
+    const long long m0 = (long long)blockIdx.x * kConvM;
+    const int n0 = blockIdx.y * kConvN;
+    const int NT = min(kConvN, Cout - n0);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, tig = lane & 3;
+    float acc[2][8][4];
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+        for (int j = 0; j < 8; j++)
+#pragma unroll
+            for (int q = 0; q < 4; q++) acc[i][j][q] = 0.0f;
+    const long long vm = m0 + threadIdx.x;  // the voxel this thread stages
+    for (int tap = 0; tap < 27; tap++) {
+        const long long src = vm < V ? shifted(vm, tap, D, H, W) : -1;
+        for (int c0 = 0; c0 < Cin; c0 += 16) {
+            // A: this thread's voxel, 16 channels
+            bf16 *arow = &As[threadIdx.x][0];
+            if (src >= 0 && c0 + 16 <= Cin) {
+                const uint4 *p = reinterpret_cast<const uint4 *>(in + src * Cin + c0);
+                reinterpret_cast<uint4 *>(arow)[0] = p[0];
+                reinterpret_cast<uint4 *>(arow)[1] = p[1];
+            } else {
+                for (int k = 0; k < 16; k++)
+                    arow[k] = (src >= 0 && c0 + k < Cin) ? in[src * Cin + c0 + k] : __float2bfloat16(0.0f);
+            }
+            // B (transposed): Bs[n][k] = w[tap][c0 + k][n0 + n]
+            for (int e = threadIdx.x; e < kConvN * 16; e += blockDim.x) {
+                const int k = e / kConvN, n = e % kConvN;
+                Bs[n][k] = (n < NT && c0 + k < Cin) ? w[((size_t)tap * Cin + c0 + k) * Cout + n0 + n]
+                                                    : __float2bfloat16(0.0f);
+            }
+            __syncthreads();
+#pragma unroll
+            for (int i = 0; i < 2; i++) {
+                const int r = warp * 32 + i * 16 + g;
+                const uint32_t a[4] = {ld_pair(&As[r][tig * 2]), ld_pair(&As[r + 8][tig * 2]),
+                                       ld_pair(&As[r][tig * 2 + 8]), ld_pair(&As[r + 8][tig * 2 + 8])};
+#pragma unroll
+                for (int j = 0; j < 8; j++) {
+                    if (j * 8 < NT) {
+                        const uint32_t b[2] = {ld_pair(&Bs[j * 8 + g][tig * 2]), ld_pair(&Bs[j * 8 + g][tig * 2 + 8])};
+                        mma_bf16(acc[i][j], a, b);
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            if (j * 8 >= NT) continue;
+            const int col = j * 8 + tig * 2;
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const long long v = m0 + warp * 32 + i * 16 + g + h * 8;
+                if (v >= V) continue;
+                for (int q = 0; q < 2; q++) {
+                    if (col + q >= NT) continue;
+                    float val = acc[i][j][h * 2 + q] + (bias ? bias[n0 + col + q] : 0.0f);
+                    if (relu) val = fmaxf(val, 0.0f);
+                    out[v * Cout + n0 + col + q] = __float2bfloat16(val);
+                }
+            }
+        }
+}
+
+constexpr int kWgChunk = 1024;  // voxels per CTA of the weight gradient
+
+// dw[tap][ci][co] += sum_v in[v + off(tap)][ci] g[v][co]; CTA tile 32 ci x 64 co.
+__global__ void __launch_bounds__(128) conv_wgrad_kernel(const bf16 *__restrict__ in, int Cin,
+                                                         const bf16 *__restrict__ gout, int Cout,
+                                                         float *__restrict__ dw, int D, int H, int W)
+{
+    __shared__ __align__(16) bf16 As[32][kPadK];  // [ci][k]
+    __shared__ __align__(16) bf16 Bs[64][kPadK];  // [co][k]
+    const long long V = (long long)D * H * W;
+    const long long v0 = (long long)blockIdx.x * kWgChunk;
+    const int tap = blockIdx.y;
+    const int nco = (Cout + 63) / 64;
+    const int ci0 = (blockIdx.z / nco) * 32, co0 = (blockIdx.z % nco) * 64;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, tig = lane & 3;
+    const int mt = warp & 1, nh = warp >> 1;  // m16 tile, half of the 64 columns
+    float acc[4][4];
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+#pragma unroll
+        for (int q = 0; q < 4; q++) acc[j][q] = 0.0f;
+    for (long long k0 = v0; k0 < min(V, v0 + kWgChunk); k0 += 16) {
+        for (int e = threadIdx.x; e < 32 * 16; e += blockDim.x) {
+            const int ci = e % 32, k = e / 32;
+            const long long v = k0 + k;
+            const long long s = v < V ? shifted(v, tap, D, H, W) : -1;
+            As[ci][k] = (s >= 0 && ci0 + ci < Cin) ? in[s * Cin + ci0 + ci] : __float2bfloat16(0.0f);
+        }
+        for (int e = threadIdx.x; e < 64 * 16; e += blockDim.x) {
+            const int co = e % 64, k = e / 64;
+            const long long v = k0 + k;
+            Bs[co][k] = (v < V && co0 + co < Cout) ? gout[v * Cout + co0 + co] : __float2bfloat16(0.0f);
+        }
+        __syncthreads();
+        const int r = mt * 16 + g;
+        const uint32_t a[4] = {ld_pair(&As[r][tig * 2]), ld_pair(&As[r + 8][tig * 2]), ld_pair(&As[r][tig * 2 + 8]),
+                               ld_pair(&As[r + 8][tig * 2 + 8])};
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const int n = nh * 32 + j * 8 + g;
+            const uint32_t b[2] = {ld_pair(&Bs[n][tig * 2]), ld_pair(&Bs[n][tig * 2 + 8])};
+            mma_bf16(acc[j], a, b);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+#pragma unroll
+        for (int h = 0; h < 2; h++)
+#pragma unroll
+            for (int q = 0; q < 2; q++) {
+                const int ci = ci0 + mt * 16 + g + h * 8, co = co0 + nh * 32 + j * 8 + tig * 2 + q;
+                if (ci < Cin && co < Cout) atomicAdd(&dw[((size_t)tap * Cin + ci) * Cout + co], acc[j][h * 2 + q]);
+            }
+}
+
+// db[co] += sum_v g[v][co]
+__global__ void bias_grad_kernel(const bf16 *__restrict__ g, long long V, int C, float *__restrict__ db)
+{
+    const int c = threadIdx.x % C, lanes = blockDim.x / C;
+    float s = 0.0f;
+    for (long long v = blockIdx.x * (long long)lanes + threadIdx.x / C; v < V && threadIdx.x < lanes * C;
+         v += (long long)gridDim.x * lanes)
+        s += __bfloat162float(g[v * C + c]);
+    if (threadIdx.x < lanes * C) atomicAdd(&db[c], s);
+}
+
+// wt[26 - tap][co][ci] = w[tap][ci][co] (the data-gradient weights)
+__global__ void flip_weights_kernel(const bf16 *__restrict__ w, int Cin, int Cout, int taps, bf16 *__restrict__ wt)
+{
+    const long long n = (long long)taps * Cin * Cout;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int co = (int)(i % Cout), ci = (int)((i / Cout) % Cin), tap = (int)(i / ((long long)Cout * Cin));
+        wt[((size_t)(taps - 1 - tap) * Cout + co) * Cin + ci] = w[i];
+    }
+}
+
+__global__ void relu_grad_kernel(bf16 *__restrict__ g, const bf16 *__restrict__ act, long long n)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        if (!(__bfloat162float(act[i]) > 0.0f)) g[i] = __float2bfloat16(0.0f);
+}
+
+// 2x2x2 max-pooling of a D x H x W grid (even sizes)
+__global__ void maxpool_kernel(const bf16 *__restrict__ in, int C, int D, int H, int W, bf16 *__restrict__ out)
+{
+    const int d = D / 2, h = H / 2, w = W / 2;
+    const long long n = (long long)d * h * w * C;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int c = (int)(i % C);
+        const long long vo = i / C;
+        const int x = (int)(vo % w), y = (int)((vo / w) % h), z = (int)(vo / ((long long)w * h));
+        float m = -INFINITY;
+        for (int q = 0; q < 8; q++) {
+            const long long vi = ((long long)(2 * z + (q >> 2)) * H + 2 * y + ((q >> 1) & 1)) * W + 2 * x + (q & 1);
+            m = fmaxf(m, __bfloat162float(in[vi * C + c]));
+        }
+        out[i] = __float2bfloat16(m);
+    }
+}
+
+// the gradient goes to the first input of each 2x2x2 block that holds the max
+__global__ void maxpool_grad_kernel(const bf16 *__restrict__ in, const bf16 *__restrict__ out,
+                                    const bf16 *__restrict__ gout, int C, int D, int H, int W, bf16 *__restrict__ gin,
+                                    int accumulate)
+{
+    const int d = D / 2, h = H / 2, w = W / 2;
+    const long long n = (long long)d * h * w * C;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int c = (int)(i % C);
+        const long long vo = i / C;
+        const int x = (int)(vo % w), y = (int)((vo / w) % h), z = (int)(vo / ((long long)w * h));
+        const float m = __bfloat162float(out[i]), gv = __bfloat162float(gout[i]);
+        bool done = false;
+        for (int q = 0; q < 8; q++) {
+            const long long vi = ((long long)(2 * z + (q >> 2)) * H + 2 * y + ((q >> 1) & 1)) * W + 2 * x + (q & 1);
+            const bool hit = !done && __bfloat162float(in[vi * C + c]) == m;
+            done |= hit;
+            const float add = hit ? gv : 0.0f;
+            gin[vi * C + c] = __float2bfloat16(accumulate ? __bfloat162float(gin[vi * C + c]) + add : add);
+        }
+    }
+}
+
+// nearest 2x upsampling of a d x h x w grid to 2d x 2h x 2w
+__global__ void upsample_kernel(const bf16 *__restrict__ in, int C, int d, int h, int w, bf16 *__restrict__ out)
+{
+    const int D = 2 * d, H = 2 * h, W = 2 * w;
+    const long long n = (long long)D * H * W * C;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int c = (int)(i % C);
+        const long long v = i / C;
+        const int x = (int)(v % W), y = (int)((v / W) % H), z = (int)(v / ((long long)W * H));
+        out[i] = in[(((long long)(z / 2) * h + y / 2) * w + x / 2) * C + c];
+    }
+}
+
+__global__ void upsample_grad_kernel(const bf16 *__restrict__ gout, int C, int d, int h, int w, bf16 *__restrict__ gin)
+{
+    const int H = 2 * h, W = 2 * w;
+    const long long n = (long long)d * h * w * C;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int c = (int)(i % C);
+        const long long v = i / C;
+        const int x = (int)(v % w), y = (int)((v / w) % h), z = (int)(v / ((long long)w * h));
+        float s = 0.0f;
+        for (int q = 0; q < 8; q++)
+            s += __bfloat162float(
+                gout[(((long long)(2 * z + (q >> 2)) * H + 2 * y + ((q >> 1) & 1)) * W + 2 * x + (q & 1)) * C + c]);
+        gin[i] = __float2bfloat16(s);
+    }
+}
+
+// cat[v] = [a[v] (Ca channels), b[v] (Cb channels)]
+__global__ void concat_kernel(const bf16 *__restrict__ a, int Ca, const bf16 *__restrict__ b, int Cb, long long V,
+                              bf16 *__restrict__ cat)
+{
+    const int C = Ca + Cb;
+    const long long n = V * C;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int c = (int)(i % C);
+        const long long v = i / C;
+        cat[i] = c < Ca ? a[v * Ca + c] : b[v * Cb + c - Ca];
+    }
+}
+
+// ga = gcat[:, :Ca]; gb += gcat[:, Ca:]
+__global__ void split_grad_kernel(const bf16 *__restrict__ gcat, int Ca, int Cb, long long V, bf16 *__restrict__ ga,
+                                  bf16 *__restrict__ gb)
+{
+    const int C = Ca + Cb;
+    const long long n = V * C;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int c = (int)(i % C);
+        const long long v = i / C;
+        if (c < Ca) ga[v * Ca + c] = gcat[i];
+        else gb[v * Cb + c - Ca] = __float2bfloat16(__bfloat162float(gb[v * Cb + c - Ca]) + __bfloat162float(gcat[i]));
+    }
+}
+
+// y = bf16(s x): the network sees the input scaled to values of order one
+__global__ void to_bf16_kernel(const float *__restrict__ x, long long n, float s, bf16 *__restrict__ y)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        y[i] = __float2bfloat16(s * x[i]);
+}
+
+// out[v] = in[v] + (b + sum_c w[c] x[v][c]) / s  (1x1x1 head, FP32 output, residual over the input)
+__global__ void head_kernel(const bf16 *__restrict__ x, int C, const float *__restrict__ w, const float *__restrict__ b,
+                            const float *__restrict__ in, long long V, float inv_s, float *__restrict__ out)
+{
+    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < V; v += (long long)gridDim.x * blockDim.x) {
+        float s = b[0];
+        for (int c = 0; c < C; c++) s += w[c] * __bfloat162float(x[v * C + c]);
+        out[v] = in[v] + s * inv_s;
+    }
+}
+
+// loss = mean (out - t)^2 (FP64 sum), g = 2 (out - t) / V; head grads: gx[v][c] = g w[c] / s,
+// dw[c] += sum_v g x[v][c] / s, db += sum_v g / s.
+__global__ void loss_head_grad_kernel(const float *__restrict__ out, const float *__restrict__ t, long long V,
+                                      const bf16 *__restrict__ x, int C, const float *__restrict__ w, float inv_s,
+                                      bf16 *__restrict__ gx, float *__restrict__ dw, float *__restrict__ db,
+                                      double *__restrict__ loss)
+{
+    __shared__ float s_dw[128];
+    __shared__ float s_db;
+    __shared__ double s_loss;
+    for (int c = threadIdx.x; c < C; c += blockDim.x) s_dw[c] = 0.0f;
+    if (threadIdx.x == 0) {
+        s_db = 0.0f;
+        s_loss = 0.0;
+    }
+    __syncthreads();
+    double l = 0.0;
+    float lb = 0.0f;
+    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < V; v += (long long)gridDim.x * blockDim.x) {
+        const float d = out[v] - t[v];
+        l += (double)d * d;
+        const float g = 2.0f * d / (float)V * inv_s;
+        lb += g;
+        for (int c = 0; c < C; c++) {
+            const float xv = __bfloat162float(x[v * C + c]);
+            gx[v * C + c] = __float2bfloat16(g * w[c]);
+            atomicAdd(&s_dw[c], g * xv);
+        }
+    }
+    atomicAdd(&s_db, lb);
+    atomicAdd(&s_loss, l / (double)V);
+    __syncthreads();
+    for (int c = threadIdx.x; c < C; c += blockDim.x) atomicAdd(&dw[c], s_dw[c]);
+    if (threadIdx.x == 0) {
+        atomicAdd(db, s_db);
+        atomicAdd(loss, s_loss);
+    }
+}
+
+// Adam on FP32 master weights; refreshes the BF16 copy.
+__global__ void adam_kernel(float *__restrict__ p, const float *__restrict__ g, float *__restrict__ m,
+                            float *__restrict__ v, long long n, float lr, float b1, float b2, float eps, float c1,
+                            float c2, bf16 *__restrict__ pb)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const float gi = g[i];
+        const float mi = b1 * m[i] + (1.0f - b1) * gi;
+        const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        const float pi = p[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+        p[i] = pi;
+        pb[i] = __float2bfloat16(pi);
+    }
+}
+
+__global__ void copy_to_bf16_kernel(const float *__restrict__ p, long long n, bf16 *__restrict__ pb)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        pb[i] = __float2bfloat16(p[i]);
+}
+
+inline unsigned grid_for(long long n, int threads = 256)
+{
+    return (unsigned)std::max<long long>(1, std::min<long long>((n + threads - 1) / threads, 148LL * 32));
+}
+
+}  // namespace
+
+// --------------------------------------------------------------------------------------------------------------
+struct UNet {
+    int c = 16;
+    struct Conv {
+        int cin, cout;
+        size_t w, b;  // offsets into the parameter arrays (FP32 master / BF16 copy)
+    };
+    std::vector<Conv> convs;  // 17 convolutions in forward order
+    size_t head_w = 0, head_b = 0, n_params = 0;
+    float *d_p = nullptr, *d_g = nullptr, *d_m = nullptr, *d_v = nullptr;
+    bf16 *d_pb = nullptr, *d_wt = nullptr;  // BF16 copy; flipped weights scratch
+    long long steps = 0;
+    float scale = 1.0f;  // input scale: the network sees scale x input
+    cudaStream_t st = nullptr;
+
+    // activations and gradients for one grid size
+    int D = 0, H = 0, W = 0;
+    std::vector<void *> bufs;
+    bf16 *x0 = nullptr;
+    bf16 *act[4][2] = {};  // encoder level l: conv a, conv b (= skip)
+    bf16 *pool[3] = {};    // pooled encoder output of level l (input of level l+1)
+    bf16 *up[3] = {}, *u[3] = {}, *cat[3] = {}, *dec[3][2] = {};
+    bf16 *gact[4][2] = {}, *gpool[3] = {}, *gup[3] = {}, *gu[3] = {}, *gcat[3] = {}, *gdec[3][2] = {};
+    float *out = nullptr;
+    double *d_loss = nullptr;
+
+    ~UNet()
+    {
+        free_acts();
+        for (void *p : {(void *)d_p, (void *)d_g, (void *)d_m, (void *)d_v, (void *)d_pb, (void *)d_wt,
+                        (void *)d_loss})
+            if (p) cudaFree(p);
+    }
+    void free_acts()
+    {
+        for (void *p : bufs) cudaFree(p);
+        bufs.clear();
+        D = H = W = 0;
+    }
+    int init(int base, uint64_t seed);
+    int ensure(int d, int h, int w);
+    long long vox(int l) const { return (long long)(D >> l) * (H >> l) * (W >> l); }
+    void conv(int i, const bf16 *in, bf16 *o, int l, bool relu);
+    void conv_back(int i, const bf16 *in, const bf16 *o, bf16 *go, bf16 *gin, int l);
+    int forward(const float *d_in);
+    int backward(const float *d_target, double *loss);
+    int step(float lr);
+};
+
+int UNet::init(int base, uint64_t seed)
+{
+    if (base < 4 || base > 16 || base % 4) return fail("U-Net base width must be 4, 8, 12 or 16 (got %d)", base);
+    c = base;
+    size_t off = 0;
+    auto add = [&](int cin, int cout) {
+        Conv k{cin, cout, off, 0};
+        off += (size_t)27 * cin * cout;
+        k.b = off;
+        off += cout;
+        convs.push_back(k);
+    };
+    const int C[4] = {c, 2 * c, 4 * c, 8 * c};
+    for (int l = 0; l < 4; l++) {
+        add(l == 0 ? 1 : C[l - 1], C[l]);
+        add(C[l], C[l]);
+    }
+    for (int l = 2; l >= 0; l--) {
+        add(C[l + 1], C[l]);
+        add(2 * C[l], C[l]);
+        add(C[l], C[l]);
+    }
+    head_w = off;
+    off += c;
+    head_b = off;
+    off += 1;
+    n_params = off;
+    // He-normal initialisation (seeded), zero biases; a small head keeps the
+    // initial output close to the input
+    std::vector<float> h(n_params, 0.0f);
+    std::mt19937_64 rng(seed);
+    for (auto &k : convs) {
+        std::normal_distribution<float> nd(0.0f, std::sqrt(2.0f / (27.0f * k.cin)));
+        for (size_t i = 0; i < (size_t)27 * k.cin * k.cout; i++) h[k.w + i] = nd(rng);
+    }
+    std::normal_distribution<float> nh(0.0f, 1e-3f);
+    for (int i = 0; i < c; i++) h[head_w + i] = nh(rng);
+    cudaError_t e = cudaSuccess;
+    for (float **p : {&d_p, &d_g, &d_m, &d_v})
+        if (e == cudaSuccess) e = cudaMalloc((void **)p, n_params * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc((void **)&d_pb, n_params * sizeof(bf16));
+    size_t wt = 0;
+    for (auto &k : convs) wt = std::max(wt, (size_t)27 * k.cin * k.cout);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&d_wt, wt * sizeof(bf16));
+    if (e == cudaSuccess) e = cudaMalloc((void **)&d_loss, sizeof(double));
+    if (e == cudaSuccess) e = cudaMemcpy(d_p, h.data(), n_params * sizeof(float), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(d_m, 0, n_params * sizeof(float));
+    if (e == cudaSuccess) e = cudaMemset(d_v, 0, n_params * sizeof(float));
+    if (e != cudaSuccess) return fail("U-Net allocation failed: %s", cudaGetErrorString(e));
+    copy_to_bf16_kernel<<<grid_for((long long)n_params), 256, 0, st>>>(d_p, (long long)n_params, d_pb);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    return e == cudaSuccess ? 0 : fail("U-Net init failed: %s", cudaGetErrorString(e));
+}
+
+int UNet::ensure(int d, int h, int w)
+{
+    if (d == D && h == H && w == W) return 0;
+    if (d % 8 || h % 8 || w % 8 || d < 8 || h < 8 || w < 8)
+        return fail("U-Net grid sizes must be multiples of 8 (got %d x %d x %d)", d, h, w);
+    free_acts();
+    D = d;
+    H = h;
+    W = w;
+    const int C[4] = {c, 2 * c, 4 * c, 8 * c};
+    cudaError_t e = cudaSuccess;
+    auto alloc = [&](bf16 **p, long long n) {
+        if (e != cudaSuccess) return;
+        e = cudaMalloc((void **)p, (size_t)n * sizeof(bf16));
+        if (e == cudaSuccess) bufs.push_back(*p);
+    };
+    alloc(&x0, vox(0));
+    for (int l = 0; l < 4; l++)
+        for (int k = 0; k < 2; k++) {
+            alloc(&act[l][k], vox(l) * C[l]);
+            alloc(&gact[l][k], vox(l) * C[l]);
+        }
+    for (int l = 0; l < 3; l++) {
+        alloc(&pool[l], vox(l + 1) * C[l]);
+        alloc(&gpool[l], vox(l + 1) * C[l]);
+        alloc(&up[l], vox(l) * C[l + 1]);
+        alloc(&gup[l], vox(l) * C[l + 1]);
+        alloc(&u[l], vox(l) * C[l]);
+        alloc(&gu[l], vox(l) * C[l]);
+        alloc(&cat[l], vox(l) * 2 * C[l]);
+        alloc(&gcat[l], vox(l) * 2 * C[l]);
+        for (int k = 0; k < 2; k++) {
+            alloc(&dec[l][k], vox(l) * C[l]);
+            alloc(&gdec[l][k], vox(l) * C[l]);
+        }
+    }
+    if (e == cudaSuccess) {
+        e = cudaMalloc((void **)&out, (size_t)vox(0) * sizeof(float));
+        if (e == cudaSuccess) bufs.push_back(out);
+    }
+    if (e != cudaSuccess) {
+        free_acts();
+        return fail("U-Net activation allocation failed: %s", cudaGetErrorString(e));
+    }
+    return 0;
+}
+
+void UNet::conv(int i, const bf16 *in, bf16 *o, int l, bool relu)
+{
+    const Conv &k = convs[i];
+    dim3 grid((unsigned)((vox(l) + kConvM - 1) / kConvM), (unsigned)((k.cout + kConvN - 1) / kConvN));
+    conv_fwd_kernel<<<grid, 128, 0, st>>>(in, k.cin, d_pb + k.w, d_p + k.b, o, k.cout, D >> l, H >> l, W >> l,
+                                          relu ? 1 : 0);
+}
+
+// o = relu(conv(in)); go: gradient w.r.t. o (overwritten by the ReLU mask);
+// gin (may be null): gradient w.r.t. in.
+void UNet::conv_back(int i, const bf16 *in, const bf16 *o, bf16 *go, bf16 *gin, int l)
+{
+    const Conv &k = convs[i];
+    const long long V = vox(l);
+    relu_grad_kernel<<<grid_for(V * k.cout), 256, 0, st>>>(go, o, V * k.cout);
+    const int nci = (k.cin + 31) / 32, nco = (k.cout + 63) / 64;
+    dim3 gw((unsigned)((V + kWgChunk - 1) / kWgChunk), 27, (unsigned)(nci * nco));
+    conv_wgrad_kernel<<<gw, 128, 0, st>>>(in, k.cin, go, k.cout, d_g + k.w, D >> l, H >> l, W >> l);
+    const int lanes = std::max(1, 256 / k.cout);
+    bias_grad_kernel<<<grid_for(V, lanes), lanes * k.cout, 0, st>>>(go, V, k.cout, d_g + k.b);
+    if (gin) {
+        flip_weights_kernel<<<grid_for((long long)27 * k.cin * k.cout), 256, 0, st>>>(d_pb + k.w, k.cin, k.cout, 27,
+                                                                                    d_wt);
+        dim3 grid((unsigned)((V + kConvM - 1) / kConvM), (unsigned)((k.cin + kConvN - 1) / kConvN));
+        conv_fwd_kernel<<<grid, 128, 0, st>>>(go, k.cout, d_wt, nullptr, gin, k.cin, D >> l, H >> l, W >> l, 0);
+    }
+}
+
+int UNet::forward(const float *d_in)
+{
+    const int C[4] = {c, 2 * c, 4 * c, 8 * c};
+    to_bf16_kernel<<<grid_for(vox(0)), 256, 0, st>>>(d_in, vox(0), scale, x0);
+    int ci = 0;
+    const bf16 *x = x0;
+    for (int l = 0; l < 4; l++) {
+        conv(ci++, x, act[l][0], l, true);
+        conv(ci++, act[l][0], act[l][1], l, true);
+        if (l < 3) {
+            maxpool_kernel<<<grid_for(vox(l + 1) * C[l]), 256, 0, st>>>(act[l][1], C[l], D >> l, H >> l, W >> l,
+                                                                        pool[l]);
+            x = pool[l];
+        }
+    }
+    const bf16 *y = act[3][1];
+    for (int l = 2; l >= 0; l--) {
+        upsample_kernel<<<grid_for(vox(l) * C[l + 1]), 256, 0, st>>>(y, C[l + 1], D >> (l + 1), H >> (l + 1),
+                                                                     W >> (l + 1), up[l]);
+        conv(ci++, up[l], u[l], l, true);
+        concat_kernel<<<grid_for(vox(l) * 2 * C[l]), 256, 0, st>>>(u[l], C[l], act[l][1], C[l], vox(l), cat[l]);
+        conv(ci++, cat[l], dec[l][0], l, true);
+        conv(ci++, dec[l][0], dec[l][1], l, true);
+        y = dec[l][1];
+    }
+    head_kernel<<<grid_for(vox(0)), 256, 0, st>>>(y, c, d_p + head_w, d_p + head_b, d_in, vox(0), 1.0f / scale, out);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? 0 : fail("U-Net forward failed: %s", cudaGetErrorString(e));
+}
+
+// Gradients of mean((out - target)^2) after forward(); the reverse of forward's order.
+int UNet::backward(const float *d_target, double *loss)
+{
+    const int C[4] = {c, 2 * c, 4 * c, 8 * c};
+    cudaError_t e = cudaMemsetAsync(d_g, 0, n_params * sizeof(float), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_loss, 0, sizeof(double), st);
+    if (e != cudaSuccess) return fail("U-Net backward failed: %s", cudaGetErrorString(e));
+    loss_head_grad_kernel<<<grid_for(vox(0)), 256, 0, st>>>(out, d_target, vox(0), dec[0][1], c, d_p + head_w,
+                                                            1.0f / scale, gdec[0][1], d_g + head_w, d_g + head_b,
+                                                            d_loss);
+    int ci = (int)convs.size() - 1;
+    // decoder, finest level first
+    for (int l = 0; l <= 2; l++) {
+        const int i2 = ci--, i1 = ci--, iu = ci--;
+        conv_back(i2, dec[l][0], dec[l][1], gdec[l][1], gdec[l][0], l);
+        conv_back(i1, cat[l], dec[l][0], gdec[l][0], gcat[l], l);
+        // split: the upsampled branch's gradient; the skip's gradient starts here
+        cudaMemsetAsync(gact[l][1], 0, (size_t)vox(l) * C[l] * sizeof(bf16), st);
+        split_grad_kernel<<<grid_for(vox(l) * 2 * C[l]), 256, 0, st>>>(gcat[l], C[l], C[l], vox(l), gu[l],
+                                                                       gact[l][1]);
+        conv_back(iu, up[l], u[l], gu[l], gup[l], l);
+        bf16 *gy = (l == 2) ? gact[3][1] : gdec[l + 1][1];
+        upsample_grad_kernel<<<grid_for(vox(l + 1) * C[l + 1]), 256, 0, st>>>(gup[l], C[l + 1], D >> (l + 1),
+                                                                              H >> (l + 1), W >> (l + 1), gy);
+    }
+    // encoder, deepest level first
+    for (int l = 3; l >= 0; l--) {
+        const int ib = ci--, ia = ci--;
+        if (l < 3)  // the pooled output's gradient adds to the skip's
+            maxpool_grad_kernel<<<grid_for(vox(l + 1) * C[l]), 256, 0, st>>>(act[l][1], pool[l], gpool[l], C[l],
+                                                                             D >> l, H >> l, W >> l, gact[l][1], 1);
+        conv_back(ib, act[l][0], act[l][1], gact[l][1], gact[l][0], l);
+        bf16 *gx = l > 0 ? gpool[l - 1] : nullptr;
+        conv_back(ia, l > 0 ? pool[l - 1] : x0, act[l][0], gact[l][0], gx, l);
+    }
+    e = cudaGetLastError();
+    if (e == cudaSuccess && loss) e = cudaMemcpyAsync(loss, d_loss, sizeof(double), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess && loss) e = cudaStreamSynchronize(st);
+    return e == cudaSuccess ? 0 : fail("U-Net backward failed: %s", cudaGetErrorString(e));
+}
+
+int UNet::step(float lr)
+{
+    steps++;
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float c1 = 1.0f - std::pow(b1, (float)steps), c2 = 1.0f - std::pow(b2, (float)steps);
+    adam_kernel<<<grid_for((long long)n_params), 256, 0, st>>>(d_p, d_g, d_m, d_v, (long long)n_params, lr, b1, b2,
+                                                               1e-8f, c1, c2, d_pb);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? 0 : fail("U-Net update failed: %s", cudaGetErrorString(e));
+}
+
+// The network applied to every frame of a volume [N_time][N_z][N_y][N_x]
+// (FP32, device), in place; completes before returning.
+int unet_apply_frames(UNet *u, float *d_vol, int N_time, int N_z, int N_y, int N_x)
+{
+    if (u->ensure(N_z, N_y, N_x)) return -1;
+    const size_t frame = (size_t)N_z * N_y * N_x;
+    for (int f = 0; f < N_time; f++) {
+        if (u->forward(d_vol + f * frame)) return -1;
+        cudaError_t e = cudaMemcpyAsync(d_vol + f * frame, u->out, frame * sizeof(float), cudaMemcpyDeviceToDevice,
+                                        u->st);
+        if (e != cudaSuccess) return fail("copy failed: %s", cudaGetErrorString(e));
+    }
+    cudaError_t e = cudaStreamSynchronize(u->st);
+    return e == cudaSuccess ? 0 : fail("U-Net inference failed: %s", cudaGetErrorString(e));
+}
+
+}  // namespace mbirgpu
+
+using mbirgpu::fail;
+using mbirgpu::UNet;
+
+#define UNETP(up)                                    \
+    if (!(up)) return fail("U-Net pointer is NULL"); \
+    UNet *u = reinterpret_cast<UNet *>(up)
+
+extern "C" {
+
+int mbirgpu_unet_create(mbirgpu_unet **out, int32_t base_channels, uint64_t seed, void *stream)
+{
+    if (!out) return fail("NULL argument");
+    *out = nullptr;
+    UNet *u = new (std::nothrow) UNet();
+    if (!u) return fail("out of host memory");
+    u->st = (cudaStream_t)stream;
+    if (u->init(base_channels, seed)) {
+        std::string why = mbirgpu_last_error();
+        delete u;
+        fail("%s", why.c_str());
+        return -1;
+    }
+    *out = reinterpret_cast<mbirgpu_unet *>(u);
+    return 0;
+}
+
+int mbirgpu_unet_destroy(mbirgpu_unet *up)
+{
+    delete reinterpret_cast<UNet *>(up);
+    return 0;
+}
+
+int64_t mbirgpu_unet_num_params(const mbirgpu_unet *up)
+{
+    return up ? (int64_t)reinterpret_cast<const UNet *>(up)->n_params : 0;
+}
+
+int mbirgpu_unet_set_input_scale(mbirgpu_unet *up, float scale)
+{
+    UNETP(up);
+    if (!(scale > 0.0f)) return fail("the input scale must be positive");
+    u->scale = scale;
+    return 0;
+}
+
+float mbirgpu_unet_get_input_scale(const mbirgpu_unet *up)
+{
+    return up ? reinterpret_cast<const UNet *>(up)->scale : 0.0f;
+}
+
+int mbirgpu_unet_get_params(mbirgpu_unet *up, float *params)
+{
+    UNETP(up);
+    if (!params) return fail("NULL argument");
+    cudaError_t e = cudaMemcpy(params, u->d_p, u->n_params * sizeof(float), cudaMemcpyDeviceToHost);
+    return e == cudaSuccess ? 0 : fail("copy failed: %s", cudaGetErrorString(e));
+}
+
+int mbirgpu_unet_set_params(mbirgpu_unet *up, const float *params)
+{
+    UNETP(up);
+    if (!params) return fail("NULL argument");
+    cudaError_t e = cudaMemcpy(u->d_p, params, u->n_params * sizeof(float), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return fail("copy failed: %s", cudaGetErrorString(e));
+    mbirgpu::copy_to_bf16_kernel<<<mbirgpu::grid_for((long long)u->n_params), 256, 0, u->st>>>(
+        u->d_p, (long long)u->n_params, u->d_pb);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(u->st);
+    return e == cudaSuccess ? 0 : fail("U-Net parameter upload failed: %s", cudaGetErrorString(e));
+}
+
+int mbirgpu_unet_forward(mbirgpu_unet *up, const float *d_input, float *d_output, int32_t D, int32_t H, int32_t W)
+{
+    UNETP(up);
+    if (!d_input || !d_output) return fail("NULL argument");
+    if (u->ensure(D, H, W) || u->forward(d_input)) return -1;
+    cudaError_t e = cudaMemcpyAsync(d_output, u->out, (size_t)D * H * W * sizeof(float), cudaMemcpyDeviceToDevice,
+                                    u->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(u->st);
+    return e == cudaSuccess ? 0 : fail("U-Net forward failed: %s", cudaGetErrorString(e));
+}
+
+int mbirgpu_unet_gradients(mbirgpu_unet *up, const float *d_input, const float *d_target, int32_t D, int32_t H,
+                           int32_t W, double *loss, float *grads)
+{
+    UNETP(up);
+    if (!d_input || !d_target) return fail("NULL argument");
+    if (u->ensure(D, H, W) || u->forward(d_input) || u->backward(d_target, loss)) return -1;
+    if (grads) {
+        cudaError_t e = cudaStreamSynchronize(u->st);
+        if (e == cudaSuccess) e = cudaMemcpy(grads, u->d_g, u->n_params * sizeof(float), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) return fail("copy failed: %s", cudaGetErrorString(e));
+    }
+    return 0;
+}
+
+int mbirgpu_unet_train_step(mbirgpu_unet *up, const float *d_input, const float *d_target, int32_t D, int32_t H,
+                            int32_t W, float lr, double *loss)
+{
+    UNETP(up);
+    if (!d_input || !d_target) return fail("NULL argument");
+    if (u->ensure(D, H, W) || u->forward(d_input) || u->backward(d_target, loss)) return -1;
+    return u->step(lr);
+}
+
+}  // extern "C"

@@ -28,6 +28,10 @@ EXPORTS = (
     "mbirgpu_session_cost", "mbirgpu_session_icd_iteration", "mbirgpu_session_forward_project",
     "mbirgpu_session_back_project", "mbirgpu_session_get_amatrix", "mbirgpu_session_get_detector_response",
     "mbirgpu_session_run", "mbirgpu_session_forward_project_noalloc", "mbirgpu_session_nh_select",
+    "mbirgpu_session_fbp", "mbirgpu_session_set_object_fbp",
+    "mbirgpu_unet_create", "mbirgpu_unet_destroy", "mbirgpu_unet_num_params", "mbirgpu_unet_set_input_scale",
+    "mbirgpu_unet_get_input_scale", "mbirgpu_unet_get_params", "mbirgpu_unet_set_params", "mbirgpu_unet_forward",
+    "mbirgpu_unet_gradients", "mbirgpu_unet_train_step", "mbirgpu_session_set_object_unet",
     "mbirgpu_batch_create", "mbirgpu_batch_destroy", "mbirgpu_batch_run", "mbirgpu_batch_problem_info",
     "mbirgpu_batch_get_object", "mbirgpu_batch_cost", "mbirgpu_reconstruct_batch",
     "phcontomo_reconstruct", "mbirgpu_pc_default_options", "mbirgpu_pc_session_create", "mbirgpu_pc_session_destroy",
@@ -125,6 +129,8 @@ def lib() -> C.CDLL:
         L.mbirgpu_session_back_project.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         L.mbirgpu_session_forward_project_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         L.mbirgpu_session_nh_select.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.mbirgpu_session_fbp.argtypes = [C.c_void_p, C.c_void_p]
+        L.mbirgpu_session_set_object_fbp.argtypes = [C.c_void_p]
         L.mbirgpu_batch_create.argtypes = [C.POINTER(C.c_void_p), C.c_void_p, C.c_int32, C.POINTER(Options),
                                            C.c_void_p]
         L.mbirgpu_batch_destroy.argtypes = [C.c_void_p]
@@ -324,6 +330,15 @@ class Session:
         sinogram [N_p][N_r][N_t] (raw device addresses), allocating nothing;
         enqueued on the session's stream, not waited for."""
         _check(lib().mbirgpu_session_forward_project_noalloc(self.h, C.c_void_p(object_dev), C.c_void_p(sino_dev)))
+
+    def fbp(self) -> np.ndarray:
+        """Filtered back-projection of the measurements, [N_time][N_z][N_y][N_x]."""
+        a = np.zeros(self.shape, np.float32)
+        _check(lib().mbirgpu_session_fbp(self.h, a.ctypes.data))
+        return a
+
+    def set_object_fbp(self) -> None:
+        _check(lib().mbirgpu_session_set_object_fbp(self.h))
 
     def nh_select(self, mag: np.ndarray) -> np.ndarray:
         """NH-ICD voxel-line selection [N_time][N_y][N_x] (uint8) for an

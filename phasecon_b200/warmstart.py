@@ -1,0 +1,213 @@
+"""Learned warm start: training pairs, the U-Net wrapper and the training loop.
+
+The network (phasecon_b200/csrc/unet.cu, run by the library's own BF16
+tensor-core kernels) maps a filtered back-projection frame to the converged
+MBIR frame of the same scan. Training pairs come from seeded phantoms: the
+scan is simulated with the reference's system matrix (GPU forward
+projector), the input is its FBP and the target is plain GPU ICD run to the
+relative-cost-change test. At use, ICD runs from the network's output to the
+same convergence test, so the network only moves the starting point.
+Device buffers are torch CUDA tensors (plumbing only; every operation on them
+is a libmbirgpu kernel).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import phantoms as P
+from .mbir import MbirError, Problem, Session, _check, get_options, lib as _mbir_lib
+from .workloads import _measure
+
+_bound = False
+
+
+def lib() -> C.CDLL:
+    global _bound
+    L = _mbir_lib()
+    if not _bound:
+        vp = C.c_void_p
+        L.mbirgpu_unet_create.argtypes = [C.POINTER(vp), C.c_int32, C.c_uint64, vp]
+        L.mbirgpu_unet_destroy.argtypes = [vp]
+        L.mbirgpu_unet_num_params.argtypes = [vp]
+        L.mbirgpu_unet_num_params.restype = C.c_int64
+        L.mbirgpu_unet_set_input_scale.argtypes = [vp, C.c_float]
+        L.mbirgpu_unet_get_input_scale.argtypes = [vp]
+        L.mbirgpu_unet_get_input_scale.restype = C.c_float
+        L.mbirgpu_unet_get_params.argtypes = [vp, vp]
+        L.mbirgpu_unet_set_params.argtypes = [vp, vp]
+        L.mbirgpu_unet_forward.argtypes = [vp, vp, vp, C.c_int32, C.c_int32, C.c_int32]
+        L.mbirgpu_unet_gradients.argtypes = [vp, vp, vp, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_double), vp]
+        L.mbirgpu_unet_train_step.argtypes = [vp, vp, vp, C.c_int32, C.c_int32, C.c_int32, C.c_float,
+                                              C.POINTER(C.c_double)]
+        L.mbirgpu_session_set_object_unet.argtypes = [vp, vp]
+        _bound = True
+    return L
+
+
+class UNet:
+    """The warm-start network (mbirgpu_unet_*)."""
+
+    def __init__(self, base_channels: int = 16, seed: int = 0):
+        self.c = base_channels
+        self.h = C.c_void_p()
+        _check(lib().mbirgpu_unet_create(C.byref(self.h), base_channels, seed, None))
+
+    def close(self):
+        if self.h:
+            lib().mbirgpu_unet_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def num_params(self) -> int:
+        return int(lib().mbirgpu_unet_num_params(self.h))
+
+    def get_params(self) -> np.ndarray:
+        p = np.zeros(self.num_params, np.float32)
+        _check(lib().mbirgpu_unet_get_params(self.h, p.ctypes.data))
+        return p
+
+    def set_params(self, p: np.ndarray) -> None:
+        p = np.ascontiguousarray(p, np.float32)
+        if p.size != self.num_params:
+            raise MbirError(f"expected {self.num_params} parameters, got {p.size}")
+        _check(lib().mbirgpu_unet_set_params(self.h, p.ctypes.data))
+
+    @property
+    def input_scale(self) -> float:
+        return float(lib().mbirgpu_unet_get_input_scale(self.h))
+
+    @input_scale.setter
+    def input_scale(self, s: float) -> None:
+        _check(lib().mbirgpu_unet_set_input_scale(self.h, s))
+
+    def save(self, path: str) -> None:
+        np.savez_compressed(path, params=self.get_params(), base=self.c, scale=self.input_scale)
+
+    @classmethod
+    def load(cls, path: str) -> "UNet":
+        d = np.load(path)
+        u = cls(int(d["base"]))
+        u.set_params(d["params"])
+        u.input_scale = float(d["scale"])
+        return u
+
+    def forward(self, x):
+        """x: torch CUDA float32 [D][H][W] -> network output (new tensor)."""
+        import torch
+        x = x.contiguous()
+        out = torch.empty_like(x)
+        D, H, W = x.shape
+        _check(lib().mbirgpu_unet_forward(self.h, x.data_ptr(), out.data_ptr(), D, H, W))
+        return out
+
+    def gradients(self, x, t):
+        """(loss, flat FP32 gradient) for one pair of torch CUDA tensors."""
+        D, H, W = x.shape
+        g = np.zeros(self.num_params, np.float32)
+        loss = C.c_double()
+        _check(lib().mbirgpu_unet_gradients(self.h, x.contiguous().data_ptr(), t.contiguous().data_ptr(), D, H, W,
+                                            C.byref(loss), g.ctypes.data))
+        return loss.value, g
+
+    def train_step(self, x, t, lr: float) -> float:
+        D, H, W = x.shape
+        loss = C.c_double()
+        _check(lib().mbirgpu_unet_train_step(self.h, x.data_ptr(), t.data_ptr(), D, H, W, lr, C.byref(loss)))
+        return loss.value
+
+
+def warm_start(session: Session, net: UNet) -> None:
+    """The session's object becomes net(FBP) per frame (e = y - A x recomputed)."""
+    _check(lib().mbirgpu_session_set_object_unet(session.h, net.h))
+
+
+def converge(session: Session, max_iter: int = 200, rel: float = 1e-4, start_iter: int = 1):
+    """Plain ICD until the relative FP64 cost change is below `rel`; returns
+    (iterations, cost history)."""
+    costs = [session.cost()[0]]
+    it = 0
+    while it < max_iter:
+        it += 1
+        session.icd_iteration(start_iter + it - 1)
+        costs.append(session.cost()[0])
+        if it > 1 and abs(costs[-2] - costs[-1]) < rel * abs(costs[-1]):
+            break
+    return it, costs
+
+
+def iterations_to_cost(session: Session, target: float, max_iter: int = 300):
+    """Plain ICD iterations until the FP64 cost is at most `target` (the
+    north star's "reaches the plain method's converged cost"); returns
+    (iterations, cost history) or (None, history) if it never does."""
+    costs = [session.cost()[0]]
+    if costs[0] <= target:
+        return 0, costs
+    for it in range(1, max_iter + 1):
+        session.icd_iteration(it)
+        costs.append(session.cost()[0])
+        if costs[-1] <= target:
+            return it, costs
+    return None, costs
+
+
+def frame_views(frame: int = 0, K: int = 8, n_theta: int = 256, n_p: int = 1024, frames: int = 8):
+    """The views of one frame of the 4-D schedule (interlaced, 128 per frame)."""
+    angles, times = P.interlaced_views(K, n_theta, n_p)
+    edges = np.linspace(0.0, float(n_p), frames + 1)
+    sel = (times >= edges[frame]) & (times < edges[frame + 1])
+    a = np.ascontiguousarray(angles[sel])
+    t = np.ascontiguousarray(times[sel] - edges[frame]).astype(np.float32)
+    return a, t, np.array([0.0, float(edges[frame + 1] - edges[frame])], np.float32)
+
+
+def training_pair(seed: int, n_xy: int = 256, n_z: int = 32, kind: str = "mixed", I0: float = 2e4,
+                  p: float = 1.2, icd_rel: float = 1e-4):
+    """(FBP input, converged ICD target, phantom), each [n_z][n_xy][n_xy] float32,
+    for one seeded phantom scanned with one frame's views of the 4-D schedule."""
+    rng = np.random.default_rng(seed)
+    k = kind if kind != "mixed" else ("ch" if rng.random() < 0.5 else "ellipsoids")
+    if k == "ch":
+        obj = P.cahn_hilliard_frames(n_xy, n_z, 1, steps=int(rng.integers(300, 1200)), seed=seed)[0]
+    else:
+        obj = P.random_ellipsoids(n_xy, n_z, seed)
+    a, t, rt = frame_views(int(rng.integers(0, 8)))
+    nv = a.size
+    z = np.zeros((nv, n_z, n_xy), np.float32)
+    pb = Problem(z, np.ones_like(z), a, t, rt, n_z, n_xy, nv, 1, rot_center=n_xy / 2, sig_s=0.01, sig_t=1.0,
+                 c_s=1.0, c_t=1.0)
+    pb = _measure(pb, obj[None], I0, seed)
+    o = get_options()
+    o.mrf_p = p
+    s = Session(pb, options=o)
+    fbp = s.fbp()[0]
+    s.set_object(np.zeros(s.shape, np.float32))
+    converge(s, rel=icd_rel)
+    target = s.get_object()[0]
+    s.close()
+    return fbp.astype(np.float32), target.astype(np.float32), obj.astype(np.float32)
+
+
+def train(net: UNet, pairs, steps: int, lr: float = 1e-3, seed: int = 0, log_every: int = 0):
+    """Adam steps over randomly drawn (input, target) pairs of host arrays;
+    returns the loss history. The network's input scale is set so that it sees
+    values of order one."""
+    import torch
+    rng = np.random.default_rng(seed)
+    net.input_scale = 1.0 / max(float(np.mean([np.abs(t).max() for _, t in pairs])), 1e-12)
+    dev = [(torch.from_numpy(np.ascontiguousarray(x, np.float32)).cuda(),
+            torch.from_numpy(np.ascontiguousarray(t, np.float32)).cuda()) for x, t in pairs]
+    hist = []
+    for s in range(steps):
+        x, t = dev[int(rng.integers(0, len(dev)))]
+        hist.append(net.train_step(x, t, lr))
+        if log_every and (s + 1) % log_every == 0:
+            print(f"step {s + 1}: loss {np.mean(hist[-log_every:]):.4g}", flush=True)
+    return hist
