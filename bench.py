@@ -56,8 +56,11 @@ def parse():
     ap.add_argument("--no-converge", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--max-converge-iters", type=int, default=400)
-    ap.add_argument("--workload", default="4d", choices=["4d", "batch"],
-                    help="4d: the 4-D benchmark (default); batch: 48 uneven 3-D problems, batched vs sequential")
+    ap.add_argument("--workload", default="4d", choices=["4d", "batch", "warmstart"],
+                    help="4d: the 4-D benchmark (default); batch: 48 uneven 3-D problems, batched vs sequential; "
+                         "warmstart: the learned warm start on the 4-D workload")
+    ap.add_argument("--train-pairs", type=int, default=64)
+    ap.add_argument("--train-steps", type=int, default=1500)
     return ap.parse_args()
 
 
@@ -452,6 +455,68 @@ def run_batch(args, world, rank, local, pg):
             "clocks": clk.summary()}))
 
 
+def run_warmstart(args, world, rank, local, pg):
+    """The learned warm start on the 4-D workload: train the U-Net on seeded
+    single-frame phantoms (FBP -> converged plain GPU ICD), then time plain ICD
+    on the 4-D problem to the plain method's converged cost (within 1e-4
+    relative) from zero, from FBP and from the network's output (the FBP and
+    network time included)."""
+    import torch
+
+    import phasecon_b200 as pc
+    from phasecon_b200 import warmstart as WS
+    from phasecon_b200 import workloads as W
+
+    torch.cuda.set_device(local)
+    t0 = time.perf_counter()
+    pairs = [WS.training_pair(1000 + rank * 100000 + i)[:2] for i in range(args.train_pairs)]
+    t_data = time.perf_counter() - t0
+    net = WS.UNet(16, seed=rank)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    hist = WS.train(net, pairs, args.train_steps, lr=1e-3, seed=rank)
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0
+    pb, _, p = W.config_4d(seed=0)
+    opt = pc.get_options()
+    opt.mrf_p = p
+    s = pc.Session(pb, options=opt)
+    s.set_object(np.zeros(s.shape, np.float32))
+    _, c_conv = WS.converge(s, rel=1e-7, max_iter=400)
+    target = c_conv[-1] * (1 + 1e-4)
+    res = {}
+    for name in ("zero", "fbp", "unet"):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        if name == "zero":
+            s.set_object(np.zeros(s.shape, np.float32))
+        elif name == "fbp":
+            s.set_object_fbp()
+        else:
+            WS.warm_start(s, net)
+        torch.cuda.synchronize()
+        t_init = time.perf_counter() - t0
+        it, costs = WS.iterations_to_cost(s, target, max_iter=400)
+        torch.cuda.synchronize()
+        res[name] = {"time_to_converged_cost_s": time.perf_counter() - t0, "init_s": t_init, "iterations": it,
+                     "initial_cost": costs[0], "final_cost": costs[-1]}
+    s.close()
+    if rank == 0:
+        tz, tu = res["zero"]["time_to_converged_cost_s"], res["unet"]["time_to_converged_cost_s"]
+        print(json.dumps({
+            "metric": "warm start: wall time to the plain method's converged cost (rel 1e-4), 4-D workload",
+            "value": tu, "unit": "s", "n_gpus": world, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "bf16 network / f32 ICD", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "unet": "4 levels 16/32/64/128, 3x3x3, BF16, FP32 accumulation",
+                       "train_pairs": args.train_pairs, "train_steps": args.train_steps,
+                       "train_phantoms": "seeded Cahn-Hilliard / random ellipsoids, 256x256x32, one 4-D frame's "
+                                         "128 views, I0 2e4; targets: plain GPU ICD to rel 1e-4"},
+            "speedup_vs_zero_init": tz / tu if tu else None,
+            "speedup_vs_fbp_init": res["fbp"]["time_to_converged_cost_s"] / tu if tu else None,
+            "target_cost": target, "starts": res, "train_data_s": t_data, "train_s": t_train,
+            "train_loss_first_last": [float(np.mean(hist[:20])), float(np.mean(hist[-20:]))]}))
+
+
 def main():
     args = parse()
     world, rank, local, pg = dist_setup()
@@ -460,6 +525,8 @@ def main():
             run_reference_arm(args, rank)
         elif args.workload == "batch":
             run_batch(args, world, rank, local, pg)
+        elif args.workload == "warmstart":
+            run_warmstart(args, world, rank, local, pg)
         else:
             run_ours(args, world, rank, local, pg)
     finally:

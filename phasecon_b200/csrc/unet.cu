@@ -13,11 +13,15 @@
 // Convolutions are implicit GEMMs on the tensor cores (mma.sync m16n8k16
 // BF16 -> FP32):
 //   forward   out[v][co] = sum_{tap, ci} in[v + off(tap)][ci] w[tap][ci][co]
-//             (M = voxels, N = co, K = 27 ci; zero padding);
+//             (M = voxels, N = co, K = 27 ci; zero padding), a CTA per
+//             2 x 8 x 16 output tile whose input halo (4 x 10 x 18 voxels, 16
+//             channels at a time) and weights sit in shared memory for all
+//             27 taps; the one-channel first layer folds the taps into K;
 //   data grad the same kernel on the output gradient with the weights
 //             flipped in space and transposed in channels;
 //   weight grad dw[tap][ci][co] = sum_v in[v + off(tap)][ci] g[v][co]
-//             (M = ci, N = co, K = voxels, split over voxel chunks, FP32 atomics).
+//             (M = ci, N = co, K = voxels) over the same tiles, all 27 taps
+//             from one staged halo, FP32 atomics once per CTA.
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -49,151 +53,309 @@ __device__ __forceinline__ void mma_bf16(float (&c)[4], const uint32_t (&a)[4], 
 
 __device__ __forceinline__ uint32_t ld_pair(const bf16 *p) { return *reinterpret_cast<const uint32_t *>(p); }
 
-// voxel v of a D x H x W grid shifted by tap (dz, dy, dx in -1..1); -1 outside
-__device__ __forceinline__ long long shifted(long long v, int tap, int D, int H, int W)
-{
-    const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
-    const int x = (int)(v % W), y = (int)((v / W) % H), z = (int)(v / ((long long)W * H));
-    const int xx = x + dx, yy = y + dy, zz = z + dz;
-    if (xx < 0 || xx >= W || yy < 0 || yy >= H || zz < 0 || zz >= D) return -1;
-    return ((long long)zz * H + yy) * W + xx;
-}
+constexpr int kPadK = 24;  // shared-memory row stride (16 + 8) in bf16: conflict-free fragment loads
 
-constexpr int kConvM = 128;  // voxels per CTA
-constexpr int kConvN = 64;   // output channels per CTA
-constexpr int kPadK = 24;    // shared-memory row stride (16 + 8) in bf16
+// Output tile of the forward convolution CTA: FZ x FY x FX voxels (256 = 8
+// warps x two m16 rows of 16 voxels along x); its input halo tile holds
+// (FZ+2)(FY+2)(FX+2) voxels x 16 channels, staged once per 16-channel chunk
+// and read by all 27 taps from shared memory.
+constexpr int FZ = 2, FY = 8, FX = 16;
+constexpr int FHZ = FZ + 2, FHY = FY + 2, FHX = FX + 2;
+constexpr int kFHalo = FHZ * FHY * FHX;
+constexpr int kFThreads = 32 * FZ * FY / 2;  // 256
 
-// out = act(conv3x3x3(in, w) + b); w is [27][Cin][Cout].
-__global__ void __launch_bounds__(128) conv_fwd_kernel(const bf16 *__restrict__ in, int Cin,
-                                                       const bf16 *__restrict__ w, const float *__restrict__ bias,
-                                                       bf16 *__restrict__ out, int Cout, int D, int H, int W,
-                                                       int relu)
+template <int NT>
+constexpr size_t conv_smem() { return (size_t)(kFHalo + 27 * NT) * kPadK * sizeof(bf16); }
+
+// The weight-gradient tile: TZ x TY x TX = 128 voxels, halo (TZ+2)(TY+2)(TX+2).
+constexpr int TZ = 2, TY = 4, TX = 16;
+constexpr int HZ = TZ + 2, HY = TY + 2, HX = TX + 2;
+constexpr int kHalo = HZ * HY * HX;
+
+// out[v][n] = act(sum_{tap, k} in[v + off(tap)][k] wt[tap][n][k] + b[n]) with
+// wt in [27][Nout][Kin] layout (the forward weights transposed per tap, or the
+// data-gradient weights flipped in space); NT output channels per CTA.
+template <int NT>
+__global__ void __launch_bounds__(kFThreads) conv_tile_kernel(const bf16 *__restrict__ in, int Kin,
+                                                        const bf16 *__restrict__ wt, const float *__restrict__ bias,
+                                                        bf16 *__restrict__ out, int Nout, int D, int H, int W,
+                                                        int relu)
 {
-    __shared__ __align__(16) bf16 As[kConvM][kPadK];
-    __shared__ __align__(16) bf16 Bs[kConvN][kPadK];
-    const long long V = (long long)D * H * W;
-    const long long m0 = (long long)blockIdx.x * kConvM;
-    const int n0 = blockIdx.y * kConvN;
-    const int NT = min(kConvN, Cout - n0);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    bf16 *Hs = reinterpret_cast<bf16 *>(smem_raw);  // [kFHalo][kPadK]
+    bf16 *Ws = Hs + kFHalo * kPadK;                   // [27][NT][kPadK]
+    const int tiles_x = (W + FX - 1) / FX, tiles_y = (H + FY - 1) / FY;
+    int b = blockIdx.x;
+    const int x0 = (b % tiles_x) * FX;
+    b /= tiles_x;
+    const int y0 = (b % tiles_y) * FY, z0 = (b / tiles_y) * FZ;
+    const int n0 = blockIdx.y * NT;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, tig = lane & 3;
-    float acc[2][8][4];
+    float acc[2][NT / 8][4];
 #pragma unroll
     for (int i = 0; i < 2; i++)
 #pragma unroll
-        for (int j = 0; j < 8; j++)
+        for (int j = 0; j < NT / 8; j++)
 #pragma unroll
             for (int q = 0; q < 4; q++) acc[i][j][q] = 0.0f;
-    const long long vm = m0 + threadIdx.x;  // the voxel this thread stages
-    for (int tap = 0; tap < 27; tap++) {
-        const long long src = vm < V ? shifted(vm, tap, D, H, W) : -1;
-        for (int c0 = 0; c0 < Cin; c0 += 16) {
-            // A: this thread's voxel, 16 channels
-            bf16 *arow = &As[threadIdx.x][0];
-            if (src >= 0 && c0 + 16 <= Cin) {
-                const uint4 *p = reinterpret_cast<const uint4 *>(in + src * Cin + c0);
-                reinterpret_cast<uint4 *>(arow)[0] = p[0];
-                reinterpret_cast<uint4 *>(arow)[1] = p[1];
+    for (int c0 = 0; c0 < Kin; c0 += 16) {
+        const bool full = c0 + 16 <= Kin;
+        for (int hv = threadIdx.x; hv < kFHalo; hv += blockDim.x) {
+            const int hz = hv / (FHY * FHX), r = hv - hz * (FHY * FHX), hy = r / FHX, hx = r - hy * FHX;
+            const int z = z0 + hz - 1, y = y0 + hy - 1, x = x0 + hx - 1;
+            bf16 *dst = Hs + hv * kPadK;
+            const bool inside = z >= 0 && z < D && y >= 0 && y < H && x >= 0 && x < W;
+            const long long v = ((long long)z * H + y) * W + x;
+            if (inside && full) {
+                const uint4 *p = reinterpret_cast<const uint4 *>(in + v * Kin + c0);
+                reinterpret_cast<uint4 *>(dst)[0] = p[0];
+                reinterpret_cast<uint4 *>(dst)[1] = p[1];
             } else {
                 for (int k = 0; k < 16; k++)
-                    arow[k] = (src >= 0 && c0 + k < Cin) ? in[src * Cin + c0 + k] : __float2bfloat16(0.0f);
+                    dst[k] = (inside && c0 + k < Kin) ? in[v * Kin + c0 + k] : __float2bfloat16(0.0f);
             }
-            // B (transposed): Bs[n][k] = w[tap][c0 + k][n0 + n]
-            for (int e = threadIdx.x; e < kConvN * 16; e += blockDim.x) {
-                const int k = e / kConvN, n = e % kConvN;
-                Bs[n][k] = (n < NT && c0 + k < Cin) ? w[((size_t)tap * Cin + c0 + k) * Cout + n0 + n]
-                                                    : __float2bfloat16(0.0f);
+        }
+        for (int e = threadIdx.x; e < 27 * NT; e += blockDim.x) {
+            const int tap = e / NT, n = e - tap * NT;
+            bf16 *dst = Ws + e * kPadK;
+            const bool ok = n0 + n < Nout;
+            const size_t src = ((size_t)tap * Nout + n0 + n) * Kin + c0;
+            if (ok && full) {
+                const uint4 *p = reinterpret_cast<const uint4 *>(wt + src);
+                reinterpret_cast<uint4 *>(dst)[0] = p[0];
+                reinterpret_cast<uint4 *>(dst)[1] = p[1];
+            } else {
+                for (int k = 0; k < 16; k++) dst[k] = (ok && c0 + k < Kin) ? wt[src + k] : __float2bfloat16(0.0f);
             }
-            __syncthreads();
+        }
+        __syncthreads();
+#pragma unroll 1
+        for (int tap = 0; tap < 27; tap++) {
+            const int dz = tap / 9, dy = (tap / 3) % 3, dx = tap % 3;  // halo offsets 0..2
 #pragma unroll
             for (int i = 0; i < 2; i++) {
-                const int r = warp * 32 + i * 16 + g;
-                const uint32_t a[4] = {ld_pair(&As[r][tig * 2]), ld_pair(&As[r + 8][tig * 2]),
-                                       ld_pair(&As[r][tig * 2 + 8]), ld_pair(&As[r + 8][tig * 2 + 8])};
+                const int row = warp * 2 + i, tz = row / FY, ty = row % FY;
+                const bf16 *hrow = Hs + (((tz + dz) * FHY + ty + dy) * FHX + dx) * kPadK;
+                const uint32_t a[4] = {ld_pair(hrow + g * kPadK + tig * 2), ld_pair(hrow + (g + 8) * kPadK + tig * 2),
+                                       ld_pair(hrow + g * kPadK + tig * 2 + 8),
+                                       ld_pair(hrow + (g + 8) * kPadK + tig * 2 + 8)};
 #pragma unroll
-                for (int j = 0; j < 8; j++) {
-                    if (j * 8 < NT) {
-                        const uint32_t b[2] = {ld_pair(&Bs[j * 8 + g][tig * 2]), ld_pair(&Bs[j * 8 + g][tig * 2 + 8])};
-                        mma_bf16(acc[i][j], a, b);
-                    }
+                for (int j = 0; j < NT / 8; j++) {
+                    const bf16 *wrow = Ws + (tap * NT + j * 8 + g) * kPadK;
+                    const uint32_t bb[2] = {ld_pair(wrow + tig * 2), ld_pair(wrow + tig * 2 + 8)};
+                    mma_bf16(acc[i][j], a, bb);
                 }
             }
-            __syncthreads();
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < 2; i++) {
+        const int row = warp * 2 + i, z = z0 + row / FY, y = y0 + row % FY;
+        if (z >= D || y >= H) continue;
+#pragma unroll
+        for (int j = 0; j < NT / 8; j++)
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int x = x0 + g + h * 8;
+                if (x >= W) continue;
+                const long long v = ((long long)z * H + y) * W + x;
+#pragma unroll
+                for (int q = 0; q < 2; q++) {
+                    const int n = n0 + j * 8 + tig * 2 + q;
+                    if (n >= Nout) continue;
+                    float val = acc[i][j][h * 2 + q] + (bias ? bias[n] : 0.0f);
+                    if (relu) val = fmaxf(val, 0.0f);
+                    out[v * Nout + n] = __float2bfloat16(val);
+                }
+            }
+    }
+}
+
+// The first convolution (one input channel): the 27 taps are the GEMM's K
+// (padded to 32) instead of 27 separate one-channel products. Same output tile
+// as conv_tile_kernel; wt in [27][Nout][1] layout.
+constexpr int kPadK32 = 40;
+
+template <int NT>
+__global__ void __launch_bounds__(kFThreads) conv_first_kernel(const bf16 *__restrict__ in,
+                                                               const bf16 *__restrict__ wt,
+                                                               const float *__restrict__ bias, bf16 *__restrict__ out,
+                                                               int Nout, int D, int H, int W, int relu)
+{
+    __shared__ __align__(16) bf16 As[FZ * FY * FX][kPadK32];
+    __shared__ __align__(16) bf16 Bs[NT][kPadK32];
+    const int tiles_x = (W + FX - 1) / FX, tiles_y = (H + FY - 1) / FY;
+    int b = blockIdx.x;
+    const int x0 = (b % tiles_x) * FX;
+    b /= tiles_x;
+    const int y0 = (b % tiles_y) * FY, z0 = (b / tiles_y) * FZ;
+    const int n0 = blockIdx.y * NT;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, tig = lane & 3;
+    {
+        const int tv = threadIdx.x;  // one output voxel per thread
+        const int tz = tv / (FY * FX), r = tv - tz * (FY * FX), ty = r / FX, tx = r - ty * FX;
+        const int z = z0 + tz, y = y0 + ty, x = x0 + tx;
+        for (int k = 0; k < 32; k++) {
+            float v = 0.0f;
+            if (k < 27) {
+                const int zz = z + k / 9 - 1, yy = y + (k / 3) % 3 - 1, xx = x + k % 3 - 1;
+                if (zz >= 0 && zz < D && yy >= 0 && yy < H && xx >= 0 && xx < W)
+                    v = __bfloat162float(in[((long long)zz * H + yy) * W + xx]);
+            }
+            As[tv][k] = __float2bfloat16(v);
         }
     }
+    for (int e = threadIdx.x; e < NT * 32; e += blockDim.x) {
+        const int n = e / 32, k = e % 32;
+        Bs[n][k] = (k < 27 && n0 + n < Nout) ? wt[(size_t)k * Nout + n0 + n] : __float2bfloat16(0.0f);
+    }
+    __syncthreads();
+    float acc[2][NT / 8][4];
 #pragma unroll
     for (int i = 0; i < 2; i++)
 #pragma unroll
-        for (int j = 0; j < 8; j++) {
-            if (j * 8 >= NT) continue;
-            const int col = j * 8 + tig * 2;
+        for (int j = 0; j < NT / 8; j++)
 #pragma unroll
-            for (int h = 0; h < 2; h++) {
-                const long long v = m0 + warp * 32 + i * 16 + g + h * 8;
-                if (v >= V) continue;
-                for (int q = 0; q < 2; q++) {
-                    if (col + q >= NT) continue;
-                    float val = acc[i][j][h * 2 + q] + (bias ? bias[n0 + col + q] : 0.0f);
-                    if (relu) val = fmaxf(val, 0.0f);
-                    out[v * Cout + n0 + col + q] = __float2bfloat16(val);
-                }
+            for (int q = 0; q < 4; q++) acc[i][j][q] = 0.0f;
+#pragma unroll
+    for (int kk = 0; kk < 32; kk += 16)
+#pragma unroll
+        for (int i = 0; i < 2; i++) {
+            const bf16 *arow = &As[(warp * 2 + i) * 16][kk];
+            const uint32_t a[4] = {ld_pair(arow + g * kPadK32 + tig * 2), ld_pair(arow + (g + 8) * kPadK32 + tig * 2),
+                                   ld_pair(arow + g * kPadK32 + tig * 2 + 8),
+                                   ld_pair(arow + (g + 8) * kPadK32 + tig * 2 + 8)};
+#pragma unroll
+            for (int j = 0; j < NT / 8; j++) {
+                const uint32_t bb[2] = {ld_pair(&Bs[j * 8 + g][kk + tig * 2]), ld_pair(&Bs[j * 8 + g][kk + tig * 2 + 8])};
+                mma_bf16(acc[i][j], a, bb);
             }
         }
+#pragma unroll
+    for (int i = 0; i < 2; i++) {
+        const int row = warp * 2 + i, z = z0 + row / FY, y = y0 + row % FY;
+        if (z >= D || y >= H) continue;
+#pragma unroll
+        for (int j = 0; j < NT / 8; j++)
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int x = x0 + g + h * 8;
+                if (x >= W) continue;
+                const long long v = ((long long)z * H + y) * W + x;
+#pragma unroll
+                for (int q = 0; q < 2; q++) {
+                    const int n = n0 + j * 8 + tig * 2 + q;
+                    if (n >= Nout) continue;
+                    float val = acc[i][j][h * 2 + q] + (bias ? bias[n] : 0.0f);
+                    if (relu) val = fmaxf(val, 0.0f);
+                    out[v * Nout + n] = __float2bfloat16(val);
+                }
+            }
+    }
 }
 
-constexpr int kWgChunk = 1024;  // voxels per CTA of the weight gradient
-
-// dw[tap][ci][co] += sum_v in[v + off(tap)][ci] g[v][co]; CTA tile 32 ci x 64 co.
-__global__ void __launch_bounds__(128) conv_wgrad_kernel(const bf16 *__restrict__ in, int Cin,
-                                                         const bf16 *__restrict__ gout, int Cout,
-                                                         float *__restrict__ dw, int D, int H, int W)
+// Tile-kernel weights from w[27][Cin][Cout]: forward wt[tap][co][ci] (per-tap
+// transpose); data gradient wt[tap][ci][co] = w[26 - tap][ci][co] (spatial flip).
+__global__ void tile_weights_kernel(const bf16 *__restrict__ w, int Cin, int Cout, int flip, bf16 *__restrict__ wt)
 {
-    __shared__ __align__(16) bf16 As[32][kPadK];  // [ci][k]
-    __shared__ __align__(16) bf16 Bs[64][kPadK];  // [co][k]
-    const long long V = (long long)D * H * W;
-    const long long v0 = (long long)blockIdx.x * kWgChunk;
-    const int tap = blockIdx.y;
-    const int nco = (Cout + 63) / 64;
-    const int ci0 = (blockIdx.z / nco) * 32, co0 = (blockIdx.z % nco) * 64;
+    const long long n = 27LL * Cin * Cout;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int co = (int)(i % Cout), ci = (int)((i / Cout) % Cin), tap = (int)(i / ((long long)Cout * Cin));
+        if (flip) wt[((size_t)(26 - tap) * Cin + ci) * Cout + co] = w[i];
+        else wt[((size_t)tap * Cout + co) * Cin + ci] = w[i];
+    }
+}
+
+// Weight gradient dw[tap][ci][co] += sum_v in[v + off(tap)][ci] g[v][co]
+// (M = 16 input channels, N = NT output channels, K = voxels). A CTA of 8 warps
+// walks output tiles (the forward kernel's 2 x 4 x 16); per tile it stages the
+// input halo transposed ([ci][halo voxel]) and the output gradient transposed
+// ([co][voxel]) in shared memory, and warp w accumulates the taps w, w + 8,
+// w + 16, w + 24 over all its tiles in registers before one FP32 atomic add
+// per weight.
+constexpr int kHaloPad = kHalo + 8;   // row stride of the transposed halo
+constexpr int kTileVox = TZ * TY * TX;  // 128
+constexpr int kTilePad = kTileVox + 8;
+
+template <int NT>
+__global__ void __launch_bounds__(256) conv_wgrad_tile_kernel(const bf16 *__restrict__ in, int Cin,
+                                                              const bf16 *__restrict__ gout, int Cout,
+                                                              float *__restrict__ dw, int D, int H, int W)
+{
+    __shared__ __align__(16) bf16 Ah[16][kHaloPad];
+    __shared__ __align__(16) bf16 Bg[NT][kTilePad];
+    const int tiles_x = (W + TX - 1) / TX, tiles_y = (H + TY - 1) / TY;
+    const int n_tiles = tiles_x * tiles_y * ((D + TZ - 1) / TZ);
+    const int c0 = blockIdx.y * 16, n0 = blockIdx.z * NT;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, tig = lane & 3;
-    const int mt = warp & 1, nh = warp >> 1;  // m16 tile, half of the 64 columns
-    float acc[4][4];
+    float acc[4][NT / 8][4];
 #pragma unroll
-    for (int j = 0; j < 4; j++)
+    for (int a = 0; a < 4; a++)
 #pragma unroll
-        for (int q = 0; q < 4; q++) acc[j][q] = 0.0f;
-    for (long long k0 = v0; k0 < min(V, v0 + kWgChunk); k0 += 16) {
-        for (int e = threadIdx.x; e < 32 * 16; e += blockDim.x) {
-            const int ci = e % 32, k = e / 32;
-            const long long v = k0 + k;
-            const long long s = v < V ? shifted(v, tap, D, H, W) : -1;
-            As[ci][k] = (s >= 0 && ci0 + ci < Cin) ? in[s * Cin + ci0 + ci] : __float2bfloat16(0.0f);
+        for (int j = 0; j < NT / 8; j++)
+#pragma unroll
+            for (int q = 0; q < 4; q++) acc[a][j][q] = 0.0f;
+    for (int t = blockIdx.x; t < n_tiles; t += gridDim.x) {
+        int b = t;
+        const int x0 = (b % tiles_x) * TX;
+        b /= tiles_x;
+        const int y0 = (b % tiles_y) * TY, z0 = (b / tiles_y) * TZ;
+        for (int e = threadIdx.x; e < kHalo * 16; e += blockDim.x) {
+            const int hv = e >> 4, ci = e & 15;
+            const int hz = hv / (HY * HX), r = hv - hz * (HY * HX), hy = r / HX, hx = r - hy * HX;
+            const int z = z0 + hz - 1, y = y0 + hy - 1, x = x0 + hx - 1;
+            const bool inside = z >= 0 && z < D && y >= 0 && y < H && x >= 0 && x < W && c0 + ci < Cin;
+            Ah[ci][hv] = inside ? in[(((long long)z * H + y) * W + x) * Cin + c0 + ci] : __float2bfloat16(0.0f);
         }
-        for (int e = threadIdx.x; e < 64 * 16; e += blockDim.x) {
-            const int co = e % 64, k = e / 64;
-            const long long v = k0 + k;
-            Bs[co][k] = (v < V && co0 + co < Cout) ? gout[v * Cout + co0 + co] : __float2bfloat16(0.0f);
+        for (int e = threadIdx.x; e < kTileVox * NT; e += blockDim.x) {
+            const int tv = e / NT, n = e - tv * NT;
+            const int tz = tv / (TY * TX), r = tv - tz * (TY * TX), ty = r / TX, tx = r - ty * TX;
+            const int z = z0 + tz, y = y0 + ty, x = x0 + tx;
+            const bool inside = z < D && y < H && x < W && n0 + n < Cout;
+            Bg[n][tv] = inside ? gout[(((long long)z * H + y) * W + x) * Cout + n0 + n] : __float2bfloat16(0.0f);
         }
         __syncthreads();
-        const int r = mt * 16 + g;
-        const uint32_t a[4] = {ld_pair(&As[r][tig * 2]), ld_pair(&As[r + 8][tig * 2]), ld_pair(&As[r][tig * 2 + 8]),
-                               ld_pair(&As[r + 8][tig * 2 + 8])};
 #pragma unroll
-        for (int j = 0; j < 4; j++) {
-            const int n = nh * 32 + j * 8 + g;
-            const uint32_t b[2] = {ld_pair(&Bs[n][tig * 2]), ld_pair(&Bs[n][tig * 2 + 8])};
-            mma_bf16(acc[j], a, b);
+        for (int a = 0; a < 4; a++) {
+            const int tap = warp + 8 * a;
+            if (tap >= 27) break;
+            const int dz = tap / 9, dy = (tap / 3) % 3, dx = tap % 3;
+#pragma unroll 2
+            for (int ks = 0; ks < TZ * TY; ks++) {  // one tile row of 16 voxels per k-step
+                const int tz = ks / TY, ty = ks % TY;
+                const int h0 = ((tz + dz) * HY + ty + dy) * HX + dx;
+                auto pack = [&](int ci, int x) {
+                    const uint32_t lo = __bfloat16_as_ushort(Ah[ci][h0 + x]);
+                    const uint32_t hi = __bfloat16_as_ushort(Ah[ci][h0 + x + 1]);
+                    return lo | (hi << 16);
+                };
+                const uint32_t av[4] = {pack(g, tig * 2), pack(g + 8, tig * 2), pack(g, tig * 2 + 8),
+                                        pack(g + 8, tig * 2 + 8)};
+#pragma unroll
+                for (int j = 0; j < NT / 8; j++) {
+                    const bf16 *brow = &Bg[j * 8 + g][ks * 16];
+                    const uint32_t bb[2] = {ld_pair(brow + tig * 2), ld_pair(brow + tig * 2 + 8)};
+                    mma_bf16(acc[a][j], av, bb);
+                }
+            }
         }
         __syncthreads();
     }
 #pragma unroll
-    for (int j = 0; j < 4; j++)
+    for (int a = 0; a < 4; a++) {
+        const int tap = warp + 8 * a;
+        if (tap >= 27) break;
 #pragma unroll
-        for (int h = 0; h < 2; h++)
+        for (int j = 0; j < NT / 8; j++)
 #pragma unroll
-            for (int q = 0; q < 2; q++) {
-                const int ci = ci0 + mt * 16 + g + h * 8, co = co0 + nh * 32 + j * 8 + tig * 2 + q;
-                if (ci < Cin && co < Cout) atomicAdd(&dw[((size_t)tap * Cin + ci) * Cout + co], acc[j][h * 2 + q]);
-            }
+            for (int h = 0; h < 2; h++)
+#pragma unroll
+                for (int q = 0; q < 2; q++) {
+                    const int ci = c0 + g + h * 8, co = n0 + j * 8 + tig * 2 + q;
+                    if (ci < Cin && co < Cout) atomicAdd(&dw[((size_t)tap * Cin + ci) * Cout + co], acc[a][j][h * 2 + q]);
+                }
+    }
 }
 
 // db[co] += sum_v g[v][co]
@@ -205,16 +367,6 @@ __global__ void bias_grad_kernel(const bf16 *__restrict__ g, long long V, int C,
          v += (long long)gridDim.x * lanes)
         s += __bfloat162float(g[v * C + c]);
     if (threadIdx.x < lanes * C) atomicAdd(&db[c], s);
-}
-
-// wt[26 - tap][co][ci] = w[tap][ci][co] (the data-gradient weights)
-__global__ void flip_weights_kernel(const bf16 *__restrict__ w, int Cin, int Cout, int taps, bf16 *__restrict__ wt)
-{
-    const long long n = (long long)taps * Cin * Cout;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        const int co = (int)(i % Cout), ci = (int)((i / Cout) % Cin), tap = (int)(i / ((long long)Cout * Cin));
-        wt[((size_t)(taps - 1 - tap) * Cout + co) * Cin + ci] = w[i];
-    }
 }
 
 __global__ void relu_grad_kernel(bf16 *__restrict__ g, const bf16 *__restrict__ act, long long n)
@@ -450,6 +602,7 @@ struct UNet {
     int ensure(int d, int h, int w);
     long long vox(int l) const { return (long long)(D >> l) * (H >> l) * (W >> l); }
     void conv(int i, const bf16 *in, bf16 *o, int l, bool relu);
+    void conv_tiles(const bf16 *in, int Kin, const float *bias, bf16 *o, int Nout, int l, bool relu);
     void conv_back(int i, const bf16 *in, const bf16 *o, bf16 *go, bf16 *gin, int l);
     int forward(const float *d_in);
     int backward(const float *d_target, double *loss);
@@ -508,6 +661,12 @@ int UNet::init(int base, uint64_t seed)
     copy_to_bf16_kernel<<<grid_for((long long)n_params), 256, 0, st>>>(d_p, (long long)n_params, d_pb);
     e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(conv_tile_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)conv_smem<64>());
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(conv_tile_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)conv_smem<32>());
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(conv_tile_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)conv_smem<16>());
     return e == cudaSuccess ? 0 : fail("U-Net init failed: %s", cudaGetErrorString(e));
 }
 
@@ -558,12 +717,32 @@ int UNet::ensure(int d, int h, int w)
     return 0;
 }
 
+// out = act(conv(in)) with weights in the tile layout (d_wt); Nout output channels.
+void UNet::conv_tiles(const bf16 *in, int Kin, const float *bias, bf16 *o, int Nout, int l, bool relu)
+{
+    const int d = D >> l, h = H >> l, w = W >> l;
+    const unsigned tiles = (unsigned)(((d + FZ - 1) / FZ) * ((h + FY - 1) / FY) * ((w + FX - 1) / FX));
+    const int r = relu ? 1 : 0;
+    if (Kin == 1) {
+        dim3 grid(tiles, (unsigned)((Nout + 15) / 16));
+        conv_first_kernel<16><<<grid, kFThreads, 0, st>>>(in, d_wt, bias, o, Nout, d, h, w, r);
+    } else if (Nout > 32) {
+        dim3 grid(tiles, (unsigned)((Nout + 63) / 64));
+        conv_tile_kernel<64><<<grid, kFThreads, conv_smem<64>(), st>>>(in, Kin, d_wt, bias, o, Nout, d, h, w, r);
+    } else if (Nout > 16) {
+        conv_tile_kernel<32><<<dim3(tiles, 1), kFThreads, conv_smem<32>(), st>>>(in, Kin, d_wt, bias, o, Nout, d, h,
+                                                                                w, r);
+    } else {
+        conv_tile_kernel<16><<<dim3(tiles, 1), kFThreads, conv_smem<16>(), st>>>(in, Kin, d_wt, bias, o, Nout, d, h,
+                                                                                w, r);
+    }
+}
+
 void UNet::conv(int i, const bf16 *in, bf16 *o, int l, bool relu)
 {
     const Conv &k = convs[i];
-    dim3 grid((unsigned)((vox(l) + kConvM - 1) / kConvM), (unsigned)((k.cout + kConvN - 1) / kConvN));
-    conv_fwd_kernel<<<grid, 128, 0, st>>>(in, k.cin, d_pb + k.w, d_p + k.b, o, k.cout, D >> l, H >> l, W >> l,
-                                          relu ? 1 : 0);
+    tile_weights_kernel<<<grid_for(27LL * k.cin * k.cout), 256, 0, st>>>(d_pb + k.w, k.cin, k.cout, 0, d_wt);
+    conv_tiles(in, k.cin, d_p + k.b, o, k.cout, l, relu);
 }
 
 // o = relu(conv(in)); go: gradient w.r.t. o (overwritten by the ReLU mask);
@@ -573,16 +752,25 @@ void UNet::conv_back(int i, const bf16 *in, const bf16 *o, bf16 *go, bf16 *gin, 
     const Conv &k = convs[i];
     const long long V = vox(l);
     relu_grad_kernel<<<grid_for(V * k.cout), 256, 0, st>>>(go, o, V * k.cout);
-    const int nci = (k.cin + 31) / 32, nco = (k.cout + 63) / 64;
-    dim3 gw((unsigned)((V + kWgChunk - 1) / kWgChunk), 27, (unsigned)(nci * nco));
-    conv_wgrad_kernel<<<gw, 128, 0, st>>>(in, k.cin, go, k.cout, d_g + k.w, D >> l, H >> l, W >> l);
+    {
+        const int d = D >> l, h = H >> l, w = W >> l;
+        const int tiles = ((d + TZ - 1) / TZ) * ((h + TY - 1) / TY) * ((w + TX - 1) / TX);
+        const int nci = (k.cin + 15) / 16;
+        const unsigned gx = (unsigned)std::max(1, std::min(tiles, 4 * 148 / std::max(1, nci)));
+        if (k.cout > 32) {
+            dim3 grid(gx, (unsigned)nci, (unsigned)((k.cout + 63) / 64));
+            conv_wgrad_tile_kernel<64><<<grid, 256, 0, st>>>(in, k.cin, go, k.cout, d_g + k.w, d, h, w);
+        } else if (k.cout > 16) {
+            conv_wgrad_tile_kernel<32><<<dim3(gx, nci, 1), 256, 0, st>>>(in, k.cin, go, k.cout, d_g + k.w, d, h, w);
+        } else {
+            conv_wgrad_tile_kernel<16><<<dim3(gx, nci, 1), 256, 0, st>>>(in, k.cin, go, k.cout, d_g + k.w, d, h, w);
+        }
+    }
     const int lanes = std::max(1, 256 / k.cout);
     bias_grad_kernel<<<grid_for(V, lanes), lanes * k.cout, 0, st>>>(go, V, k.cout, d_g + k.b);
     if (gin) {
-        flip_weights_kernel<<<grid_for((long long)27 * k.cin * k.cout), 256, 0, st>>>(d_pb + k.w, k.cin, k.cout, 27,
-                                                                                    d_wt);
-        dim3 grid((unsigned)((V + kConvM - 1) / kConvM), (unsigned)((k.cin + kConvN - 1) / kConvN));
-        conv_fwd_kernel<<<grid, 128, 0, st>>>(go, k.cout, d_wt, nullptr, gin, k.cin, D >> l, H >> l, W >> l, 0);
+        tile_weights_kernel<<<grid_for(27LL * k.cin * k.cout), 256, 0, st>>>(d_pb + k.w, k.cin, k.cout, 1, d_wt);
+        conv_tiles(go, k.cout, nullptr, gin, k.cin, l, false);
     }
 }
 

@@ -3,6 +3,7 @@
     python -m phasecon_b200.run_workload [--workload 4d|3d] [--iters N] [--sv S] [--warps W]
                                          [--refresh] [--cost] [--ch-steps K]
     python -m phasecon_b200.run_workload --workload pc [--iters N] [--views V] [--nms-order 0|1]
+    python -m phasecon_b200.run_workload --workload unet [--iters N]
 
 Builds the seeded workload (phasecon_b200/workloads.py). For 4d / 3d: one
 session with the given schedule (autotuned when --sv/--warps are 0), N ICD
@@ -10,7 +11,8 @@ iterations from zero, then optionally one FP64 error-sinogram refresh and one
 FP64 cost evaluation; --ch-steps shortens the phantom simulation (same array
 sizes) to keep the number of unrelated kernel launches small under a
 profiler. For pc: the phase-contrast scan, Paganin retrieval, the ADMM start
-and N phase-retrieval iterations of every view.
+and N phase-retrieval iterations of every view. For unet: N training steps and
+one inference of the warm-start network on a seeded 32 x 256 x 256 frame.
 """
 from __future__ import annotations
 
@@ -23,7 +25,7 @@ from . import workloads as W
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("--workload", default="4d", choices=["4d", "3d", "pc"])
+    ap.add_argument("--workload", default="4d", choices=["4d", "3d", "pc", "unet"])
     ap.add_argument("--views", type=int, default=180)
     ap.add_argument("--nms-order", type=int, default=0)
     ap.add_argument("--iters", type=int, default=2)
@@ -35,6 +37,8 @@ def main(argv=None):
     a = ap.parse_args(argv)
     if a.workload == "pc":
         return run_pc(a)
+    if a.workload == "unet":
+        return run_unet(a)
     if a.workload == "4d":
         pb, _, p = W.config_4d(ch_steps=a.ch_steps)
     else:
@@ -63,6 +67,28 @@ def run_pc(a):
     print(f"workload pc: views {a.views} iters {a.iters} sd_steps {st.sd_steps} transforms "
           f"{st.fresnel_transforms} device {st.kernel_ms:.1f} ms wall {time.perf_counter() - t0:.3f}s "
           f"cost[0] {costs[0, :a.iters + 1]}")
+
+
+def run_unet(a):
+    import numpy as np
+    import torch
+
+    from .warmstart import UNet
+    rng = np.random.default_rng(0)
+    x = torch.from_numpy((0.01 + 0.01 * rng.random((32, 256, 256))).astype(np.float32)).cuda()
+    t = x * 1.1
+    net = UNet(16)
+    net.input_scale = 50.0
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(a.iters):
+        loss = net.train_step(x, t, 1e-3)
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    net.forward(x)
+    torch.cuda.synchronize()
+    print(f"workload unet: {a.iters} training steps {1e3 * (t1 - t0) / max(a.iters, 1):.1f} ms/step, "
+          f"inference {1e3 * (time.perf_counter() - t1):.1f} ms, loss {loss:.4g}")
 
 
 if __name__ == "__main__":
