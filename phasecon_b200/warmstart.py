@@ -195,10 +195,31 @@ def training_pair(seed: int, n_xy: int = 256, n_z: int = 32, kind: str = "mixed"
     return fbp.astype(np.float32), target.astype(np.float32), obj.astype(np.float32)
 
 
+def training_pairs_4d(seed: int, ch_steps: int | None = None, rel: float = 1e-4):
+    """The 8 (FBP frame, converged frame) pairs of one seeded 4-D scan with the
+    4-D workload's geometry and schedule (Cahn-Hilliard evolution, 1,024
+    interlaced views, Poisson I0 = 2e4): targets from plain GPU ICD on the
+    whole 4-D problem, temporal prior included."""
+    from .workloads import config_4d
+    rng = np.random.default_rng(seed)
+    steps = ch_steps if ch_steps is not None else int(rng.integers(2000, 8001))
+    pb, _, p = config_4d(seed=seed, ch_steps=steps)
+    o = get_options()
+    o.mrf_p = p
+    s = Session(pb, options=o)
+    fbp = s.fbp()
+    s.set_object(np.zeros(s.shape, np.float32))
+    converge(s, rel=rel)
+    target = s.get_object()
+    s.close()
+    return [(fbp[f], target[f]) for f in range(fbp.shape[0])]
+
+
 def train(net: UNet, pairs, steps: int, lr: float = 1e-3, seed: int = 0, log_every: int = 0):
-    """Adam steps over randomly drawn (input, target) pairs of host arrays;
-    returns the loss history. The network's input scale is set so that it sees
-    values of order one."""
+    """Adam steps over randomly drawn (input, target) pairs of host arrays,
+    learning rate on a cosine schedule from `lr` down to lr / 100; returns the
+    loss history. The network's input scale is set so that it sees values of
+    order one."""
     import torch
     rng = np.random.default_rng(seed)
     net.input_scale = 1.0 / max(float(np.mean([np.abs(t).max() for _, t in pairs])), 1e-12)
@@ -207,7 +228,8 @@ def train(net: UNet, pairs, steps: int, lr: float = 1e-3, seed: int = 0, log_eve
     hist = []
     for s in range(steps):
         x, t = dev[int(rng.integers(0, len(dev)))]
-        hist.append(net.train_step(x, t, lr))
+        lr_s = lr * (0.01 + 0.99 * 0.5 * (1.0 + np.cos(np.pi * s / max(1, steps))))
+        hist.append(net.train_step(x, t, float(lr_s)))
         if log_every and (s + 1) % log_every == 0:
             print(f"step {s + 1}: loss {np.mean(hist[-log_every:]):.4g}", flush=True)
     return hist
