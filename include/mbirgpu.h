@@ -70,6 +70,9 @@ typedef struct {
     int32_t sv_colors;       /* super-voxel colouring: K x K colour classes, K = 2 (4 phases per
                                 sweep) or 4 (16 phases: same-colour super-voxels twice as far
                                 apart); 0 = autotuned */
+    int32_t stage_records;   /* 1 (default): the ICD sweep copies each next voxel column's A
+                                records into shared memory while it updates the current one;
+                                0: records are read from global memory where they are used */
 } mbirgpu_options;
 
 /* Defaults as listed above. */
@@ -377,6 +380,58 @@ int mbirgpu_pc_nms_sweep(mbirgpu_pc_session *s);
  * phase-retrieval cost before and after each iteration, NaN after a view
  * stops), iters [proj_num] (may be NULL). */
 int mbirgpu_pc_run(mbirgpu_pc_session *s, double *costs, int32_t *iters, mbirgpu_pc_stats *stats);
+
+/* --------------------------------------------------------------------------
+ * Phase-contrast data simulator.
+ *
+ * Drop-in for phcontomo_forward_project of PCMBIR_3D/XT_Engine.c:199-253
+ * (include/pcmbir4d.h:36), which runs ForwardProject
+ * (PCMBIR_3D/XT_genSinogram.c:59-343) on the geometry of
+ * initPhantomStructures (PCMBIR_3D/XT_Init.c:611-684): the absorption and
+ * refractive-index-decrement phantoms [phantom_z][phantom_xy][phantom_xy]
+ * (float32 files) are projected with the A matrix times the wavenumber, the
+ * exit field sqrt(expected_count) e^{-P_mag} e^{-i P_phase} is propagated by
+ * the windowed Fresnel transform, |.|^2 is averaged over the
+ * (phantom_z / proj_rows) x (phantom_xy / proj_cols) phantom pixels of each
+ * detector pixel, and noise |m + sqrt|m| n| is added with n the reference's
+ * randlib normal() sequence after srandom2(761521). *measurements
+ * ([proj_num][proj_rows][proj_cols]) and *brights ([proj_rows][proj_cols],
+ * = expected_count) are caller-allocated, as in the reference driver
+ * (reconstruct/phase_data/XT_Main.c:130-134). With write_files the
+ * reference's SimMagProjs.bin / SimPhaseProjs.bin (FP64
+ * [proj_num][phantom_z][phantom_xy]) and mag_phantom.bin / phase_phantom.bin
+ * (FP64 phantoms) are written to the working directory. Returns 0 or -1.
+ * ------------------------------------------------------------------------ */
+int phcontomo_forward_project(float **measurements, float **brights, float *proj_angles, int32_t proj_rows,
+                              int32_t proj_cols, int32_t proj_num, float vox_wid, float rot_center,
+                              float obj2det_dist, float light_energy, float pag_regparam, FILE *debug_msg_ptr);
+
+/* The simulator's compile-time constants of PCMBIR_3D/XT_Constants.h as
+ * run-time settings; defaults are the reference's values. */
+typedef struct {
+    char mag_phantom_path[1024];   /* MAG_PHANTOM_FILEPATH (:91) */
+    char phase_phantom_path[1024]; /* PHASE_PHANTOM_FILEPATH (:92) */
+    int32_t phantom_xy;            /* PHANTOM_XY_SIZE (:203): 512 */
+    int32_t phantom_z;             /* PHANTOM_Z_SIZE (:204): 128 */
+    float expected_count;          /* EXPECTED_COUNT_MEASUREMENT (:89): 2500 */
+    int32_t write_files;           /* the reference's output files (default 1) */
+} mbirgpu_pc_sim_options;
+
+void mbirgpu_pc_sim_default_options(mbirgpu_pc_sim_options *opt);
+int mbirgpu_pc_sim_set_options(const mbirgpu_pc_sim_options *opt);
+int mbirgpu_pc_sim_get_options(mbirgpu_pc_sim_options *opt);
+
+/* The simulator on phantoms in host memory (no files are read; files are
+ * written only if opt->write_files). sim_mag_projs / sim_phase_projs
+ * ([proj_num][phantom_z][phantom_xy] FP64, the reference's projs_real /
+ * projs_imag) and measurement_avg may be NULL. opt NULL = the current
+ * settings. No counterpart in the reference, which reads the phantoms from
+ * fixed paths. */
+int mbirgpu_pc_simulate(const float *mag_phantom, const float *phase_phantom, const mbirgpu_pc_sim_options *opt,
+                        float *measurements, float *brights, const float *proj_angles, int32_t proj_rows,
+                        int32_t proj_cols, int32_t proj_num, float vox_wid, float rot_center, float obj2det_dist,
+                        float light_energy, double *sim_mag_projs, double *sim_phase_projs,
+                        double *measurement_avg);
 
 #ifdef __cplusplus
 }

@@ -500,3 +500,55 @@ def ref_pc_filter(g):
     f, d = np.zeros(27), np.zeros(4)
     ref_pc_lib().ref_pc_filter(C.byref(pc_params(g)), f, d)
     return f.reshape(3, 3, 3), d.reshape(2, 2)
+
+
+def ref_pc_forward_project(mag, phase, angles, proj_rows, proj_cols, vox_wid, rot_center, obj2det_dist,
+                           light_energy, pag_regparam, workdir):
+    """The reference's own phcontomo_forward_project (PCMBIR_3D/XT_Engine.c:199-253,
+    XT_genSinogram.c:59-343) on phantoms mag / phase [P_z][P_xy][P_xy]: the
+    phantoms are written where the patched build reads them
+    (oracle_mag_phantom_input.bin / oracle_phase_phantom_input.bin in
+    `workdir`), the phantom-size globals are set, and the reference runs in
+    `workdir`. Returns (measurements [proj_num][proj_rows][proj_cols], brights,
+    SimMagProjs, SimPhaseProjs [proj_num][P_z][P_xy] FP64, mag_phantom,
+    phase_phantom FP64)."""
+    mag = np.ascontiguousarray(mag, np.float32)
+    phase = np.ascontiguousarray(phase, np.float32)
+    P_z, P_xy, _ = mag.shape
+    lib = ref_pc_lib()
+    C.c_int.in_dll(lib, "oracle_ref_phantom_xy").value = P_xy
+    C.c_int.in_dll(lib, "oracle_ref_phantom_z").value = P_z
+    fp = C.POINTER(C.c_float)
+    lib.phcontomo_forward_project.argtypes = [C.POINTER(fp), C.POINTER(fp), _f32p, C.c_int32, C.c_int32, C.c_int32,
+                                              C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, C.c_void_p]
+    lib.phcontomo_forward_project.restype = C.c_int
+    V = len(angles)
+    meas = np.zeros(V * proj_rows * proj_cols, np.float32)
+    br = np.zeros(proj_rows * proj_cols, np.float32)
+    pm, pb = meas.ctypes.data_as(fp), br.ctypes.data_as(fp)
+    libc = C.CDLL(None)
+    libc.fopen.restype = C.c_void_p
+    libc.fopen.argtypes = [C.c_char_p, C.c_char_p]
+    libc.fclose.argtypes = [C.c_void_p]
+    cwd = os.getcwd()
+    os.makedirs(workdir, exist_ok=True)
+    os.chdir(workdir)
+    dbg = libc.fopen(b"debug.txt", b"w")
+    try:
+        mag.tofile("oracle_mag_phantom_input.bin")
+        phase.tofile("oracle_phase_phantom_input.bin")
+        rc = lib.phcontomo_forward_project(C.byref(pm), C.byref(pb), np.ascontiguousarray(angles, np.float32),
+                                           proj_rows, proj_cols, V, vox_wid, rot_center, obj2det_dist, light_energy,
+                                           pag_regparam, dbg)
+        libc.fclose(dbg)
+        if rc != 0:
+            raise RuntimeError("reference phcontomo_forward_project failed")
+        n = V * P_z * P_xy
+        out = (meas.reshape(V, proj_rows, proj_cols), br.reshape(proj_rows, proj_cols),
+               np.fromfile("SimMagProjs.bin", np.float64, n).reshape(V, P_z, P_xy),
+               np.fromfile("SimPhaseProjs.bin", np.float64, n).reshape(V, P_z, P_xy),
+               np.fromfile("mag_phantom.bin", np.float64).reshape(P_z, P_xy, P_xy),
+               np.fromfile("phase_phantom.bin", np.float64).reshape(P_z, P_xy, P_xy))
+    finally:
+        os.chdir(cwd)
+    return out

@@ -36,6 +36,7 @@ class PcGeom:
     mrf_q: float = 2.0
     mu: float = 0.5  # ADMM_mu, XT_Init.c:496
     nu: float = 0.5  # ADMM_nu, XT_Init.c:497
+    sim_window: bool = False  # the data simulator's window (initPhantomStructures, XT_Init.c:677)
 
     @property
     def wavelength(self) -> float:  # XT_Init.c:258
@@ -46,7 +47,9 @@ class PcGeom:
         return 2 * math.pi / self.wavelength
 
     @property
-    def window_sigma(self) -> float:  # XT_Init.c:530
+    def window_sigma(self) -> float:  # XT_Init.c:530; the simulator's XT_Init.c:677
+        if self.sim_window:
+            return 1.0 / math.sqrt(0.5 * self.wavelength * self.distance)
         return 2.0 / math.sqrt(self.wavelength * self.distance)
 
     def freqs(self, scale: float = 1.0):
@@ -327,3 +330,199 @@ def estimate_projection(g: PcGeom, y, om, D, zr, zi, lam, w, pret_iters=100, sd_
         if dual < pret_thresh and it > 1:
             break
     return zr, zi, w, v, om, costs
+
+
+# ---- data simulator (phcontomo_forward_project) -----------------------------------------------
+
+PM_MODULUS = 2147483647  # MAXPRIME, PCMBIR_3D/randlib.c:42
+PM_MULTIPLIER = 16807
+SIM_NOISE_SEED = 761521  # srandom2 seed of phcontomo_forward_project, PCMBIR_3D/XT_Engine.c:212
+
+
+def random2_states(seed: int, n: int) -> np.ndarray:
+    """States x_1..x_n of randlib's random2() after srandom2(seed)
+    (PCMBIR_3D/randlib.c:119-141, 168-174): x_k = seed 16807^k mod (2^31 - 1);
+    random2() returns x_k / (2^31 - 1). Computed in blocks: the first B
+    states one by one, then each block from the previous one times 16807^B."""
+    B = 4096
+    first = np.empty(min(n, B), np.uint64)
+    x = seed % PM_MODULUS
+    for i in range(first.size):
+        x = (x * PM_MULTIPLIER) % PM_MODULUS
+        first[i] = x
+    if n <= B:
+        return first
+    out = np.empty(n, np.uint64)
+    out[:B] = first
+    step = np.uint64(pow(PM_MULTIPLIER, B, PM_MODULUS))
+    for s in range(B, n, B):
+        e = min(n, s + B)
+        out[s:e] = (out[s - B:e - B] * step) % np.uint64(PM_MODULUS)
+    return out
+
+
+def randlib_normals(n: int, seed: int = SIM_NOISE_SEED) -> np.ndarray:
+    """The first n values of randlib's normal() (PCMBIR_3D/randlib.c:208-225)
+    after srandom2(seed), from a fresh process: pair p draws theta = 2 pi u and
+    r = sqrt(-2 log u') from two consecutive random2() values and returns
+    r cos(theta), then r sin(theta)."""
+    pairs = (n + 1) // 2
+    x = random2_states(seed, 2 * pairs).astype(np.float64) / PM_MODULUS
+    theta = 2 * 3.14159265358979323846 * x[0::2]
+    r = np.sqrt(-2 * np.log(x[1::2]))
+    out = np.empty(2 * pairs)
+    out[0::2] = r * np.cos(theta)
+    out[1::2] = r * np.sin(theta)
+    return out[:n]
+
+
+def sim_detector(intensity: np.ndarray, proj_rows: int, proj_cols: int, seed: int = SIM_NOISE_SEED) -> np.ndarray:
+    """The detector stage of ForwardProject (PCMBIR_3D/XT_genSinogram.c:239-262):
+    intensity |F|^2 [V][N_r][N_t] (phantom resolution) averaged over the
+    (N_t / proj_rows) x (N_r / proj_cols) pixels of each detector pixel (a
+    float32 running sum of FP64 terms, t outer, r inner), then
+    m <- |m + sqrt|m| n| with n the normal() sequence in (view, row, col) order."""
+    V, R, Cn = intensity.shape
+    rs, ts = R // proj_cols, Cn // proj_rows
+    m = np.zeros((V, proj_rows, proj_cols), np.float32)
+    for ti in range(ts):
+        for ri in range(rs):
+            blk = intensity[:, ri:rs * proj_cols:rs, ti:ts * proj_rows:ts]  # [V][col][row]
+            m = (m.astype(np.float64) + blk.transpose(0, 2, 1)).astype(np.float32)
+    m = (m / np.float32(ts * rs)).astype(np.float32)
+    n = randlib_normals(m.size, seed).reshape(m.shape)
+    md = m.astype(np.float64)
+    return np.abs(md + np.sqrt(np.abs(md)) * n).astype(np.float32)
+
+
+def sim_geometry(P_xy: int, P_z: int, proj_rows: int, proj_cols: int, vox_wid: float, energy_kev: float,
+                 distance: float) -> PcGeom:
+    """Transform geometry of the simulator (initPhantomStructures, XT_Init.c:611-684):
+    N_r = P_xy rows of pitch vox_wid proj_cols / P_xy, N_t = P_z columns of
+    pitch vox_wid proj_rows / P_z, window sigma 1 / sqrt(lambda z / 2)."""
+    return PcGeom(rows=P_xy, cols=P_z, delta_rows=float(np.float32(vox_wid)) * proj_cols / P_xy,
+                  delta_cols=float(np.float32(vox_wid)) * proj_rows / P_z, energy_kev=float(np.float32(energy_kev)),
+                  distance=float(np.float32(distance)), sim_window=True)
+
+
+def sim_from_projections(pm: np.ndarray, pp: np.ndarray, g: PcGeom, proj_rows: int, proj_cols: int,
+                         count: float = 2500.0) -> np.ndarray:
+    """Measurements of ForwardProject (XT_genSinogram.c:212-262) from the FP64
+    projections P_mag, P_phase [V][N_t][N_r] (the reference's SimMagProjs /
+    SimPhaseProjs): field sqrt(count) e^{-P_mag} (cos, sin)(-P_phase) per view
+    ([N_r][N_t]), the windowed Fresnel transform, |.|^2, then sim_detector."""
+    e = np.exp(-pm)
+    a_r, a_i = e * np.cos(-pp), e * np.sin(-pp)
+    s = math.sqrt(count)
+    field = (a_r * s - a_i * 0.0) + 1j * (a_r * 0.0 + a_i * s)
+    field = field.transpose(0, 2, 1)  # [V][N_r][N_t]
+    F = np.fft.ifft2(np.fft.fft2(field, axes=(1, 2)) * g.transfer(False)[None], axes=(1, 2))
+    inten = F.real * F.real + F.imag * F.imag
+    return sim_detector(inten, proj_rows, proj_cols)
+
+
+SIM_BINS = 256      # DETECTOR_RESPONSE_BINS of PCMBIR_3D/XT_Constants.h:163
+SIM_BEAM_RES = 256  # BEAM_RESOLUTION, XT_Constants.h:162
+SIM_PROFILE_RES = 1536  # PROFILE_RESOLUTION, XT_Constants.h:161
+
+
+def sim_project(mag: np.ndarray, phase: np.ndarray, angles, proj_rows: int, proj_cols: int, vox_wid: float,
+                rot_center: float, light_energy: float):
+    """FP64 projections P_mag, P_phase [V][N_t][N_r] of ForwardProject
+    (PCMBIR_3D/XT_genSinogram.c:141-181) on the geometry of
+    initPhantomStructures (XT_Init.c:611-684): A columns of
+    calcAMatrixColumnforAngle x wavenumber (XT_AMatrix.c:50-110) from the
+    detector response of DetectorResponseProfile (XT_Profile.c:47-180) and the
+    voxel-line response of storeVoxelLineResponse (XT_Profile.c:182-297).
+    Sums run in another order than the reference's (agreement ~1e-15)."""
+    P_z, P_xy, _ = mag.shape
+    vox, rot = float(np.float32(vox_wid)), float(np.float32(rot_center))
+    lam = PLANCK_KEV_S * LIGHT_SPEED_UM_S / float(np.float32(light_energy))
+    k = 2 * math.pi / lam
+    LR, LT = vox * proj_cols, vox * proj_rows
+    RC = rot * (P_xy // proj_cols)
+    dr, dt = LR / P_xy, LT / P_z
+    R0, RMax, T0, TMax = -RC * dr, (P_xy - RC) * dr, -LT / 2.0, LT / 2.0
+    dxy, dz = dr, dt
+    x0, y0, z0 = R0, -LR / 2.0, T0
+    off_r = (dxy / math.sqrt(2.0) + dr / 2.0) / SIM_BINS
+    off_t = ((dz / 2) + dt / 2) / SIM_BINS
+    # voxel-line response Z[slice][t]
+    ht = np.zeros(SIM_BINS + 1)
+    for i in range(SIM_BINS):
+        c = i * off_t
+        h = dt if c <= (dz / 2 - dt / 2) else -c + dz / 2 + dt / 2
+        if dz < dt:
+            h = dz if c <= dt / 2 - dz / 2 else -c + dz / 2 + dt / 2
+        ht[i] = max(h, 0.0) / dt
+    Z = np.zeros((P_z, P_z))
+    for i in range(P_z):
+        t = (i + 0.5) * dz + z0
+        tmin = t - dz / 2 if (t - dz / 2) > T0 else T0
+        tmax = t + dz / 2 if (t + dz / 2) <= TMax else TMax
+        lo, hi = max(int(math.floor((tmin - T0) / dt)), 0), min(int(math.floor((tmax - T0) / dt)), P_z - 1)
+        for it in range(lo, hi + 1):
+            d = abs(((it + 0.5) * dt + T0) - t)
+            idx = int(math.floor(d / off_t))
+            if idx < SIM_BINS:
+                Z[i, it] = ((idx + 1) * off_t - d) / off_t * ht[idx] + (d - idx * off_t) / off_t * ht[idx + 1]
+    # z response of every column: p[t][col]
+    pm = np.einsum("st,sc->tc", Z, mag.reshape(P_z, -1).astype(np.float64))
+    pp = np.einsum("st,sc->tc", Z, phase.reshape(P_z, -1).astype(np.float64))
+    beam = 0.54 - 0.46 * np.cos((2 * math.pi / SIM_BEAM_RES) * np.arange(SIM_BEAM_RES))
+    beam = beam / beam.sum()
+    rows_, cols_ = np.meshgrid(np.arange(P_xy), np.arange(P_xy), indexing="ij")
+    x = (x0 + (cols_.ravel() + 0.5) * dxy)
+    y = (y0 + (rows_.ravel() + 0.5) * dxy)
+    V = len(angles)
+    out_m = np.zeros((V, P_z, P_xy))
+    out_p = np.zeros((V, P_z, P_xy))
+    jprof = 2.0 * np.arange(SIM_PROFILE_RES) / SIM_PROFILE_RES
+    for v in range(V):
+        a = float(np.float32(angles[v]))
+        cs, sn = math.cos(a), math.sin(a)
+        ang = a
+        while ang > math.pi / 2:
+            ang -= math.pi / 2
+        while ang < 0:
+            ang += math.pi / 2
+        peak = dxy / math.cos(ang) if ang <= math.pi / 4 else dxy / math.cos(math.pi / 2 - ang)
+        t45 = math.cos(math.pi / 4)
+        d1, d2 = t45 * math.cos(math.pi / 4 - ang), t45 * abs(math.cos(math.pi / 4 + ang))
+        lc, ln, rn, rc = 1 - d1, 1 - d2, 1 + d2, 1 + d1
+        prof = np.where((jprof <= lc) | (jprof >= rc), 0.0,
+                        np.where(jprof > rn, peak * (rc - jprof) / (rc - rn),
+                                 np.where(jprof >= ln, peak, peak * (jprof - lc) / (ln - lc))))
+        r_beam = -dr / 2 + np.arange(SIM_BEAM_RES) * (dr / SIM_BEAM_RES)
+        rmin_b = np.arange(SIM_BINS)[:, None] * off_r - dxy
+        pidx = np.floor((r_beam[None, :] - rmin_b) * (SIM_PROFILE_RES / (2 * dxy))).astype(np.int64)
+        ok = (pidx >= 0) & (pidx <= SIM_PROFILE_RES - 1)
+        H = np.zeros(SIM_BINS + 1)
+        H[:SIM_BINS] = np.where(ok, prof[np.clip(pidx, 0, SIM_PROFILE_RES - 1)] * beam[None, :], 0.0).sum(1)
+        r = x * cs - y * sn
+        live = ~((r + dxy < R0) | (r - dxy > RMax))
+        imin = np.maximum(np.floor((r - dxy - R0) / dr).astype(np.int64), 0)
+        imax = np.minimum(np.floor((r + dxy - R0) / dr).astype(np.int64), P_xy - 1)
+        for o in range(3):
+            j = imin + o
+            sel = live & (j <= imax)
+            dd = np.abs(r - (R0 + (j + 0.5) * dr))
+            b = np.floor(dd / off_r).astype(np.int64)
+            sel &= (b >= 0) & (b < SIM_BINS)
+            bb = np.clip(b, 0, SIM_BINS - 1)
+            w1 = dd - bb * off_r
+            f1 = ((off_r - w1) * H[bb] + w1 * H[bb + 1]) / off_r
+            sel &= f1 > 0
+            cidx = np.nonzero(sel)[0]
+            aval = f1[cidx] * k
+            np.add.at(out_m[v].T, j[cidx], aval[:, None] * pm[:, cidx].T)
+            np.add.at(out_p[v].T, j[cidx], aval[:, None] * pp[:, cidx].T)
+    return out_m, out_p
+
+
+def simulate(mag, phase, angles, proj_rows, proj_cols, vox_wid, rot_center, obj2det_dist, light_energy,
+             count: float = 2500.0):
+    """The whole simulator (phcontomo_forward_project): (measurements, P_mag, P_phase)."""
+    pm, pp = sim_project(mag, phase, angles, proj_rows, proj_cols, vox_wid, rot_center, light_energy)
+    g = sim_geometry(mag.shape[1], mag.shape[0], proj_rows, proj_cols, vox_wid, light_energy, obj2det_dist)
+    return sim_from_projections(pm, pp, g, proj_rows, proj_cols, count), pm, pp

@@ -18,8 +18,8 @@ BUILD = os.path.join(PKG, "_build")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contract=off", "-I", CSRC,
           "-I", os.path.join(os.path.dirname(PKG), "include")]
-# files whose double-precision geometry must match the reference bit for bit
-NO_FMA = {"kernels_amatrix.cu"}
+# files whose double-precision geometry must round like the reference
+NO_FMA = {"kernels_amatrix.cu", "pc_simulate.cu"}
 
 
 def _nvcc() -> str:

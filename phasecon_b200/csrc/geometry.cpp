@@ -28,19 +28,21 @@ double grid_distance(int a, int b, int c, int d)
 
 // Detector response H_r[view][0..64] (XT_Profile.c:129-218): the voxel's
 // trapezoidal line-integral profile at the view's angle (XT_Profile.c:47-104,
-// stored in float like the reference's Real_arr_t) convolved with a
-// normalised Hamming beam (XT_Profile.c:108-124), sampled every OffsetR.
-void detector_response(const Geom &g, const float *angles, float *H_r)
+// stored as the reference's Real_arr_t: float in MBIR_4D, double in
+// PCMBIR_3D) convolved with a normalised Hamming beam (XT_Profile.c:108-124),
+// sampled every OffsetR.
+template <typename T>
+void detector_response_t(const Geom &g, const float *angles, T *H_r, int bins, int beam_res)
 {
-    std::vector<double> beam(kBeamRes);
-    std::vector<float> prof(kProfileRes);
+    std::vector<double> beam(beam_res);
+    std::vector<T> prof(kProfileRes);
     double total = 0;
-    for (int i = 0; i < kBeamRes; i++) {
-        beam[i] = 0.54 - 0.46 * std::cos((2 * 3.14159265358979323846 / kBeamRes) * i);
+    for (int i = 0; i < beam_res; i++) {
+        beam[i] = 0.54 - 0.46 * std::cos((2 * 3.14159265358979323846 / beam_res) * i);
         total = total + beam[i];
     }
-    for (int i = 0; i < kBeamRes; i++) beam[i] /= total;
-    const double r0 = -(g.delta_r) / 2, step = (g.delta_r) / kBeamRes;
+    for (int i = 0; i < beam_res; i++) beam[i] /= total;
+    const double r0 = -(g.delta_r) / 2, step = (g.delta_r) / beam_res;
     const double to_bin = (kProfileRes) / (2 * g.delta_xy);
     for (int v = 0; v < g.N_p; v++) {
         double ang = angles[v];
@@ -53,29 +55,38 @@ void detector_response(const Geom &g, const float *angles, float *H_r)
         const double left_corner = 1 - d1, left_near = 1 - d2, right_near = 1 + d2, right_corner = 1 + d1;
         for (int j = 0; j < kProfileRes; j++) {
             const double t = 2.0 * j / kProfileRes;
-            float val;
+            T val;
             if (t <= left_corner || t >= right_corner) val = 0;
-            else if (t > right_near) val = (float)(peak * (right_corner - t) / (right_corner - right_near));
-            else if (t >= left_near) val = (float)peak;
-            else val = (float)(peak * (t - left_corner) / (left_near - left_corner));
+            else if (t > right_near) val = (T)(peak * (right_corner - t) / (right_corner - right_near));
+            else if (t >= left_near) val = (T)peak;
+            else val = (T)(peak * (t - left_corner) / (left_near - left_corner));
             prof[j] = val;
         }
-        float *h = H_r + (size_t)v * (kRespBins + 1);
-        for (int i = 0; i < kRespBins; i++) {
+        T *h = H_r + (size_t)v * (bins + 1);
+        for (int i = 0; i < bins; i++) {
             const double center = i * g.OffsetR, rmin = center - g.delta_xy;
             double acc = 0;
-            for (int p = 0; p < kBeamRes; p++) {
+            for (int p = 0; p < beam_res; p++) {
                 const double r = r0 + p * step;
                 const int idx = (int)std::floor((r - rmin) * to_bin);
                 if (idx >= 0 && idx <= kProfileRes - 1) acc += (prof[idx] * beam[p]);
             }
-            h[i] = (float)acc;
+            h[i] = (T)acc;
         }
-        h[kRespBins] = 0.0f;
+        h[bins] = 0;
     }
 }
 
 }  // namespace
+
+void detector_response(const Geom &g, const float *angles, float *H_r)
+{
+    detector_response_t<float>(g, angles, H_r, kRespBins, kBeamRes);
+}
+void detector_response_f64(const Geom &g, const float *angles, double *H_r, int bins, int beam_res)
+{
+    detector_response_t<double>(g, angles, H_r, bins, beam_res);
+}
 
 std::string build_setup(HostSetup &hs, const ProblemDesc &pd, const float *angles, const float *proj_times,
                         const float *recon_times, int mult_xy, int mult_z)

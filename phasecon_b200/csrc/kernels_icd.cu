@@ -86,6 +86,29 @@ __device__ __forceinline__ Rec<KW> load_rec(const uint32_t *p)
 }
 
 template <int KW>
+__device__ __forceinline__ Rec<KW> load_rec_smem(const uint32_t *p)
+{
+    Rec<KW> r;
+    const uint4 *q = reinterpret_cast<const uint4 *>(p);
+#pragma unroll
+    for (int i = 0; i < KW; i++) r.w[i] = q[i];
+    return r;
+}
+
+// Copy a column's A records (nwords 32-bit words, a multiple of 4, 16-byte
+// aligned on both sides) into shared memory with cp.async; the copies land
+// while the CTA works on the current column and are waited for (per thread,
+// cp.async.wait_all) before the barrier that precedes their first use.
+__device__ __forceinline__ void stage_records(uint32_t *dst, const uint32_t *src, int nwords)
+{
+    const unsigned base = (unsigned)__cvta_generic_to_shared(dst);
+    for (int i = threadIdx.x * 4; i < nwords; i += blockDim.x * 4)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(base + 4u * i), "l"(src + i) : "memory");
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+__device__ __forceinline__ void wait_staged() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+template <int KW>
 __device__ __forceinline__ float rec_val(const Rec<KW> &r, int q)
 {
     // word 1 + q of the record
@@ -158,15 +181,19 @@ __device__ __forceinline__ void flush_counts(IcdCount &cnt, IcdStats *stats)
 // cooperates (see the file comment for the four passes per column).
 // KW: 16-byte words per A record (1, 2, 3 for voxel scale 1, 2, 4);
 // kUnroll: views whose records and sinogram entries are in flight together;
-// VEC: consecutive detector rows one lane owns (4 when N_t % 4 == 0, else 2).
-template <int KW, int kUnroll, int VEC>
+// VEC: consecutive detector rows one lane owns (4 when N_t % 4 == 0, else 2);
+// kStaged: the column's records are read from shared memory (srec: two
+// buffers of stage_words words), the next column's copied in with cp.async
+// while the current one is updated, so the theta pass waits on one global
+// round trip per view group instead of two and the apply pass on none.
+template <int KW, int kUnroll, int VEC, bool kStaged>
 __device__ __forceinline__ void icd_update_sv(const Geom &g, const IcdLaunch &L, const IcdConst &K,
                                               const uint32_t *__restrict__ table,
                                               const int32_t *__restrict__ view_first,
                                               const uint8_t *__restrict__ mask, float *__restrict__ x,
                                               float *__restrict__ err, const float *__restrict__ wgt,
                                               float *__restrict__ mag, int f, int sx, int sy, IcdSmem &S,
-                                              IcdCount &cnt)
+                                              IcdCount &cnt, uint32_t *srec, int stage_words)
 {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, W = blockDim.x >> 5;
     const int NX = g.N_x, NY = g.N_y, NZ = g.N_z, NT = g.N_t, MZ = g.z_overlap;
@@ -221,17 +248,19 @@ __device__ __forceinline__ void icd_update_sv(const Geom &g, const IcdLaunch &L,
     }
     __syncthreads();
     const int ncols = S.ncols;
+    const size_t rec_frame = (size_t)fv0 * nxy;
+    if (kStaged && ncols > 0) stage_records(srec, table + (rec_frame + (size_t)S.order[0] * nv) * RW, nv * RW);
 
     for (int ci = 0; ci < ncols; ci++) {
         const int c = S.order[ci];
         const int j = c / NX, k = c - j * NX;
         const size_t col_off = ((size_t)f * nxy + c) * NZ;
-        const uint32_t *col_rec = table + ((size_t)fv0 * nxy + (size_t)c * nv) * RW;
+        const uint32_t *col_rec = kStaged ? srec + (ci & 1) * stage_words : table + (rec_frame + (size_t)c * nv) * RW;
 
         // ---- 1. neighbourhood (sources split over warps) + column activity ------
         int active_pred;
+        const float V = zl ? x[col_off + lane] : 0.0f;  // the column itself (warp 0 reuses it in the solve)
         {
-            const float V = zl ? x[col_off + lane] : 0.0f;
             float num = 0.0f, den = 0.0f;
             int pos = 0;
             for (int s = warp; s < 10; s += W) {
@@ -276,7 +305,14 @@ __device__ __forceinline__ void icd_update_sv(const Geom &g, const IcdLaunch &L,
             // neighbour (in-column neighbours are the column's own values)
             active_pred = !L.zero_skipping || L.iter <= 1 || (zl && V != 0.0f) || pos;
         }
-        if (!__syncthreads_or(active_pred)) {
+        if (kStaged) wait_staged();  // this column's records (issued one column earlier)
+        const int any_active = __syncthreads_or(active_pred);
+        // every thread is past the previous column's apply pass: its record
+        // buffer may be refilled with the next column's
+        if (kStaged && ci + 1 < ncols)
+            stage_records(srec + ((ci + 1) & 1) * stage_words,
+                          table + (rec_frame + (size_t)S.order[ci + 1] * nv) * RW, nv * RW);
+        if (!any_active) {
             if (warp == 0 && zl) cnt.skip++;
             if (warp == 0 && lane == 0) mag[(size_t)f * nxy + c] = 0.0f;
             continue;  // uniform across the CTA
@@ -293,7 +329,8 @@ __device__ __forceinline__ void icd_update_sv(const Geom &g, const IcdLaunch &L,
 #pragma unroll
                     for (int u = 0; u < kUnroll; u++) {
                         const int v = v0 + u * gstride;
-                        if (v < nv) R[u] = load_rec<KW>(col_rec + (size_t)v * RW);
+                        if (v < nv) R[u] = kStaged ? load_rec_smem<KW>(col_rec + (size_t)v * RW)
+                                               : load_rec<KW>(col_rec + (size_t)v * RW);
                         else R[u].w[0].x = 0u;
                     }
 #pragma unroll
@@ -344,7 +381,7 @@ __device__ __forceinline__ void icd_update_sv(const Geom &g, const IcdLaunch &L,
 
         // ---- 3. zero-skipping and solve (warp 0, lane = slice) -------------------
         if (warp == 0) {
-            const float V0 = zl ? x[col_off + lane] : 0.0f;
+            const float V0 = V;
             float numA = 0.0f, denA = 0.0f, t1 = 0.0f, t2 = 0.0f;
             int pos = 0;
             for (int w = 0; w < W; w++) {
@@ -428,7 +465,8 @@ __device__ __forceinline__ void icd_update_sv(const Geom &g, const IcdLaunch &L,
 #pragma unroll
                     for (int u = 0; u < kUnroll; u++) {
                         const int v = v0 + u * gstride;
-                        if (v < nv) R[u] = load_rec<KW>(col_rec + (size_t)v * RW);
+                        if (v < nv) R[u] = kStaged ? load_rec_smem<KW>(col_rec + (size_t)v * RW)
+                                               : load_rec<KW>(col_rec + (size_t)v * RW);
                         else R[u].w[0].x = 0u;
                     }
 #pragma unroll
@@ -456,13 +494,16 @@ __device__ __forceinline__ void icd_update_sv(const Geom &g, const IcdLaunch &L,
 }  // namespace
 
 // One colour phase of one problem: persistent CTAs drain the phase's SV queue.
-template <int KW, int kUnroll, int VEC>
+// With kStaged, the dynamic shared memory holds two record buffers of
+// stage_words words each (the current and the next column's A records).
+template <int KW, int kUnroll, int VEC, bool kStaged>
 __global__ void __launch_bounds__(kMaxWarps * 32, 4) icd_phase_kernel(
     Geom g, IcdLaunch L, IcdConst K, const uint32_t *__restrict__ table, const int32_t *__restrict__ view_first,
     const uint8_t *__restrict__ mask, float *__restrict__ x, float *__restrict__ err, const float *__restrict__ wgt,
-    float *__restrict__ mag, IcdStats *__restrict__ stats, unsigned int *__restrict__ queue)
+    float *__restrict__ mag, IcdStats *__restrict__ stats, unsigned int *__restrict__ queue, int stage_words)
 {
     __shared__ IcdSmem S;
+    extern __shared__ __align__(16) uint32_t s_rec[];
     const int KC = L.colors_k;
     const int hx = (L.n_sv_x + KC - 1) / KC, slots = hx * ((L.n_sv_y + KC - 1) / KC);
     const int n_items = g.N_time * slots;
@@ -479,9 +520,34 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 4) icd_phase_kernel(
         const int sx = KC * (rem % hx) + color % KC;
         const int sy = KC * (rem / hx) + color / KC;
         if (sx >= L.n_sv_x || sy >= L.n_sv_y) continue;  // uniform
-        icd_update_sv<KW, kUnroll, VEC>(g, L, K, table, view_first, mask, x, err, wgt, mag, f, sx, sy, S, cnt);
+        icd_update_sv<KW, kUnroll, VEC, kStaged>(g, L, K, table, view_first, mask, x, err, wgt, mag, f, sx, sy, S,
+                                                 cnt, s_rec, stage_words);
     }
     flush_counts(cnt, stats);
+}
+
+// Record staging needs two buffers of (most views in a frame) x record words;
+// above this size the sweep reads records from global memory instead.
+constexpr int kMaxStageBytes = 16 * 1024;
+
+template <int KW, int U, int VEC, bool kStaged>
+static void launch_staged(const Geom &g, const IcdLaunch &L, const IcdConst &K, const uint32_t *d_table,
+                          const int32_t *d_view_first, const uint8_t *d_mask, float *d_x, float *d_err,
+                          const float *d_w, float *d_mag, IcdStats *d_stats, unsigned int *d_queue, int stage_words,
+                          cudaStream_t st)
+{
+    const int threads = L.warps * 32;
+    const size_t smem = kStaged ? 2 * (size_t)stage_words * sizeof(uint32_t) : 0;
+    int dev = 0, sms = 148, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, icd_phase_kernel<KW, U, VEC, kStaged>, threads, smem);
+    const long long items = (long long)g.N_time * sv_slots(g.N_x, g.N_y, L.sv, L.colors_k);
+    long long grid = (long long)sms * (per_sm > 0 ? per_sm : 1);
+    if (grid > items) grid = items;
+    if (L.max_ctas > 0 && grid > L.max_ctas) grid = L.max_ctas;
+    icd_phase_kernel<KW, U, VEC, kStaged><<<(unsigned)grid, threads, smem, st>>>(
+        g, L, K, d_table, d_view_first, d_mask, d_x, d_err, d_w, d_mag, d_stats, d_queue, stage_words);
 }
 
 template <int KW, int U, int VEC>
@@ -489,17 +555,13 @@ static void launch_kw(const Geom &g, const IcdLaunch &L, const IcdConst &K, cons
                       const int32_t *d_view_first, const uint8_t *d_mask, float *d_x, float *d_err, const float *d_w,
                       float *d_mag, IcdStats *d_stats, unsigned int *d_queue, cudaStream_t st)
 {
-    const int threads = L.warps * 32;
-    int dev = 0, sms = 148, per_sm = 1;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, icd_phase_kernel<KW, U, VEC>, threads, 0);
-    const long long items = (long long)g.N_time * sv_slots(g.N_x, g.N_y, L.sv, L.colors_k);
-    long long grid = (long long)sms * (per_sm > 0 ? per_sm : 1);
-    if (grid > items) grid = items;
-    if (L.max_ctas > 0 && grid > L.max_ctas) grid = L.max_ctas;
-    icd_phase_kernel<KW, U, VEC><<<(unsigned)grid, threads, 0, st>>>(g, L, K, d_table, d_view_first, d_mask, d_x,
-                                                                     d_err, d_w, d_mag, d_stats, d_queue);
+    const int stage_words = g.max_views * g.rec_words;  // a multiple of 4 words: 16-byte aligned buffers
+    if (L.stage_records && 2 * (size_t)stage_words * sizeof(uint32_t) <= (size_t)kMaxStageBytes)
+        launch_staged<KW, U, VEC, true>(g, L, K, d_table, d_view_first, d_mask, d_x, d_err, d_w, d_mag, d_stats,
+                                        d_queue, stage_words, st);
+    else
+        launch_staged<KW, U, VEC, false>(g, L, K, d_table, d_view_first, d_mask, d_x, d_err, d_w, d_mag, d_stats,
+                                         d_queue, 0, st);
 }
 
 IcdConst make_icd_const(const Geom &g)
@@ -595,8 +657,8 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 4) icd_batch_kernel(const Batc
         const int sx = K * (rem % hx) + color % K;
         const int sy = K * (rem / hx) + color / K;
         if (sx >= P.L.n_sv_x || sy >= P.L.n_sv_y) continue;
-        icd_update_sv<KW, kUnroll, VEC>(P.g, P.L, P.K, P.table, P.view_first, P.mask, P.x, P.err, P.w, P.mag, f, sx,
-                                        sy, S, cnt);
+        icd_update_sv<KW, kUnroll, VEC, false>(P.g, P.L, P.K, P.table, P.view_first, P.mask, P.x, P.err, P.w, P.mag,
+                                               f, sx, sy, S, cnt, nullptr, 0);
     }
     if (cur >= 0) flush_counts(cnt, P.stats);
 }
@@ -647,7 +709,7 @@ int icd_grid(int warps)
     int dev = 0, sms = 148, per_sm = 1;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, icd_phase_kernel<1, 2, 4>, warps * 32, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, icd_phase_kernel<1, 2, 4, false>, warps * 32, 0);
     return sms * (per_sm > 0 ? per_sm : 1);
 }
 

@@ -51,6 +51,12 @@ struct ProblemDesc {
     double mrf_p, mrf_q, alpha;
 };
 
+// Detector response H_r [N_p][bins + 1] of the views' angles for g's geometry
+// (XT_Profile.c:129-218): MBIR_4D's (float, 64 bins, a 512-sample beam) and
+// PCMBIR_3D's (double; 256 bins and a 256-sample beam, PCMBIR_3D/XT_Constants.h:162-163).
+void detector_response(const Geom &g, const float *angles, float *H_r);
+void detector_response_f64(const Geom &g, const float *angles, double *H_r, int bins, int beam_res);
+
 // Returns "" on success, else the failure message.
 std::string build_setup(HostSetup &hs, const ProblemDesc &pd, const float *angles, const float *proj_times,
                         const float *recon_times, int mult_xy, int mult_z);
@@ -106,6 +112,7 @@ struct IcdLaunch {
     int perm;             // queue order inside a frame: SV slot = (queue index * perm) mod slots
     int colors_k;         // K x K colour classes; phase p updates colour (p + frame) mod K^2
     long long max_ctas;   // cap on the persistent grid (sv_max_concurrent); 0 = none
+    int stage_records;    // prefetch each next column's A records into shared memory (cp.async)
 };
 
 // SV slots of one colour per frame and the items (all frames) of one phase.

@@ -1,6 +1,7 @@
 // Internal declarations of the phase-contrast (PCMBIR) part of libmbirgpu.
 #pragma once
 #include <cstdint>
+#include <vector>
 #include <cuda_runtime.h>
 
 namespace mbirgpu {
@@ -77,5 +78,17 @@ __global__ void pc_nms(PcDims d, PcArgs A, const __grid_constant__ PcPrior P, in
                        float threshold);
 __global__ void pc_nms_wavefront(PcDims d, PcArgs A, const __grid_constant__ PcPrior P, int max_iter,
                                  float threshold);
+
+// Launch geometry of the three-pass transform for V views of R x C (powers of
+// two): fills d's sizes and per-CTA tiles, the dynamic shared memory of the
+// row and column passes, and raises the kernels' shared-memory limits.
+int pc_transform_dims(PcDims &d, int V, int R, int C, size_t *smem_rows, size_t *smem_cols);
+// exp(-2 pi i m / nmax), m < nmax / 2, computed in double and rounded once
+std::vector<float2> pc_twiddles(int nmax);
+// One Fresnel-type transform of every view: prologue + FFT along C, FFT along
+// R x transfer table x inverse FFT along R, inverse FFT along C / N + epilogue.
+void pc_transform(const PcDims &d, PcArgs A, size_t smem_rows, size_t smem_cols, int prologue, const float2 *in,
+                  const float2 *table, int epilogue, float2 *out, int acc_slot, cudaStream_t st);
+int fail(const char *fmt, ...);
 
 }  // namespace mbirgpu

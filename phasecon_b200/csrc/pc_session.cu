@@ -34,6 +34,49 @@ double freq(int i, int n, double delta) { return i >= n / 2 ? -(double)(n - i) /
 
 }  // namespace
 
+int pc_transform_dims(PcDims &d, int V, int R, int C, size_t *smem_rows, size_t *smem_cols)
+{
+    d.V = V;
+    d.R = R;
+    d.C = C;
+    d.N = R * C;
+    d.logR = ilog2(R);
+    d.logC = ilog2(C);
+    d.nmax = std::max(R, C);
+    d.rows_per_cta = std::max(1, std::min(R, 2048 / C));
+    d.cols_per_cta = std::max(1, std::min(C, 4096 / R));
+    *smem_rows = (size_t)(d.nmax / 2 + 2 * d.rows_per_cta * C) * sizeof(float2);
+    *smem_cols = (size_t)(d.nmax / 2 + 2 * d.cols_per_cta * R) * sizeof(float2);
+    cudaError_t e = cudaFuncSetAttribute(pc_rows_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem_rows);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(pc_rows_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem_rows);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(pc_cols_filter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem_cols);
+    return e == cudaSuccess ? 0 : fail("cudaFuncSetAttribute failed: %s", cudaGetErrorString(e));
+}
+
+std::vector<float2> pc_twiddles(int nmax)
+{
+    std::vector<float2> tw(nmax / 2);
+    for (int m = 0; m < nmax / 2; m++) {
+        const double a = -2.0 * kPi * m / nmax;
+        tw[m] = make_float2((float)std::cos(a), (float)std::sin(a));
+    }
+    return tw;
+}
+
+void pc_transform(const PcDims &d, PcArgs A, size_t smem_rows, size_t smem_cols, int prologue, const float2 *in,
+                  const float2 *table, int epilogue, float2 *out, int acc_slot, cudaStream_t st)
+{
+    A.in = in;
+    A.out = out;
+    A.acc_slot = acc_slot;
+    dim3 grows((d.R + d.rows_per_cta - 1) / d.rows_per_cta, d.V), gcols(d.C / d.cols_per_cta, d.V);
+    pc_rows_forward<<<grows, 256, smem_rows, st>>>(d, A, prologue);
+    pc_cols_filter<<<gcols, 256, smem_cols, st>>>(d, A, table);
+    pc_rows_inverse<<<grows, 256, smem_rows, st>>>(d, A, epilogue);
+}
+
 #define PCK(call)                                                                              \
     do {                                                                                       \
         cudaError_t e_ = (call);                                                               \
@@ -106,13 +149,7 @@ struct PcSession {
     void transform(PcArgs A, int prologue, const float2 *in, const float2 *table, int epilogue, float2 *out,
                    int acc_slot)
     {
-        A.in = in;
-        A.out = out;
-        A.acc_slot = acc_slot;
-        dim3 grows((d.R + d.rows_per_cta - 1) / d.rows_per_cta, d.V), gcols(d.C / d.cols_per_cta, d.V);
-        pc_rows_forward<<<grows, 256, smem_rows, st>>>(d, A, prologue);
-        pc_cols_filter<<<gcols, 256, smem_cols, st>>>(d, A, table);
-        pc_rows_inverse<<<grows, 256, smem_rows, st>>>(d, A, epilogue);
+        pc_transform(d, A, smem_rows, smem_cols, prologue, in, table, epilogue, out, acc_slot, st);
     }
 
     dim3 pointwise_grid() const { return dim3(std::max(1, std::min(64, d.N / 1024)), d.V); }
@@ -146,23 +183,10 @@ int PcSession::init(const mbirgpu_pc_problem *pb, const mbirgpu_pc_options *o, v
         return fail("phase retrieval needs power-of-two detector sizes up to 1024 (got %d x %d)", C, R);
     if (V < 1) return fail("proj_num must be positive");
     if (opt.nms_order != 0 && opt.nms_order != 1) return fail("nms_order must be 0 (raster) or 1 (colour classes)");
-    d.V = V;
-    d.R = R;
-    d.C = C;
-    d.N = R * C;
-    d.logR = ilog2(R);
-    d.logC = ilog2(C);
-    d.nmax = std::max(R, C);
-    d.rows_per_cta = std::max(1, std::min(R, 2048 / C));
-    d.cols_per_cta = std::max(1, std::min(C, 4096 / R));
+    if (pc_transform_dims(d, V, R, C, &smem_rows, &smem_cols)) return -1;
     d.nu = (float)opt.nu;
     dob = pb->pag_regparam;
     d.delta_over_beta = (float)dob;
-    smem_rows = (size_t)(d.nmax / 2 + 2 * d.rows_per_cta * C) * sizeof(float2);
-    smem_cols = (size_t)(d.nmax / 2 + 2 * d.cols_per_cta * R) * sizeof(float2);
-    PCK(cudaFuncSetAttribute(pc_rows_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_rows));
-    PCK(cudaFuncSetAttribute(pc_rows_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_rows));
-    PCK(cudaFuncSetAttribute(pc_cols_filter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cols));
 
     // physics constants (XT_Init.c:256-260, 530)
     wavelength = kPlanck * kLightSpeed / (double)pb->light_energy;
@@ -181,11 +205,8 @@ int PcSession::init(const mbirgpu_pc_problem *pb, const mbirgpu_pc_options *o, v
         return -1;
 
     // twiddles and transfer tables in double, rounded once to float
-    std::vector<float2> tw(d.nmax / 2), Hf(d.N), Hh(d.N), Hp(d.N);
-    for (int m = 0; m < d.nmax / 2; m++) {
-        const double a = -2.0 * kPi * m / d.nmax;
-        tw[m] = make_float2((float)std::cos(a), (float)std::sin(a));
-    }
+    const std::vector<float2> tw = pc_twiddles(d.nmax);
+    std::vector<float2> Hf(d.N), Hh(d.N), Hp(d.N);
     const double kover2R = kPi / (distance * wavelength);
     const double reg = dob / (2 * wavenumber);
     for (int i = 0; i < R; i++)

@@ -307,6 +307,7 @@ int Session::icd_iteration(int iter, mbirgpu_iter_stats *out)
     L.colors_k = colors;
     L.perm = spread_multiplier(sv_slots(g.N_x, g.N_y, sv, colors));
     L.max_ctas = sv_max_concurrent(g.N_x, g.N_y, g.N_time, sv, colors);
+    L.stage_records = opt.stage_records;
     const int phases = colors * colors;
     Geom gb = g;
     gb.N_p = n_assigned;
@@ -557,6 +558,7 @@ void mbirgpu_default_options(mbirgpu_options *o)
     o->seed = 761521;  // the reference's srandom2 seed, XT_Engine.c:99
     o->nhicd_passes = mbirgpu::kNhicdIterations;  // the reference runs NH-ICD by default (NO_NHICD 0)
     o->sv_colors = 0;
+    o->stage_records = 1;
 }
 
 int mbirgpu_set_options(const mbirgpu_options *o)

@@ -37,6 +37,8 @@ EXPORTS = (
     "phcontomo_reconstruct", "mbirgpu_pc_default_options", "mbirgpu_pc_session_create", "mbirgpu_pc_session_destroy",
     "mbirgpu_pc_fresnel", "mbirgpu_pc_paganin", "mbirgpu_pc_set_z", "mbirgpu_pc_init_admm", "mbirgpu_pc_set_state",
     "mbirgpu_pc_get_state", "mbirgpu_pc_sd_step", "mbirgpu_pc_nms_sweep", "mbirgpu_pc_run",
+    "phcontomo_forward_project", "mbirgpu_pc_sim_default_options", "mbirgpu_pc_sim_set_options",
+    "mbirgpu_pc_sim_get_options", "mbirgpu_pc_simulate",
 )
 
 
@@ -50,7 +52,7 @@ class Options(C.Structure):
         ("num_stages", C.c_int32), ("cost_rel_tol", C.c_double), ("zero_skipping", C.c_int32),
         ("write_files", C.c_int32), ("compute_cost", C.c_int32), ("refresh_every", C.c_int32),
         ("sv_size", C.c_int32), ("cta_warps", C.c_int32), ("icd_unroll", C.c_int32), ("seed", C.c_uint64),
-        ("nhicd_passes", C.c_int32), ("sv_colors", C.c_int32),
+        ("nhicd_passes", C.c_int32), ("sv_colors", C.c_int32), ("stage_records", C.c_int32),
     ]
 
 

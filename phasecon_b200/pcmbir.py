@@ -45,6 +45,14 @@ class PcStats(C.Structure):
     _fields_ = [("sd_steps", C.c_int64), ("fresnel_transforms", C.c_int64), ("kernel_ms", C.c_double)]
 
 
+class SimOptions(C.Structure):
+    """mbirgpu_pc_sim_options: the simulator's constants of PCMBIR_3D/XT_Constants.h."""
+    _fields_ = [
+        ("mag_phantom_path", C.c_char * 1024), ("phase_phantom_path", C.c_char * 1024), ("phantom_xy", C.c_int32),
+        ("phantom_z", C.c_int32), ("expected_count", C.c_float), ("write_files", C.c_int32),
+    ]
+
+
 _bound = False
 
 
@@ -69,6 +77,14 @@ def lib() -> C.CDLL:
         L.mbirgpu_pc_sd_step.argtypes = [vp, vp, vp]
         L.mbirgpu_pc_nms_sweep.argtypes = [vp]
         L.mbirgpu_pc_run.argtypes = [vp, vp, vp, C.POINTER(PcStats)]
+        L.phcontomo_forward_project.argtypes = [C.POINTER(fp), C.POINTER(fp), vp, C.c_int32, C.c_int32, C.c_int32] + \
+            [C.c_float] * 5 + [vp]
+        L.mbirgpu_pc_sim_default_options.argtypes = [C.POINTER(SimOptions)]
+        L.mbirgpu_pc_sim_default_options.restype = None
+        L.mbirgpu_pc_sim_set_options.argtypes = [C.POINTER(SimOptions)]
+        L.mbirgpu_pc_sim_get_options.argtypes = [C.POINTER(SimOptions)]
+        L.mbirgpu_pc_simulate.argtypes = [vp, vp, C.POINTER(SimOptions), vp, vp, vp, C.c_int32, C.c_int32, C.c_int32] + \
+            [C.c_float] * 4 + [vp, vp, C.POINTER(C.c_double)]
         _bound = True
     return L
 
@@ -218,6 +234,75 @@ def phcontomo_reconstruct(measurements, brights, proj_angles, proj_times, recon_
                                          mag_c_s, mag_c_t, phase_sig_s, phase_sig_t, phase_c_s, phase_c_t,
                                          convg_thresh, obj2det_dist, light_energy, pag_regparam, restart,
                                          recon_type, None)
+    finally:
+        os.chdir(cwd)
+    _check(rc)
+
+
+def sim_options(**kw) -> SimOptions:
+    """The current simulator settings, with fields overridden by keyword."""
+    o = SimOptions()
+    _check(lib().mbirgpu_pc_sim_get_options(C.byref(o)))
+    for k, v in kw.items():
+        if not hasattr(o, k):
+            raise MbirError(f"unknown simulator option {k}")
+        setattr(o, k, v.encode() if isinstance(v, str) else v)
+    return o
+
+
+def set_sim_options(o: SimOptions) -> None:
+    _check(lib().mbirgpu_pc_sim_set_options(C.byref(o)))
+
+
+def simulate(mag, phase, proj_angles, proj_rows: int, proj_cols: int, vox_wid: float, rot_center: float,
+             obj2det_dist: float, light_energy: float, options: SimOptions | None = None,
+             projections: bool = False):
+    """mbirgpu_pc_simulate on phantoms [P_z][P_xy][P_xy]: returns (measurements
+    [proj_num][proj_rows][proj_cols], brights, average) and, with projections,
+    also the FP64 projections (SimMagProjs, SimPhaseProjs) [proj_num][P_z][P_xy]."""
+    mag = np.ascontiguousarray(mag, np.float32)
+    phase = np.ascontiguousarray(phase, np.float32)
+    ang = np.ascontiguousarray(proj_angles, np.float32)
+    o = options if options is not None else sim_options(write_files=0)
+    if mag.shape != (o.phantom_z, o.phantom_xy, o.phantom_xy) or phase.shape != mag.shape:
+        raise MbirError(f"phantoms must be [{o.phantom_z}][{o.phantom_xy}][{o.phantom_xy}]")
+    V = ang.size
+    meas = np.zeros((V, proj_rows, proj_cols), np.float32)
+    br = np.zeros((proj_rows, proj_cols), np.float32)
+    pm = np.zeros((V, o.phantom_z, o.phantom_xy)) if projections else None
+    pp = np.zeros_like(pm) if projections else None
+    avg = C.c_double()
+    _check(lib().mbirgpu_pc_simulate(mag.ctypes.data, phase.ctypes.data, C.byref(o), meas.ctypes.data,
+                                     br.ctypes.data, ang.ctypes.data, proj_rows, proj_cols, V, vox_wid, rot_center,
+                                     obj2det_dist, light_energy, pm.ctypes.data if projections else None,
+                                     pp.ctypes.data if projections else None, C.byref(avg)))
+    if projections:
+        return meas, br, avg.value, pm, pp
+    return meas, br, avg.value
+
+
+def phcontomo_forward_project(measurements: np.ndarray, brights: np.ndarray, proj_angles, proj_rows: int,
+                              proj_cols: int, proj_num: int, vox_wid: float, rot_center: float, obj2det_dist: float,
+                              light_energy: float, pag_regparam: float, workdir: str | None = None) -> None:
+    """The reference's phcontomo_forward_project: fills the caller's float32
+    arrays measurements [proj_num][proj_rows][proj_cols] and brights
+    [proj_rows][proj_cols] from the phantom files named by the simulator
+    settings; output files go to `workdir` (default: the current directory)."""
+    for a in (measurements, brights):
+        if a.dtype != np.float32 or not a.flags.c_contiguous:
+            raise MbirError("measurements and brights must be C-contiguous float32 arrays")
+    if measurements.size != proj_num * proj_rows * proj_cols or brights.size != proj_rows * proj_cols:
+        raise MbirError("measurements / brights sizes do not match the detector")
+    ang = np.ascontiguousarray(proj_angles, np.float32)
+    fp = C.POINTER(C.c_float)
+    pm, pb = measurements.ctypes.data_as(fp), brights.ctypes.data_as(fp)
+    cwd = os.getcwd()
+    if workdir is not None:
+        os.chdir(workdir)
+    try:
+        rc = lib().phcontomo_forward_project(C.byref(pm), C.byref(pb), ang.ctypes.data, proj_rows, proj_cols,
+                                             proj_num, vox_wid, rot_center, obj2det_dist, light_energy,
+                                             pag_regparam, None)
     finally:
         os.chdir(cwd)
     _check(rc)

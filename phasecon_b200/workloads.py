@@ -28,6 +28,8 @@ from .mbir import Problem, Session, get_options
 
 def _measure(pb: Problem, obj: np.ndarray, I0: float, seed: int) -> Problem:
     o = get_options()
+    # a projection-only session: a fixed schedule skips the ICD autotuner
+    o.sv_size, o.cta_warps, o.sv_colors, o.nhicd_passes = 8, 4, 2, 0
     s = Session(pb, options=o)
     ax = s.forward_project(obj)  # [view][col][row]
     s.close()
