@@ -73,6 +73,11 @@ typedef struct {
     int32_t stage_records;   /* 1 (default): the ICD sweep copies each next voxel column's A
                                 records into shared memory while it updates the current one;
                                 0: records are read from global memory where they are used */
+    int32_t nh_sv_size;      /* super-voxel edge of the non-homogeneous passes; 0 = autotuned */
+    int32_t nh_sv_colors;    /* K of their K x K colouring (2 or 4); 0 = autotuned */
+    int32_t nh_cta_warps;    /* warps cooperating on one voxel column in those passes; 0 = autotuned */
+    int32_t nh_work_lists;   /* 1 (default): those passes visit only super-voxels holding selected
+                                columns, the ones with the most first; 0: every super-voxel */
 } mbirgpu_options;
 
 /* Defaults as listed above. */

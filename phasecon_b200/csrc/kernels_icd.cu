@@ -58,14 +58,16 @@ __device__ __forceinline__ uint64_t mix64(uint64_t z)
 // Surrogate weight rho'(d)/d of the qGGMRF potential
 // |d|^q / sq / (c + |d|^(q-p) / sqp) (derivative per XT_ICD_update.c:92-118;
 // value at d = 0 per :119-128): |d|^(q-2) (q - (q-p) t1 / t3) / (t3 sq),
-// t1 = |d|^(q-p) / sqp, t3 = c + t1.
-__device__ __forceinline__ float qg_weight(float d, float q, float qmp, float sq, float sqp, float c, float b0)
+// t1 = |d|^(q-p) / sqp, t3 = c + t1. Takes isq = 1 / sq and isqp = 1 / sqp
+// and divides by t3 through one correctly rounded reciprocal (the weight is
+// evaluated ~28 times per voxel update, so its instruction count matters).
+__device__ __forceinline__ float qg_weight(float d, float q, float qmp, float isq, float isqp, float c, float b0)
 {
     if (d == 0.0f) return b0;
     const float ad = fabsf(d);
-    const float t1 = __expf(qmp * __logf(ad)) / sqp;
-    const float t3 = c + t1;
-    float r = (q - qmp * t1 / t3) / (t3 * sq);
+    const float t1 = __expf(qmp * __logf(ad)) * isqp;
+    const float rt3 = __frcp_rn(c + t1);
+    float r = (q - qmp * t1 * rt3) * rt3 * isq;
     if (q != 2.0f) r *= __expf((q - 2.0f) * __logf(ad));
     return r;
 }
@@ -279,7 +281,7 @@ __device__ __forceinline__ void icd_update_sv(const Geom &g, const IcdLaunch &L,
                             const int zz = lane + dz;
                             if (zz < 0 || zz >= NZ) continue;
                             const float n = nb[dz + 1];
-                            const float b = qg_weight(V - n, K.q, K.qmp, K.ssq, K.ssqp, K.cs, K.bs0);
+                            const float b = qg_weight(V - n, K.q, K.qmp, K.issq, K.issqp, K.cs, K.bs0);
                             const float cf = K.sf[(dz + 1) * 9 + (dy + 1) * 3 + (dx + 1)] * b;
                             num += cf * n;
                             den += cf;
@@ -290,7 +292,7 @@ __device__ __forceinline__ void icd_update_sv(const Geom &g, const IcdLaunch &L,
                     const int ff = f + (s == 8 ? -1 : 1);
                     if (ff >= 0 && ff < g.N_time && zl) {
                         const float n = x[((size_t)ff * nxy + c) * NZ + lane];
-                        const float b = qg_weight(V - n, K.q, K.qmp, K.stq, K.stqp, K.ct, K.bt0);
+                        const float b = qg_weight(V - n, K.q, K.qmp, K.istq, K.istqp, K.ct, K.bt0);
                         const float cf = K.tf * b;
                         num += cf * n;
                         den += cf;
@@ -337,13 +339,14 @@ __device__ __forceinline__ void icd_update_sv(const Geom &g, const IcdLaunch &L,
                     for (int u = 0; u < kUnroll; u++) {
                         const uint32_t hdr = R[u].w[0].x;
                         const int cnt_q = hdr >> 24;
-                        const size_t sb = (size_t)(hdr & 0xFFFFFF) * NT + t0;
+                        // sinogram rows stay below 2^24 and N_t <= 32: 32-bit offsets
+                        const unsigned sb = (hdr & 0xFFFFFFu) * (unsigned)NT + (unsigned)t0;
 #pragma unroll
                         for (int q = 0; q < 4 * KW - 1; q++) {
                             if (q < cnt_q) {
                                 float ev[VEC], wv[VEC];
-                                VecF<VEC>::get(__ldcg(reinterpret_cast<const VT *>(err + sb + (size_t)q * NT)), ev);
-                                VecF<VEC>::get(__ldg(reinterpret_cast<const VT *>(wgt + sb + (size_t)q * NT)), wv);
+                                VecF<VEC>::get(__ldcg(reinterpret_cast<const VT *>(err + (sb + (unsigned)(q * NT)))), ev);
+                                VecF<VEC>::get(__ldg(reinterpret_cast<const VT *>(wgt + (sb + (unsigned)(q * NT)))), wv);
                                 const float a = rec_val<KW>(R[u], q) * K.dt;
 #pragma unroll
                                 for (int i = 0; i < VEC; i++) {
@@ -418,12 +421,12 @@ __device__ __forceinline__ void icd_update_sv(const Geom &g, const IcdLaunch &L,
                 if (!skip && (lane & 1) == parity) {
                     float num = numA, den = denA;
                     if (lane >= 1) {
-                        const float cf = K.sf[0 * 9 + 4] * qg_weight(V0 - vm, K.q, K.qmp, K.ssq, K.ssqp, K.cs, K.bs0);
+                        const float cf = K.sf[0 * 9 + 4] * qg_weight(V0 - vm, K.q, K.qmp, K.issq, K.issqp, K.cs, K.bs0);
                         num += cf * vm;
                         den += cf;
                     }
                     if (lane + 1 < NZ) {
-                        const float cf = K.sf[2 * 9 + 4] * qg_weight(V0 - vp, K.q, K.qmp, K.ssq, K.ssqp, K.cs, K.bs0);
+                        const float cf = K.sf[2 * 9 + 4] * qg_weight(V0 - vp, K.q, K.qmp, K.issq, K.issqp, K.cs, K.bs0);
                         num += cf * vp;
                         den += cf;
                     }
@@ -473,7 +476,8 @@ __device__ __forceinline__ void icd_update_sv(const Geom &g, const IcdLaunch &L,
                     for (int u = 0; u < kUnroll; u++) {
                         const uint32_t hdr = R[u].w[0].x;
                         const int cnt_q = hdr >> 24;
-                        const size_t sb = (size_t)(hdr & 0xFFFFFF) * NT + t0;
+                        // sinogram rows stay below 2^24 and N_t <= 32: 32-bit offsets
+                        const unsigned sb = (hdr & 0xFFFFFFu) * (unsigned)NT + (unsigned)t0;
 #pragma unroll
                         for (int q = 0; q < 4 * KW - 1; q++) {
                             if (q < cnt_q) {
@@ -481,7 +485,7 @@ __device__ __forceinline__ void icd_update_sv(const Geom &g, const IcdLaunch &L,
                                 float d[VEC];
 #pragma unroll
                                 for (int i = 0; i < VEC; i++) d[i] = a * dxv[i];
-                                red_add(err + sb + (size_t)q * NT, d);
+                                red_add(err + (sb + (unsigned)(q * NT)), d);
                             }
                         }
                     }
@@ -506,7 +510,7 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 4) icd_phase_kernel(
     extern __shared__ __align__(16) uint32_t s_rec[];
     const int KC = L.colors_k;
     const int hx = (L.n_sv_x + KC - 1) / KC, slots = hx * ((L.n_sv_y + KC - 1) / KC);
-    const int n_items = g.N_time * slots;
+    const int n_items = L.items ? *L.n_items : g.N_time * slots;
     IcdCount cnt{};
     for (;;) {
         __syncthreads();  // S.item / S.order of the previous SV are no longer read
@@ -514,11 +518,19 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 4) icd_phase_kernel(
         __syncthreads();
         const int item = S.item;
         if (item >= n_items) break;
-        const int f = item % g.N_time;  // frames fastest: concurrent SVs spread over the frames
-        const int rem = (int)((long long)(item / g.N_time) * L.perm % slots);
-        const int color = (L.phase + f) % (KC * KC);  // frame f +- 1 is never on the same colour
-        const int sx = KC * (rem % hx) + color % KC;
-        const int sy = KC * (rem / hx) + color / KC;
+        int f, sx, sy;
+        if (L.items) {  // explicit work list (its SVs hold columns to update)
+            const uint32_t code = L.items[item];
+            f = (int)(code >> 22);
+            sy = (int)((code >> 11) & 2047u);
+            sx = (int)(code & 2047u);
+        } else {
+            f = item % g.N_time;  // frames fastest: concurrent SVs spread over the frames
+            const int rem = (int)((long long)(item / g.N_time) * L.perm % slots);
+            const int color = (L.phase + f) % (KC * KC);  // frame f +- 1 is never on the same colour
+            sx = KC * (rem % hx) + color % KC;
+            sy = KC * (rem / hx) + color / KC;
+        }
         if (sx >= L.n_sv_x || sy >= L.n_sv_y) continue;  // uniform
         icd_update_sv<KW, kUnroll, VEC, kStaged>(g, L, K, table, view_first, mask, x, err, wgt, mag, f, sx, sy, S,
                                                  cnt, s_rec, stage_words);
@@ -575,6 +587,10 @@ IcdConst make_icd_const(const Geom &g)
     K.ssqp = (float)g.sigma_s_q_p;
     K.stq = (float)g.sigma_t_q;
     K.stqp = (float)g.sigma_t_q_p;
+    K.issq = (float)(1.0 / g.sigma_s_q);
+    K.issqp = (float)(1.0 / g.sigma_s_q_p);
+    K.istq = (float)(1.0 / g.sigma_t_q);
+    K.istqp = (float)(1.0 / g.sigma_t_q_p);
     K.cs = (float)g.c_s;
     K.ct = (float)g.c_t;
     K.bs0 = (float)(g.q / (g.sigma_s_q * g.c_s));

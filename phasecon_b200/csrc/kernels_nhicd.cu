@@ -101,7 +101,109 @@ __global__ void __launch_bounds__(1024) nh_select_kernel(int nxy, int k, const f
         out[i] = (uint8_t)(mask[i] && (!found || key[i] > prefix));
 }
 
+// number of selected columns of every (frame, SV); histogram per (phase, count)
+__global__ void nh_count_kernel(int n_frames, int NY, int NX, int sv, int K, const uint8_t *__restrict__ sel,
+                                int *__restrict__ svcount, int *__restrict__ hist)
+{
+    const int nsx = (NX + sv - 1) / sv, nsy = (NY + sv - 1) / sv, maxc = sv * sv;
+    const long long n = (long long)n_frames * nsx * nsy;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int f = (int)(i / ((long long)nsx * nsy));
+        const int r = (int)(i - (long long)f * nsx * nsy), sy = r / nsx, sx = r - sy * nsx;
+        const uint8_t *s = sel + (size_t)f * NX * NY;
+        int cnt = 0;
+        for (int a = 0; a < sv; a++) {
+            const int j = sy * sv + a;
+            if (j >= NY) break;
+            for (int b = 0; b < sv; b++) {
+                const int k = sx * sv + b;
+                if (k < NX) cnt += s[j * NX + k] != 0;
+            }
+        }
+        svcount[i] = cnt;
+        if (cnt) {
+            const int color = (sy % K) * K + sx % K;
+            const int phase = ((color - f) % (K * K) + K * K) % (K * K);
+            atomicAdd(&hist[phase * (maxc + 1) + cnt], 1);
+        }
+    }
+}
+
+// per phase: bucket offsets, counts descending; the phase's total
+__global__ void nh_offsets_kernel(int phases, int maxc, const int *__restrict__ hist, int *__restrict__ off,
+                                  int *__restrict__ n_items)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= phases) return;
+    int o = 0;
+    for (int c = maxc; c >= 1; c--) {
+        off[p * (maxc + 1) + c] = o;
+        o += hist[p * (maxc + 1) + c];
+    }
+    n_items[p] = o;
+}
+
+// walk each phase's SVs in the sweep's own queue order (frames fastest, spread
+// slots) and append the non-empty ones to their count's bucket
+__global__ void nh_scatter_kernel(int n_frames, int NY, int NX, int sv, int K, int perm, int per_phase,
+                                  const int *__restrict__ svcount, const int *__restrict__ off,
+                                  int *__restrict__ cursor, uint32_t *__restrict__ items)
+{
+    const int nsx = (NX + sv - 1) / sv, nsy = (NY + sv - 1) / sv, maxc = sv * sv, KK = K * K;
+    const int hx = (nsx + K - 1) / K, slots = hx * ((nsy + K - 1) / K);
+    const long long n = (long long)KK * n_frames * slots;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int p = (int)(i / ((long long)n_frames * slots));
+        const int q = (int)(i - (long long)p * n_frames * slots);
+        const int f = q % n_frames;
+        const int rem = (int)((long long)(q / n_frames) * perm % slots);
+        const int color = (p + f) % KK;
+        const int sx = K * (rem % hx) + color % K, sy = K * (rem / hx) + color / K;
+        if (sx >= nsx || sy >= nsy) continue;
+        const int cnt = svcount[((size_t)f * nsy + sy) * nsx + sx];
+        if (!cnt) continue;
+        const int pos = atomicAdd(&cursor[p * (maxc + 1) + cnt], 1);
+        items[(size_t)p * per_phase + off[p * (maxc + 1) + cnt] + pos] =
+            ((uint32_t)f << 22) | ((uint32_t)sy << 11) | (uint32_t)sx;
+    }
+}
+
 }  // namespace
+
+int nh_items_per_phase(int n_frames, int N_y, int N_x, int sv, int K)
+{
+    return n_frames * sv_slots(N_x, N_y, sv, K);
+}
+
+size_t nh_items_scratch_ints(int n_frames, int N_y, int N_x, int sv, int K)
+{
+    const size_t nsv = (size_t)((N_x + sv - 1) / sv) * ((N_y + sv - 1) / sv);
+    return (size_t)n_frames * nsv + 3 * (size_t)K * K * (sv * sv + 1);
+}
+
+bool nh_items_supported(int n_frames, int N_y, int N_x, int sv)
+{
+    return n_frames <= 1024 && (N_x + sv - 1) / sv <= 2048 && (N_y + sv - 1) / sv <= 2048;
+}
+
+void launch_nh_items(int n_frames, int N_y, int N_x, int sv, int K, const uint8_t *d_sel, uint32_t *d_items,
+                     int *d_n_items, int *d_scratch, cudaStream_t st)
+{
+    const int nsx = (N_x + sv - 1) / sv, nsy = (N_y + sv - 1) / sv, maxc = sv * sv, KK = K * K;
+    const size_t nsv = (size_t)n_frames * nsx * nsy, hsz = (size_t)KK * (maxc + 1);
+    int *svcount = d_scratch, *hist = d_scratch + nsv, *off = hist + hsz, *cursor = off + hsz;
+    cudaMemsetAsync(hist, 0, hsz * sizeof(int), st);
+    cudaMemsetAsync(cursor, 0, hsz * sizeof(int), st);
+    const int blocks = (int)std::min<size_t>((nsv + 255) / 256, 148 * 8);
+    nh_count_kernel<<<blocks, 256, 0, st>>>(n_frames, N_y, N_x, sv, K, d_sel, svcount, hist);
+    nh_offsets_kernel<<<1, 32, 0, st>>>(KK, maxc, hist, off, d_n_items);
+    const int per_phase = nh_items_per_phase(n_frames, N_y, N_x, sv, K);
+    const long long n = (long long)KK * per_phase;
+    const int sblocks = (int)std::min<long long>((n + 255) / 256, 148LL * 8);
+    nh_scatter_kernel<<<sblocks, 256, 0, st>>>(n_frames, N_y, N_x, sv, K,
+                                               spread_multiplier(sv_slots(N_x, N_y, sv, K)), per_phase, svcount, off,
+                                               cursor, d_items);
+}
 
 void launch_nh_select(int n_frames, int N_y, int N_x, const float *d_mag, const uint8_t *d_mask, int k,
                       float *d_filt, uint8_t *d_sel, cudaStream_t st)

@@ -113,6 +113,11 @@ struct IcdLaunch {
     int colors_k;         // K x K colour classes; phase p updates colour (p + frame) mod K^2
     long long max_ctas;   // cap on the persistent grid (sv_max_concurrent); 0 = none
     int stage_records;    // prefetch each next column's A records into shared memory (cp.async)
+    // optional explicit work list of the phase (non-homogeneous passes): items[i]
+    // = frame << 22 | sv_y << 11 | sv_x, *n_items of them (device memory);
+    // null = every SV slot of the phase's colour in every frame
+    const uint32_t *items;
+    const int *n_items;
 };
 
 // SV slots of one colour per frame and the items (all frames) of one phase.
@@ -150,6 +155,7 @@ struct IcdConst {
     float sf[27];
     float tf;
     float q, qmp, ssq, ssqp, stq, stqp, cs, ct, bs0, bt0, alpha, dt;
+    float issq, issqp, istq, istqp;  // reciprocals of ssq, ssqp, stq, stqp
     float huber_T, huber_delta;
     int huber;
 };
@@ -220,5 +226,16 @@ constexpr int kMaxNhPasses = 16;
 constexpr int kNhicdIterations = 10;  // NHICD_Iterations, XT_Init.c:406
 void launch_nh_select(int n_frames, int N_y, int N_x, const float *d_mag, const uint8_t *d_mask, int k,
                       float *d_filt, uint8_t *d_sel, cudaStream_t st);
+// Work lists of the non-homogeneous passes: for each of the K x K phases of
+// the (sv, K) tiling (phase p of frame f updates colour (p + f) mod K^2), the
+// super-voxels holding selected columns, ordered by their number of selected
+// columns, most first (the longest chains of sequential column updates start
+// first), and in the phases' spread queue order within equal counts. Buffers:
+// items [K^2][items_per_phase], n_items [K^2], scratch of nh_items_scratch_ints().
+int nh_items_per_phase(int n_frames, int N_y, int N_x, int sv, int K);
+size_t nh_items_scratch_ints(int n_frames, int N_y, int N_x, int sv, int K);
+bool nh_items_supported(int n_frames, int N_y, int N_x, int sv);
+void launch_nh_items(int n_frames, int N_y, int N_x, int sv, int K, const uint8_t *d_sel, uint32_t *d_items,
+                     int *d_n_items, int *d_scratch, cudaStream_t st);
 
 }  // namespace mbirgpu

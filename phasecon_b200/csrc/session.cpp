@@ -64,7 +64,8 @@ static int dalloc(T **p, size_t n, size_t *acc)
 Session::~Session()
 {
     void *ptrs[] = {d_y, d_w, d_err, d_x, d_tmp, d_table, d_Hr, d_cos, d_sin, d_views, d_view_first, d_view_frame,
-                    d_mask, d_mag, d_stats, d_cost_partials, d_cost_out, d_flag, d_acc, d_queue, d_filt, d_sel};
+                    d_mask, d_mag, d_stats, d_cost_partials, d_cost_out, d_flag, d_acc, d_queue, d_filt, d_sel,
+                    d_nh_items, d_nh_n, d_nh_scratch};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     for (auto &ev : ev_pairs) {
@@ -120,6 +121,17 @@ int Session::init(const mbirgpu_problem *pb, const mbirgpu_options *o, int mult_
     if (opt.nhicd_passes > 0 &&
         (dalloc(&d_filt, (size_t)g.N_time * nxy, &acc) || dalloc(&d_sel, (size_t)g.N_time * nxy, &acc)))
         return -1;
+    if (opt.nhicd_passes > 0) {
+        // work lists for any NH schedule: the smallest super-voxels need the most
+        for (int K : {2, 4}) {
+            nh_items_cap = std::max(nh_items_cap, (size_t)K * K * nh_items_per_phase(g.N_time, g.N_y, g.N_x, 1, K));
+            for (int sv = 1; sv <= 16; sv *= 2)
+                nh_scratch_cap = std::max(nh_scratch_cap, nh_items_scratch_ints(g.N_time, g.N_y, g.N_x, sv, K));
+        }
+        if (dalloc(&d_nh_items, nh_items_cap, &acc) || dalloc(&d_nh_n, (size_t)kMaxPhases, &acc) ||
+            dalloc(&d_nh_scratch, nh_scratch_cap, &acc))
+            return -1;
+    }
 
     // views not assigned to any frame keep no A records; frame map for the builder
     std::vector<int32_t> view_frame(g.N_p, 0);
@@ -192,6 +204,20 @@ void Session::choose_schedule()
     sv = opt.sv_size > 0 ? std::min(opt.sv_size, 16) : 8;
     colors = opt.sv_colors > 0 ? opt.sv_colors : 2;
     warps = opt.cta_warps > 0 ? std::min(opt.cta_warps, 8) : std::max(2, std::min(8, g.max_views / (16 * (32 / ntp))));
+    sync_nh_schedule();
+}
+
+// Schedule of the non-homogeneous passes: the user's, else the full sweep's
+// super-voxels and colours with twice its warps per column (up to 8). Those
+// passes are bound by chains of column updates inside the few super-voxels
+// that hold many selected columns, so a shorter time per column pays more
+// than the occupancy the wider CTAs cost (4-D workload: 18.6 ms per
+// iteration with 8 warps against 20.6 ms with 4).
+void Session::sync_nh_schedule()
+{
+    nh_sv = opt.nh_sv_size > 0 ? std::min(opt.nh_sv_size, 16) : sv;
+    nh_colors = opt.nh_sv_colors > 0 ? opt.nh_sv_colors : colors;
+    nh_warps = opt.nh_cta_warps > 0 ? std::min(opt.nh_cta_warps, 8) : std::min(8, 2 * warps);
 }
 
 int Session::autotune()
@@ -219,6 +245,7 @@ int Session::autotune()
             sv = cand[a][0];
             colors = cand[a][1];
             warps = ws[b];
+            sync_nh_schedule();
             // time a full iteration as the run will do it: with non-homogeneous
             // passes that is iteration 2 (they start there), after iteration 1
             mbirgpu_iter_stats st_;
@@ -244,6 +271,7 @@ int Session::autotune()
     sv = best_sv;
     warps = best_w;
     colors = best_k;
+    sync_nh_schedule();
     CK(cudaMemsetAsync(d_mag, 0, (size_t)g.N_time * g.N_x * g.N_y * sizeof(float), st));
     CK(cudaStreamSynchronize(st));
     return 0;
@@ -337,12 +365,27 @@ int Session::icd_iteration(int iter, mbirgpu_iter_stats *out)
         IcdLaunch Ln = L;
         Ln.sel = d_sel;
         Ln.seed = L.seed ^ (0x9E3779B97F4A7C15ull * (uint64_t)(pass + 1));
-        for (int ph = 0; ph < phases; ph++) {
+        Ln.sv = nh_sv;
+        Ln.n_sv_x = (g.N_x + nh_sv - 1) / nh_sv;
+        Ln.n_sv_y = (g.N_y + nh_sv - 1) / nh_sv;
+        Ln.colors_k = nh_colors;
+        Ln.warps = nh_warps;
+        Ln.perm = spread_multiplier(sv_slots(g.N_x, g.N_y, nh_sv, nh_colors));
+        Ln.max_ctas = sv_max_concurrent(g.N_x, g.N_y, g.N_time, nh_sv, nh_colors);
+        const int nh_phases = nh_colors * nh_colors;
+        const int per_phase = nh_items_per_phase(g.N_time, g.N_y, g.N_x, nh_sv, nh_colors);
+        const bool lists = opt.nh_work_lists && nh_items_supported(g.N_time, g.N_y, g.N_x, nh_sv) &&
+                           (size_t)nh_phases * per_phase <= nh_items_cap &&
+                           nh_items_scratch_ints(g.N_time, g.N_y, g.N_x, nh_sv, nh_colors) <= nh_scratch_cap;
+        if (lists) launch_nh_items(g.N_time, g.N_y, g.N_x, nh_sv, nh_colors, d_sel, d_nh_items, d_nh_n, d_nh_scratch, st);
+        for (int ph = 0; ph < nh_phases; ph++) {
             Ln.phase = ph;
+            Ln.items = lists ? d_nh_items + (size_t)ph * per_phase : nullptr;
+            Ln.n_items = lists ? d_nh_n + ph : nullptr;
             launch_icd_phase(gb, Ln, d_table, d_view_first, d_mask, d_x, d_err, d_w, d_mag, d_stats,
                              d_queue + kMaxPhases * (pass + 1) + ph, st);
         }
-        launches += phases + 2;
+        launches += nh_phases + 2 + (lists ? 3 : 0);
     }
     if (nh > 0 && timing) CK(cudaEventRecord(ev_pairs[1].second, st));
     CK(cudaGetLastError());
@@ -559,6 +602,10 @@ void mbirgpu_default_options(mbirgpu_options *o)
     o->nhicd_passes = mbirgpu::kNhicdIterations;  // the reference runs NH-ICD by default (NO_NHICD 0)
     o->sv_colors = 0;
     o->stage_records = 1;
+    o->nh_sv_size = 0;
+    o->nh_sv_colors = 0;
+    o->nh_cta_warps = 0;
+    o->nh_work_lists = 1;
 }
 
 int mbirgpu_set_options(const mbirgpu_options *o)
@@ -572,6 +619,10 @@ int mbirgpu_set_options(const mbirgpu_options *o)
     if (o->nhicd_passes < 0 || o->nhicd_passes > mbirgpu::kMaxNhPasses)
         return fail("nhicd_passes must be 0 (off) .. %d", mbirgpu::kMaxNhPasses);
     if (o->sv_colors != 0 && o->sv_colors != 2 && o->sv_colors != 4) return fail("sv_colors must be 0 (auto), 2 or 4");
+    if (o->nh_sv_size < 0 || o->nh_sv_size > 16) return fail("nh_sv_size must be 0 (auto) or 1..16");
+    if (o->nh_sv_colors != 0 && o->nh_sv_colors != 2 && o->nh_sv_colors != 4)
+        return fail("nh_sv_colors must be 0 (auto), 2 or 4");
+    if (o->nh_cta_warps < 0 || o->nh_cta_warps > 8) return fail("nh_cta_warps must be 0 (auto) or 1..8");
     mbirgpu_options cur = mbirgpu::current_options();
     (void)cur;
     std::lock_guard<std::mutex> lk(mbirgpu::g_opt_mu);

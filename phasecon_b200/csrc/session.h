@@ -21,6 +21,7 @@ struct Session {
     int64_t masked_columns = 0;
     int64_t masked_nnz = 0;  // A nonzeros over masked columns, all frames, per voxel slice
     int sv = 8, warps = 4, colors = 2;
+    int nh_sv = 8, nh_colors = 2, nh_warps = 4;  // schedule of the non-homogeneous passes
     bool timing = false;
 
     float *d_y = nullptr, *d_w = nullptr, *d_err = nullptr, *d_x = nullptr, *d_tmp = nullptr;
@@ -39,12 +40,17 @@ struct Session {
     static constexpr int kQueueCounters = kMaxPhases * (1 + kMaxNhPasses);
     float *d_filt = nullptr;          // NH-ICD filtered update magnitudes [N_time][N_y][N_x]
     uint8_t *d_sel = nullptr;         // NH-ICD selected columns [N_time][N_y][N_x]
+    uint32_t *d_nh_items = nullptr;   // NH-ICD work lists (launch_nh_items), per phase
+    int *d_nh_n = nullptr;            // their lengths [kMaxPhases]
+    int *d_nh_scratch = nullptr;
+    size_t nh_items_cap = 0, nh_scratch_cap = 0;  // ints allocated
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pairs;
 
     ~Session();
     int init(const mbirgpu_problem *pb, const mbirgpu_options *o, int mult_xy, int mult_z, void *stream);
     void choose_schedule();
     int autotune();
+    void sync_nh_schedule();
     struct TuneEntry {
         int sv, warps;
         double ms;

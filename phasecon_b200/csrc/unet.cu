@@ -29,6 +29,8 @@
 #include <cstring>
 #include <random>
 #include <string>
+#include <map>
+#include <utility>
 #include <vector>
 
 #include "../../include/mbirgpu.h"
@@ -74,12 +76,14 @@ constexpr int kHalo = HZ * HY * HX;
 
 // out[v][n] = act(sum_{tap, k} in[v + off(tap)][k] wt[tap][n][k] + b[n]) with
 // wt in [27][Nout][Kin] layout (the forward weights transposed per tap, or the
-// data-gradient weights flipped in space); NT output channels per CTA.
+// data-gradient weights flipped in space); NT output channels per CTA. The
+// grid is D slices deep, a stack of frames Df slices each (Df a multiple of
+// FZ, so no tile straddles two frames); zero padding is per frame.
 template <int NT>
 __global__ void __launch_bounds__(kFThreads) conv_tile_kernel(const bf16 *__restrict__ in, int Kin,
                                                         const bf16 *__restrict__ wt, const float *__restrict__ bias,
                                                         bf16 *__restrict__ out, int Nout, int D, int H, int W,
-                                                        int relu)
+                                                        int relu, int Df)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     bf16 *Hs = reinterpret_cast<bf16 *>(smem_raw);  // [kFHalo][kPadK]
@@ -89,6 +93,7 @@ __global__ void __launch_bounds__(kFThreads) conv_tile_kernel(const bf16 *__rest
     const int x0 = (b % tiles_x) * FX;
     b /= tiles_x;
     const int y0 = (b % tiles_y) * FY, z0 = (b / tiles_y) * FZ;
+    const int zf0 = (z0 / Df) * Df, zf1 = min(zf0 + Df, D);  // this tile's frame
     const int n0 = blockIdx.y * NT;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, tig = lane & 3;
     float acc[2][NT / 8][4];
@@ -104,7 +109,7 @@ __global__ void __launch_bounds__(kFThreads) conv_tile_kernel(const bf16 *__rest
             const int hz = hv / (FHY * FHX), r = hv - hz * (FHY * FHX), hy = r / FHX, hx = r - hy * FHX;
             const int z = z0 + hz - 1, y = y0 + hy - 1, x = x0 + hx - 1;
             bf16 *dst = Hs + hv * kPadK;
-            const bool inside = z >= 0 && z < D && y >= 0 && y < H && x >= 0 && x < W;
+            const bool inside = z >= zf0 && z < zf1 && y >= 0 && y < H && x >= 0 && x < W;
             const long long v = ((long long)z * H + y) * W + x;
             if (inside && full) {
                 const uint4 *p = reinterpret_cast<const uint4 *>(in + v * Kin + c0);
@@ -181,7 +186,7 @@ template <int NT>
 __global__ void __launch_bounds__(kFThreads) conv_first_kernel(const bf16 *__restrict__ in,
                                                                const bf16 *__restrict__ wt,
                                                                const float *__restrict__ bias, bf16 *__restrict__ out,
-                                                               int Nout, int D, int H, int W, int relu)
+                                                               int Nout, int D, int H, int W, int relu, int Df)
 {
     __shared__ __align__(16) bf16 As[FZ * FY * FX][kPadK32];
     __shared__ __align__(16) bf16 Bs[NT][kPadK32];
@@ -196,11 +201,12 @@ __global__ void __launch_bounds__(kFThreads) conv_first_kernel(const bf16 *__res
         const int tv = threadIdx.x;  // one output voxel per thread
         const int tz = tv / (FY * FX), r = tv - tz * (FY * FX), ty = r / FX, tx = r - ty * FX;
         const int z = z0 + tz, y = y0 + ty, x = x0 + tx;
+        const int zf0 = (z / Df) * Df, zf1 = min(zf0 + Df, D);  // this voxel's frame
         for (int k = 0; k < 32; k++) {
             float v = 0.0f;
             if (k < 27) {
                 const int zz = z + k / 9 - 1, yy = y + (k / 3) % 3 - 1, xx = x + k % 3 - 1;
-                if (zz >= 0 && zz < D && yy >= 0 && yy < H && xx >= 0 && xx < W)
+                if (zz >= zf0 && zz < zf1 && yy >= 0 && yy < H && xx >= 0 && xx < W)
                     v = __bfloat162float(in[((long long)zz * H + yy) * W + xx]);
             }
             As[tv][k] = __float2bfloat16(v);
@@ -574,9 +580,12 @@ struct UNet {
     float scale = 1.0f;  // input scale: the network sees scale x input
     cudaStream_t st = nullptr;
 
-    // activations and gradients for one grid size
-    int D = 0, H = 0, W = 0;
-    std::vector<void *> bufs;
+    // activations (and, for training, gradients) for one grid size: D slices
+    // = a stack of D / Df frames of Df slices each
+    int D = 0, H = 0, W = 0, Df = 0;
+    bool has_grads = false;
+    std::vector<std::pair<void *, size_t>> bufs;     // activation blocks in use (pointer, bytes)
+    std::multimap<size_t, void *> spare;              // released blocks kept for reuse, by size
     bf16 *x0 = nullptr;
     bf16 *act[4][2] = {};  // encoder level l: conv a, conv b (= skip)
     bf16 *pool[3] = {};    // pooled encoder output of level l (input of level l+1)
@@ -588,18 +597,23 @@ struct UNet {
     ~UNet()
     {
         free_acts();
+        for (auto &b : spare) cudaFree(b.second);
         for (void *p : {(void *)d_p, (void *)d_g, (void *)d_m, (void *)d_v, (void *)d_pb, (void *)d_wt,
                         (void *)d_loss})
             if (p) cudaFree(p);
     }
+    // Activation blocks go back to a size-keyed pool instead of to the driver:
+    // switching between the training grid and the stacked inference grid then
+    // allocates only the first time each block size is needed.
     void free_acts()
     {
-        for (void *p : bufs) cudaFree(p);
+        for (auto &b : bufs) spare.emplace(b.second, b.first);
         bufs.clear();
-        D = H = W = 0;
+        D = H = W = Df = 0;
+        has_grads = false;
     }
     int init(int base, uint64_t seed);
-    int ensure(int d, int h, int w);
+    int ensure(int d, int h, int w, int frames = 1, bool grads = true);
     long long vox(int l) const { return (long long)(D >> l) * (H >> l) * (W >> l); }
     void conv(int i, const bf16 *in, bf16 *o, int l, bool relu);
     void conv_tiles(const bf16 *in, int Kin, const float *bias, bf16 *o, int Nout, int l, bool relu);
@@ -670,46 +684,59 @@ int UNet::init(int base, uint64_t seed)
     return e == cudaSuccess ? 0 : fail("U-Net init failed: %s", cudaGetErrorString(e));
 }
 
-int UNet::ensure(int d, int h, int w)
+int UNet::ensure(int d, int h, int w, int frames, bool grads)
 {
-    if (d == D && h == H && w == W) return 0;
+    if (d * frames == D && d == Df && h == H && w == W && (has_grads || !grads)) return 0;
     if (d % 8 || h % 8 || w % 8 || d < 8 || h < 8 || w < 8)
         return fail("U-Net grid sizes must be multiples of 8 (got %d x %d x %d)", d, h, w);
+    if (frames > 1 && d % 16)
+        return fail("stacked frames need a depth that is a multiple of 16 (got %d)", d);
     free_acts();
-    D = d;
+    D = d * frames;
+    Df = d;
     H = h;
     W = w;
+    has_grads = grads;
     const int C[4] = {c, 2 * c, 4 * c, 8 * c};
     cudaError_t e = cudaSuccess;
-    auto alloc = [&](bf16 **p, long long n) {
+    auto block = [&](void **p, size_t bytes) {
         if (e != cudaSuccess) return;
-        e = cudaMalloc((void **)p, (size_t)n * sizeof(bf16));
-        if (e == cudaSuccess) bufs.push_back(*p);
+        auto it = spare.find(bytes);
+        if (it != spare.end()) {
+            *p = it->second;
+            spare.erase(it);
+        } else {
+            e = cudaMalloc(p, bytes);
+            if (e != cudaSuccess) return;
+        }
+        bufs.emplace_back(*p, bytes);
+    };
+    auto alloc = [&](bf16 **p, long long n) { block((void **)p, (size_t)n * sizeof(bf16)); };
+    auto galloc = [&](bf16 **p, long long n) {  // gradient buffers: training only
+        if (grads) alloc(p, n);
+        else *p = nullptr;
     };
     alloc(&x0, vox(0));
     for (int l = 0; l < 4; l++)
         for (int k = 0; k < 2; k++) {
             alloc(&act[l][k], vox(l) * C[l]);
-            alloc(&gact[l][k], vox(l) * C[l]);
+            galloc(&gact[l][k], vox(l) * C[l]);
         }
     for (int l = 0; l < 3; l++) {
         alloc(&pool[l], vox(l + 1) * C[l]);
-        alloc(&gpool[l], vox(l + 1) * C[l]);
+        galloc(&gpool[l], vox(l + 1) * C[l]);
         alloc(&up[l], vox(l) * C[l + 1]);
-        alloc(&gup[l], vox(l) * C[l + 1]);
+        galloc(&gup[l], vox(l) * C[l + 1]);
         alloc(&u[l], vox(l) * C[l]);
-        alloc(&gu[l], vox(l) * C[l]);
+        galloc(&gu[l], vox(l) * C[l]);
         alloc(&cat[l], vox(l) * 2 * C[l]);
-        alloc(&gcat[l], vox(l) * 2 * C[l]);
+        galloc(&gcat[l], vox(l) * 2 * C[l]);
         for (int k = 0; k < 2; k++) {
             alloc(&dec[l][k], vox(l) * C[l]);
-            alloc(&gdec[l][k], vox(l) * C[l]);
+            galloc(&gdec[l][k], vox(l) * C[l]);
         }
     }
-    if (e == cudaSuccess) {
-        e = cudaMalloc((void **)&out, (size_t)vox(0) * sizeof(float));
-        if (e == cudaSuccess) bufs.push_back(out);
-    }
+    block((void **)&out, (size_t)vox(0) * sizeof(float));
     if (e != cudaSuccess) {
         free_acts();
         return fail("U-Net activation allocation failed: %s", cudaGetErrorString(e));
@@ -720,21 +747,21 @@ int UNet::ensure(int d, int h, int w)
 // out = act(conv(in)) with weights in the tile layout (d_wt); Nout output channels.
 void UNet::conv_tiles(const bf16 *in, int Kin, const float *bias, bf16 *o, int Nout, int l, bool relu)
 {
-    const int d = D >> l, h = H >> l, w = W >> l;
+    const int d = D >> l, h = H >> l, w = W >> l, df = Df >> l;
     const unsigned tiles = (unsigned)(((d + FZ - 1) / FZ) * ((h + FY - 1) / FY) * ((w + FX - 1) / FX));
     const int r = relu ? 1 : 0;
     if (Kin == 1) {
         dim3 grid(tiles, (unsigned)((Nout + 15) / 16));
-        conv_first_kernel<16><<<grid, kFThreads, 0, st>>>(in, d_wt, bias, o, Nout, d, h, w, r);
+        conv_first_kernel<16><<<grid, kFThreads, 0, st>>>(in, d_wt, bias, o, Nout, d, h, w, r, df);
     } else if (Nout > 32) {
         dim3 grid(tiles, (unsigned)((Nout + 63) / 64));
-        conv_tile_kernel<64><<<grid, kFThreads, conv_smem<64>(), st>>>(in, Kin, d_wt, bias, o, Nout, d, h, w, r);
+        conv_tile_kernel<64><<<grid, kFThreads, conv_smem<64>(), st>>>(in, Kin, d_wt, bias, o, Nout, d, h, w, r, df);
     } else if (Nout > 16) {
         conv_tile_kernel<32><<<dim3(tiles, 1), kFThreads, conv_smem<32>(), st>>>(in, Kin, d_wt, bias, o, Nout, d, h,
-                                                                                w, r);
+                                                                                w, r, df);
     } else {
         conv_tile_kernel<16><<<dim3(tiles, 1), kFThreads, conv_smem<16>(), st>>>(in, Kin, d_wt, bias, o, Nout, d, h,
-                                                                                w, r);
+                                                                                w, r, df);
     }
 }
 
@@ -807,6 +834,7 @@ int UNet::forward(const float *d_in)
 // Gradients of mean((out - target)^2) after forward(); the reverse of forward's order.
 int UNet::backward(const float *d_target, double *loss)
 {
+    if (!has_grads || D != Df) return fail("U-Net backward needs a single-frame grid with gradient buffers");
     const int C[4] = {c, 2 * c, 4 * c, 8 * c};
     cudaError_t e = cudaMemsetAsync(d_g, 0, n_params * sizeof(float), st);
     if (e == cudaSuccess) e = cudaMemsetAsync(d_loss, 0, sizeof(double), st);
@@ -860,8 +888,17 @@ int UNet::step(float lr)
 // (FP32, device), in place; completes before returning.
 int unet_apply_frames(UNet *u, float *d_vol, int N_time, int N_z, int N_y, int N_x)
 {
-    if (u->ensure(N_z, N_y, N_x)) return -1;
     const size_t frame = (size_t)N_z * N_y * N_x;
+    if (N_time > 1 && N_z % 16 == 0) {
+        // all frames in one pass: the convolutions see a stack of frames (zero
+        // padding per frame), so the coarse levels get N_time times the tiles
+        if (u->ensure(N_z, N_y, N_x, N_time, false) || u->forward(d_vol)) return -1;
+        cudaError_t e = cudaMemcpyAsync(d_vol, u->out, N_time * frame * sizeof(float), cudaMemcpyDeviceToDevice,
+                                        u->st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(u->st);
+        return e == cudaSuccess ? 0 : fail("U-Net inference failed: %s", cudaGetErrorString(e));
+    }
+    if (u->ensure(N_z, N_y, N_x)) return -1;
     for (int f = 0; f < N_time; f++) {
         if (u->forward(d_vol + f * frame)) return -1;
         cudaError_t e = cudaMemcpyAsync(d_vol + f * frame, u->out, frame * sizeof(float), cudaMemcpyDeviceToDevice,
@@ -949,7 +986,7 @@ int mbirgpu_unet_forward(mbirgpu_unet *up, const float *d_input, float *d_output
 {
     UNETP(up);
     if (!d_input || !d_output) return fail("NULL argument");
-    if (u->ensure(D, H, W) || u->forward(d_input)) return -1;
+    if (u->ensure(D, H, W, 1, false) || u->forward(d_input)) return -1;
     cudaError_t e = cudaMemcpyAsync(d_output, u->out, (size_t)D * H * W * sizeof(float), cudaMemcpyDeviceToDevice,
                                     u->st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(u->st);

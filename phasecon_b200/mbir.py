@@ -53,6 +53,8 @@ class Options(C.Structure):
         ("write_files", C.c_int32), ("compute_cost", C.c_int32), ("refresh_every", C.c_int32),
         ("sv_size", C.c_int32), ("cta_warps", C.c_int32), ("icd_unroll", C.c_int32), ("seed", C.c_uint64),
         ("nhicd_passes", C.c_int32), ("sv_colors", C.c_int32), ("stage_records", C.c_int32),
+        ("nh_sv_size", C.c_int32), ("nh_sv_colors", C.c_int32), ("nh_cta_warps", C.c_int32),
+        ("nh_work_lists", C.c_int32),
     ]
 
 

@@ -116,3 +116,33 @@ def test_trained_warm_start_needs_fewer_iterations():
     print(f"iterations to the plain method's converged cost: zero {it_zero}, FBP {it_fbp}, U-Net {it_net}")
     assert it_zero is not None and it_net is not None and it_net < it_zero, (it_net, it_fbp, it_zero)
     assert c_net[0] < c_zero[0]
+
+
+def test_stacked_frame_inference_equals_per_frame():
+    """The warm start runs the network on all frames of a 4-D problem in one
+    stacked pass (zero padding per frame); every voxel must equal the
+    one-frame-at-a-time network output bit for bit (same tiles, same sums)."""
+    import torch
+    n, nz, frames = 32, 16, 3
+    angles, times, rt = P.uniform_views(60)
+    times = np.linspace(0, frames, angles.size, endpoint=False).astype(np.float32)
+    rt = np.linspace(0, frames, frames + 1).astype(np.float32)
+    z = np.zeros((angles.size, nz, n), np.float32)
+    pb = pc.Problem(z, np.ones_like(z), angles, times, rt, nz, n, angles.size, frames, rot_center=n / 2)
+    obj = np.stack([P.random_ellipsoids(n, nz, s) for s in range(frames)])
+    pb = _measure(pb, obj, 2e4, 0)
+    s = pc.Session(pb)
+    fbp = s.fbp()
+    net = WS.UNet(8, seed=2)
+    params = net.get_params()
+    params[-9:-1] = np.random.default_rng(0).normal(0, 0.3, 8)  # a head with weight: the network matters
+    net.set_params(params)
+    net.input_scale = 40.0
+    WS.warm_start(s, net)
+    got = s.get_object()
+    inside = got != 0
+    assert inside.mean() > 0.4
+    for f in range(frames):
+        exp = net.forward(torch.from_numpy(np.ascontiguousarray(fbp[f])).cuda()).cpu().numpy()
+        np.testing.assert_array_equal(got[f][inside[f]], exp[inside[f]])
+    s.close()
