@@ -7,7 +7,8 @@
 // float like filtMagUpdateMap); the threshold is the (N - k)-th smallest
 // filtered value over all N = N_y N_x columns (RandomizedSelect's order
 // statistic), found here by an exact 4-digit radix select on the float bit
-// patterns (non-negative floats order like their bits); the selected columns
+// patterns (non-negative floats order like their bits) spread over many CTAs
+// per frame; the selected columns
 // are those strictly above it -- the k largest -- that lie inside the mask
 // (the reference also picks unmasked columns near the edge but its update
 // skips them, XT_VoxUpdate.c:168).
@@ -46,59 +47,6 @@ __global__ void vsc_filter_kernel(int n_frames, int NY, int NX, const float *__r
         }
         filt[i] = (float)acc;
     }
-}
-
-// One CTA per frame: T = the (k+1)-th largest key (the (N-k)-th smallest), then
-// sel = mask && key > T.
-__global__ void __launch_bounds__(1024) nh_select_kernel(int nxy, int k, const float *__restrict__ filt,
-                                                         const uint8_t *__restrict__ mask, uint8_t *__restrict__ sel)
-{
-    __shared__ unsigned int hist[256];
-    __shared__ unsigned int s_prefix;
-    __shared__ int s_rank;
-    const int f = blockIdx.x;
-    const unsigned int *key = reinterpret_cast<const unsigned int *>(filt + (size_t)f * nxy);
-    uint8_t *out = sel + (size_t)f * nxy;
-    if (k <= 0) {  // nothing to select: the threshold is the maximum
-        for (int i = threadIdx.x; i < nxy; i += blockDim.x) out[i] = 0;
-        return;
-    }
-    unsigned int prefix = 0, pmask = 0;
-    int rank = k + 1;  // 1-based rank from the top
-    bool found = true;
-    for (int shift = 24; shift >= 0; shift -= 8) {
-        for (int b = threadIdx.x; b < 256; b += blockDim.x) hist[b] = 0;
-        __syncthreads();
-        for (int i = threadIdx.x; i < nxy; i += blockDim.x) {
-            const unsigned int u = key[i];
-            if ((u & pmask) == prefix) atomicAdd(&hist[(u >> shift) & 255u], 1u);
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            int cum = 0, b = 255;
-            for (; b >= 0; b--) {
-                if (cum + (int)hist[b] >= rank) break;
-                cum += (int)hist[b];
-            }
-            if (b < 0) {  // fewer than k + 1 keys: every key is above the threshold
-                s_rank = -1;
-            } else {
-                s_prefix = prefix | ((unsigned int)b << shift);
-                s_rank = rank - cum;
-            }
-        }
-        __syncthreads();
-        if (s_rank < 0) {
-            found = false;
-            break;
-        }
-        prefix = s_prefix;
-        rank = s_rank;
-        pmask |= 0xFFu << shift;
-        __syncthreads();
-    }
-    for (int i = threadIdx.x; i < nxy; i += blockDim.x)
-        out[i] = (uint8_t)(mask[i] && (!found || key[i] > prefix));
 }
 
 // number of selected columns of every (frame, SV); histogram per (phase, count)
@@ -168,6 +116,82 @@ __global__ void nh_scatter_kernel(int n_frames, int NY, int NX, int sv, int K, i
     }
 }
 
+// The order statistic by radix select over the float bit patterns, spread
+// over many CTAs per frame: per 8-bit digit (most significant first) a
+// histogram kernel over all keys that match the prefix so far, then a
+// one-warp-per-frame kernel that picks the digit holding the rank (the
+// (k+1)-th largest key, the threshold); state[f] = {prefix, prefix mask,
+// remaining rank, found}. sel = mask && key > threshold: the k largest.
+struct NhSelState {
+    unsigned int prefix, pmask;
+    int rank, found;
+};
+
+__global__ void nh_sel_init_kernel(int n_frames, int k, NhSelState *__restrict__ state, unsigned int *__restrict__ ghist)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n_frames) state[i] = NhSelState{0u, 0u, k + 1, 1};
+    for (int b = i; b < n_frames * 256; b += gridDim.x * blockDim.x) ghist[b] = 0u;
+}
+
+__global__ void nh_sel_hist_kernel(int nxy, int shift, const float *__restrict__ filt,
+                                   const NhSelState *__restrict__ state, unsigned int *__restrict__ ghist)
+{
+    __shared__ unsigned int hist[256];
+    const int f = blockIdx.y;
+    const NhSelState st = state[f];
+    if (!st.found) return;  // uniform: this frame's selection is settled
+    for (int b = threadIdx.x; b < 256; b += blockDim.x) hist[b] = 0u;
+    __syncthreads();
+    const unsigned int *key = reinterpret_cast<const unsigned int *>(filt + (size_t)f * nxy);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nxy; i += gridDim.x * blockDim.x) {
+        const unsigned int u = key[i];
+        if ((u & st.pmask) == st.prefix) atomicAdd(&hist[(u >> shift) & 255u], 1u);
+    }
+    __syncthreads();
+    for (int b = threadIdx.x; b < 256; b += blockDim.x)
+        if (hist[b]) atomicAdd(&ghist[f * 256 + b], hist[b]);
+}
+
+// one warp per frame: the digit whose cumulative count from the top reaches
+// the rank; clears the histogram for the next digit
+__global__ void nh_sel_pick_kernel(int shift, NhSelState *__restrict__ state, unsigned int *__restrict__ ghist)
+{
+    const int f = blockIdx.x, lane = threadIdx.x;
+    NhSelState st = state[f];
+    unsigned int *h = ghist + f * 256;
+    if (st.found && lane == 0) {
+        int cum = 0, b = 255;
+        for (; b >= 0; b--) {
+            if (cum + (int)h[b] >= st.rank) break;
+            cum += (int)h[b];
+        }
+        if (b < 0) {  // fewer than k + 1 keys: every key is above the threshold
+            st.found = 0;
+        } else {
+            st.prefix |= (unsigned int)b << shift;
+            st.pmask |= 0xFFu << shift;
+            st.rank -= cum;
+        }
+        state[f] = st;
+    }
+    __syncwarp();
+    for (int b = lane; b < 256; b += 32) h[b] = 0u;
+}
+
+__global__ void nh_sel_final_kernel(int n_frames, int nxy, int k, const float *__restrict__ filt,
+                                    const uint8_t *__restrict__ mask, const NhSelState *__restrict__ state,
+                                    uint8_t *__restrict__ sel)
+{
+    const long long n = (long long)n_frames * nxy;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int f = (int)(i / nxy), c = (int)(i - (long long)f * nxy);
+        const unsigned int u = reinterpret_cast<const unsigned int *>(filt)[i];
+        const NhSelState st = state[f];
+        sel[i] = (uint8_t)(k > 0 && mask[c] && (!st.found || u > st.prefix));
+    }
+}
+
 }  // namespace
 
 int nh_items_per_phase(int n_frames, int N_y, int N_x, int sv, int K)
@@ -206,12 +230,27 @@ void launch_nh_items(int n_frames, int N_y, int N_x, int sv, int K, const uint8_
 }
 
 void launch_nh_select(int n_frames, int N_y, int N_x, const float *d_mag, const uint8_t *d_mask, int k,
-                      float *d_filt, uint8_t *d_sel, cudaStream_t st)
+                      float *d_filt, uint8_t *d_sel, cudaStream_t st, void *d_sel_scratch)
 {
-    const long long n = (long long)n_frames * N_y * N_x;
+    const int nxy = N_y * N_x;
+    const long long n = (long long)n_frames * nxy;
     const int blocks = (int)std::min<long long>((n + 255) / 256, 148LL * 16);
     vsc_filter_kernel<<<blocks, 256, 0, st>>>(n_frames, N_y, N_x, d_mag, d_filt);
-    nh_select_kernel<<<n_frames, 1024, 0, st>>>(N_y * N_x, k, d_filt, d_mask, d_sel);
+    NhSelState *state = reinterpret_cast<NhSelState *>(d_sel_scratch);
+    unsigned int *ghist = reinterpret_cast<unsigned int *>(state + n_frames);
+    nh_sel_init_kernel<<<(n_frames * 256 + 255) / 256, 256, 0, st>>>(n_frames, k, state, ghist);
+    // about 4 keys per thread: enough CTAs per frame to spread the reads over the GPU
+    const int per_frame = std::max(1, std::min(64, (nxy + 1023) / 1024));
+    for (int shift = 24; shift >= 0; shift -= 8) {
+        nh_sel_hist_kernel<<<dim3(per_frame, n_frames), 256, 0, st>>>(nxy, shift, d_filt, state, ghist);
+        nh_sel_pick_kernel<<<n_frames, 32, 0, st>>>(shift, state, ghist);
+    }
+    nh_sel_final_kernel<<<blocks, 256, 0, st>>>(n_frames, nxy, k, d_filt, d_mask, state, d_sel);
+}
+
+size_t nh_select_scratch_bytes(int n_frames)
+{
+    return (size_t)n_frames * (sizeof(NhSelState) + 256 * sizeof(unsigned int));
 }
 
 }  // namespace mbirgpu

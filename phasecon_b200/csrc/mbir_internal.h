@@ -224,8 +224,11 @@ void launch_batch_end(BatchDesc *d_descs, int n, cudaStream_t st);
 // value, N = N_x N_y (RandomizedSelect's threshold), i.e. the k largest.
 constexpr int kMaxNhPasses = 16;
 constexpr int kNhicdIterations = 10;  // NHICD_Iterations, XT_Init.c:406
+// d_sel_scratch: nh_select_scratch_bytes(n_frames) bytes of device memory
+// (the radix select's per-frame state and digit histograms).
 void launch_nh_select(int n_frames, int N_y, int N_x, const float *d_mag, const uint8_t *d_mask, int k,
-                      float *d_filt, uint8_t *d_sel, cudaStream_t st);
+                      float *d_filt, uint8_t *d_sel, cudaStream_t st, void *d_sel_scratch);
+size_t nh_select_scratch_bytes(int n_frames);
 // Work lists of the non-homogeneous passes: for each of the K x K phases of
 // the (sv, K) tiling (phase p of frame f updates colour (p + f) mod K^2), the
 // super-voxels holding selected columns, ordered by their number of selected

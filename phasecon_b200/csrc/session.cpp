@@ -65,7 +65,7 @@ Session::~Session()
 {
     void *ptrs[] = {d_y, d_w, d_err, d_x, d_tmp, d_table, d_Hr, d_cos, d_sin, d_views, d_view_first, d_view_frame,
                     d_mask, d_mag, d_stats, d_cost_partials, d_cost_out, d_flag, d_acc, d_queue, d_filt, d_sel,
-                    d_nh_items, d_nh_n, d_nh_scratch};
+                    d_nh_items, d_nh_n, d_nh_scratch, d_nh_selstate};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     for (auto &ev : ev_pairs) {
@@ -129,7 +129,8 @@ int Session::init(const mbirgpu_problem *pb, const mbirgpu_options *o, int mult_
                 nh_scratch_cap = std::max(nh_scratch_cap, nh_items_scratch_ints(g.N_time, g.N_y, g.N_x, sv, K));
         }
         if (dalloc(&d_nh_items, nh_items_cap, &acc) || dalloc(&d_nh_n, (size_t)kMaxPhases, &acc) ||
-            dalloc(&d_nh_scratch, nh_scratch_cap, &acc))
+            dalloc(&d_nh_scratch, nh_scratch_cap, &acc) ||
+            dalloc(&d_nh_selstate, (nh_select_scratch_bytes(g.N_time) + 7) / 8, &acc))
             return -1;
     }
 
@@ -361,7 +362,7 @@ int Session::icd_iteration(int iter, mbirgpu_iter_stats *out)
     if (nh > 0 && timing) CK(cudaEventRecord(ev_pairs[1].first, st));
     for (int pass = 0; pass < nh; pass++) {
         const int k = (int)(masked_columns / std::max(1, g.N_time)) / kNhicdIterations;
-        launch_nh_select(g.N_time, g.N_y, g.N_x, d_mag, d_mask, k, d_filt, d_sel, st);
+        launch_nh_select(g.N_time, g.N_y, g.N_x, d_mag, d_mask, k, d_filt, d_sel, st, d_nh_selstate);
         IcdLaunch Ln = L;
         Ln.sel = d_sel;
         Ln.seed = L.seed ^ (0x9E3779B97F4A7C15ull * (uint64_t)(pass + 1));
@@ -385,7 +386,7 @@ int Session::icd_iteration(int iter, mbirgpu_iter_stats *out)
             launch_icd_phase(gb, Ln, d_table, d_view_first, d_mask, d_x, d_err, d_w, d_mag, d_stats,
                              d_queue + kMaxPhases * (pass + 1) + ph, st);
         }
-        launches += nh_phases + 2 + (lists ? 3 : 0);
+        launches += nh_phases + 11 + (lists ? 3 : 0);  // filter + 10 select launches, 3 list launches
     }
     if (nh > 0 && timing) CK(cudaEventRecord(ev_pairs[1].second, st));
     CK(cudaGetLastError());
@@ -789,13 +790,15 @@ int mbirgpu_session_nh_select(mbirgpu_session *sp, const float *mag, uint8_t *se
     const size_t n = (size_t)g.N_time * g.N_y * g.N_x;
     float *d_m = nullptr, *d_f = nullptr;
     uint8_t *d_s = nullptr;
+    void *d_scr = nullptr;
     cudaError_t e = cudaMalloc((void **)&d_m, n * sizeof(float));
     if (e == cudaSuccess) e = cudaMalloc((void **)&d_f, n * sizeof(float));
     if (e == cudaSuccess) e = cudaMalloc((void **)&d_s, n);
+    if (e == cudaSuccess) e = cudaMalloc(&d_scr, mbirgpu::nh_select_scratch_bytes(g.N_time));
     if (e == cudaSuccess) e = cudaMemcpyAsync(d_m, mag, n * sizeof(float), cudaMemcpyHostToDevice, s->st);
     if (e == cudaSuccess) {
         const int k = (int)(s->masked_columns / std::max(1, g.N_time)) / mbirgpu::kNhicdIterations;
-        mbirgpu::launch_nh_select(g.N_time, g.N_y, g.N_x, d_m, s->d_mask, k, d_f, d_s, s->st);
+        mbirgpu::launch_nh_select(g.N_time, g.N_y, g.N_x, d_m, s->d_mask, k, d_f, d_s, s->st, d_scr);
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cudaMemcpyAsync(sel, d_s, n, cudaMemcpyDeviceToHost, s->st);
@@ -803,6 +806,7 @@ int mbirgpu_session_nh_select(mbirgpu_session *sp, const float *mag, uint8_t *se
     cudaFree(d_m);
     cudaFree(d_f);
     cudaFree(d_s);
+    cudaFree(d_scr);
     if (e != cudaSuccess) return fail("NH-ICD selection failed: %s", cudaGetErrorString(e));
     return 0;
 }

@@ -43,6 +43,7 @@ struct Session {
     uint32_t *d_nh_items = nullptr;   // NH-ICD work lists (launch_nh_items), per phase
     int *d_nh_n = nullptr;            // their lengths [kMaxPhases]
     int *d_nh_scratch = nullptr;
+    uint64_t *d_nh_selstate = nullptr;  // radix-select state (nh_select_scratch_bytes)
     size_t nh_items_cap = 0, nh_scratch_cap = 0;  // ints allocated
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pairs;
 
