@@ -31,8 +31,10 @@ extern "C" {
  * halo slices are zero. Writes the reference's side-effect files in the
  * working directory (object_time_<i>.bin, cost.bin, status.bin,
  * variance_estimate.bin, mag_update.bin, proj_offset.bin) unless disabled by
- * mbirgpu_set_options. remove_rings != 0 is rejected (ring correction is not
- * built). restart = 1 resumes from status.bin like XT_Engine.c:143-150.
+ * mbirgpu_set_options. remove_rings 1-3 estimates the per-detector-pixel
+ * offset as the reference does (none in the coarsest stage, from zero in the
+ * second, carried over after that; see mbirgpu_session_set_ring_correction).
+ * restart = 1 resumes from status.bin like XT_Engine.c:143-150.
  * No MPI is required.
  * ------------------------------------------------------------------------ */
 int reconstruct(float **object, float *projections, float *weights, float *proj_angles, float *proj_times,
@@ -182,6 +184,32 @@ int mbirgpu_session_back_project(mbirgpu_session *s, const float *sino, float *o
 int mbirgpu_session_fbp(mbirgpu_session *s, float *object);
 int mbirgpu_session_set_object_fbp(mbirgpu_session *s);
 
+/* Ring correction (remove_rings of reconstruct, MBIR_4D/XT_Engine.c:73):
+ * the session estimates one offset d per detector pixel, shared by all views,
+ * so that e = y - Ax - d (update_Sinogram_Offset, XT_ICD_update.c:749-923);
+ * mode 1 leaves d free, 2 constrains its mean to zero, 3 is the reference's
+ * rectangular-window mode, whose windows its reconstruct never builds
+ * (gen_offset_constraint_windows runs only in the simulator's set-up), so d
+ * becomes the weighted mean of e + d over the views; 0 turns it off. d is
+ * re-estimated after every full-sweep colour phase and every NH pass.
+ * offset: the starting d, [proj_cols][proj_rows] (the reference's
+ * ProjOffset[N_r][N_t]), or NULL for zero. The error sinogram is recomputed. */
+int mbirgpu_session_set_ring_correction(mbirgpu_session *s, int32_t remove_rings, const float *offset);
+/* Noise-variance re-estimation of the generalised-Huber data term
+ * (update_variance_parameter, MBIR_4D/XT_ICD_update.c:716-747), which
+ * reconstruct runs after its first multires stage when quad_convex = 0: with
+ * on != 0 the variance (starting at 1) is re-estimated at the end of every
+ * ICD iteration and the weights are rescaled by it; the cost then includes
+ * N log(var) / 2 (XT_ICD_update.c:307). update_variance runs one
+ * re-estimation now; get_variance returns the current value. */
+int mbirgpu_session_set_variance_estimation(mbirgpu_session *s, int32_t on);
+int mbirgpu_session_update_variance(mbirgpu_session *s);
+int mbirgpu_session_get_variance(mbirgpu_session *s, double *var_est);
+/* One offset update with the object fixed (the step the ICD iteration runs
+ * after each phase): d and e change together. */
+int mbirgpu_session_update_offset(mbirgpu_session *s);
+/* The current offset d, [proj_cols][proj_rows] (zero without ring correction). */
+int mbirgpu_session_get_offset(mbirgpu_session *s, float *offset);
 /* The NH-ICD voxel-line selection for a given update-magnitude map (for
  * inspection): mag [N_time][N_y][N_x] (sum over z of |update| of each voxel
  * column's latest visit, MagUpdateMap), sel [N_time][N_y][N_x] receives 1

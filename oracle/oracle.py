@@ -163,7 +163,9 @@ def ref_lib() -> C.CDLL:
         lib.ref_random2_sequence.argtypes = [C.c_uint32, C.c_int32, _f64p]
         lib.ref_vsc_select.argtypes = [C.c_int32, C.c_int32, _f32p, C.c_int32, _u8p]
         lib.ref_vsc_select.restype = C.c_int32
-        lib.ref_reconstruct.argtypes = [P, C.c_int32, C.POINTER(C.POINTER(C.c_float))]
+        lib.ref_reconstruct.argtypes = [P, C.c_int32, C.c_int32, C.POINTER(C.POINTER(C.c_float))]
+        lib.ref_offset_update.argtypes = [P, C.c_int32, _f32p, _f32p]
+        lib.ref_variance_update.argtypes = [P, _f32p, _f32p, C.POINTER(C.c_double)]
         lib.ref_reconstruct.restype = C.c_int
         lib.ref_free.argtypes = [C.c_void_p]
         lib.ref_vox_updates.restype = C.c_longlong
@@ -361,8 +363,33 @@ def ref_random2_sequence(seed: int, n: int) -> np.ndarray:
     return out
 
 
-def ref_reconstruct(pb: Problem, workdir: str, max_iter: int = 1000, num_stages: int = 0, threads: int = 0):
-    """Run the reference's ``reconstruct`` in ``workdir``.
+def ref_offset_update(pb: Problem, mode: int, err: np.ndarray, d: np.ndarray):
+    """The reference's update_Sinogram_Offset (MBIR_4D/XT_ICD_update.c:749-923)
+    on err [N_p][N_r][N_t] and offset d [N_r][N_t]; returns the updated copies."""
+    e2 = np.ascontiguousarray(err, np.float32).copy()
+    d2 = np.ascontiguousarray(d, np.float32).copy()
+    s = pb.ref_struct()
+    if ref_lib().ref_offset_update(C.byref(s), mode, e2, d2) != 0:
+        raise RuntimeError("reference offset update failed")
+    return e2, d2
+
+
+def ref_variance_update(pb: Problem, err: np.ndarray, w: np.ndarray, var_est: float):
+    """The reference's update_variance_parameter (MBIR_4D/XT_ICD_update.c:716-747)
+    on err and weights w ([N_p][N_r][N_t]) with the current variance; returns
+    (new weights, new variance)."""
+    w2 = np.ascontiguousarray(w, np.float32).copy()
+    v = C.c_double(var_est)
+    if ref_lib().ref_variance_update(C.byref(pb.ref_struct()), np.ascontiguousarray(err, np.float32), w2,
+                                     C.byref(v)) != 0:
+        raise RuntimeError("reference variance update failed")
+    return w2, v.value
+
+
+def ref_reconstruct(pb: Problem, workdir: str, max_iter: int = 1000, num_stages: int = 0, threads: int = 0,
+                    remove_rings: int = 0):
+    """Run the reference's ``reconstruct`` in ``workdir`` (remove_rings: its
+    ring-correction mode, 0 = off).
 
     Returns (object with halo [N_time][N_z+2][N_y][N_x] as the reference
     returns it, FP64 cost per iteration from cost.bin, voxel updates counted).
@@ -376,7 +403,7 @@ def ref_reconstruct(pb: Problem, workdir: str, max_iter: int = 1000, num_stages:
     os.makedirs(workdir, exist_ok=True)
     os.chdir(workdir)
     try:
-        rc = lib.ref_reconstruct(C.byref(s), threads, C.byref(out))
+        rc = lib.ref_reconstruct(C.byref(s), threads, remove_rings, C.byref(out))
     finally:
         os.chdir(cwd)
     if rc != 0:

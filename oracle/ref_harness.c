@@ -77,7 +77,7 @@ static FILE *ref_log(void)
     return f;
 }
 
-static int ref_init(RefState *st, const RefProblem *pb)
+static int ref_init_rings(RefState *st, const RefProblem *pb, int32_t remove_rings)
 {
     int32_t mxy[1], mz[1];
     memset(st, 0, sizeof(*st));
@@ -86,14 +86,16 @@ static int ref_init(RefState *st, const RefProblem *pb)
     st->T.debug_file_ptr = ref_log();
     if (initStructures(&st->S, &st->O, &st->T, 0, mxy, mz, pb->projections, pb->weights, pb->proj_angles,
                        pb->proj_times, pb->recon_times, pb->proj_rows, pb->proj_cols, pb->proj_num, pb->recon_num,
-                       pb->vox_wid, pb->rot_center, pb->sig_s, pb->sig_t, pb->c_s, pb->c_t, pb->convg_thresh, 0,
-                       pb->quad_convex, pb->huber_delta, pb->huber_T))
+                       pb->vox_wid, pb->rot_center, pb->sig_s, pb->sig_t, pb->c_s, pb->c_t, pb->convg_thresh,
+                       remove_rings, pb->quad_convex, pb->huber_delta, pb->huber_T))
         return -1;
     st->H_r = (Real_arr_t **)multialloc(sizeof(Real_arr_t), 2, st->S.N_p, DETECTOR_RESPONSE_BINS + 1);
     st->H_t = (Real_arr_t *)get_spc(DETECTOR_RESPONSE_BINS + 1, sizeof(Real_arr_t));
     DetectorResponseProfile(st->H_r, st->H_t, &st->S, &st->O, &st->T);
     return 0;
 }
+
+static int ref_init(RefState *st, const RefProblem *pb) { return ref_init_rings(st, pb, 0); }
 
 static void ref_fini(RefState *st, int projection_freed)
 {
@@ -275,16 +277,77 @@ void ref_random2_sequence(uint32_t seed, int32_t n, double *out)
  * The returned buffer is the reference's own allocation and must be passed to
  * ref_free.
  */
-int ref_reconstruct(const RefProblem *pb, int32_t threads, float **object)
+int ref_reconstruct(const RefProblem *pb, int32_t threads, int32_t remove_rings, float **object)
 {
     int rc;
     if (threads > 0) omp_set_num_threads(threads);
     *object = NULL;
     rc = reconstruct(object, pb->projections, pb->weights, pb->proj_angles, pb->proj_times, pb->recon_times,
                      pb->proj_rows, pb->proj_cols, pb->proj_num, pb->recon_num, pb->vox_wid, pb->rot_center,
-                     pb->sig_s, pb->sig_t, pb->c_s, pb->c_t, pb->convg_thresh, 0, pb->quad_convex,
+                     pb->sig_s, pb->sig_t, pb->c_s, pb->c_t, pb->convg_thresh, remove_rings, pb->quad_convex,
                      pb->huber_delta, pb->huber_T, 0, ref_log());
     return rc;
 }
 
 void ref_free(void *p) { free(p); }
+
+/*
+ * One ring-correction update, update_Sinogram_Offset (XT_ICD_update.c:916-923),
+ * of a problem set up by initStructures with remove_rings = mode: err
+ * [N_p][N_r][N_t] (the error sinogram y - Ax - d) and d [N_r][N_t] (the
+ * offset) are updated in place. ProjSelect is set from err first, as the
+ * reference keeps it (|e sqrt(w)| < ErrorSinoThresh).
+ */
+void update_Sinogram_Offset(Sinogram *SinogramPtr, TomoInputs *TomoInputsPtr, Real_arr_t ***ErrorSino);
+
+int ref_offset_update(const RefProblem *pb, int32_t mode, float *err, float *d)
+{
+    RefState st;
+    Real_arr_t ***E;
+    size_t i, n, nrt;
+    if (ref_init_rings(&st, pb, mode)) return -1;
+    n = (size_t)st.S.N_p * st.S.N_r * st.S.N_t;
+    nrt = (size_t)st.S.N_r * st.S.N_t;
+    E = (Real_arr_t ***)multialloc(sizeof(Real_arr_t), 3, st.S.N_p, st.S.N_r, st.S.N_t);
+    memcpy(&E[0][0][0], err, n * sizeof(float));
+    memcpy(&st.S.ProjOffset[0][0], d, nrt * sizeof(float));
+    for (i = 0; i < n; i++)
+        (&st.S.ProjSelect[0][0][0])[i] =
+            fabs((&E[0][0][0])[i] * sqrt((&st.T.Weight[0][0][0])[i])) < st.T.ErrorSinoThresh;
+    update_Sinogram_Offset(&st.S, &st.T, E);
+    memcpy(err, &E[0][0][0], n * sizeof(float));
+    memcpy(d, &st.S.ProjOffset[0][0], nrt * sizeof(float));
+    multifree(E, 3);
+    ref_fini(&st, 0);
+    return 0;
+}
+
+/*
+ * One noise-variance re-estimation, update_variance_parameter
+ * (XT_ICD_update.c:716-747), of a problem set up by initStructures: err
+ * [N_p][N_r][N_t], w [N_p][N_r][N_t] (the current weights, updated in place)
+ * and *var_est (updated). ProjSelect is set from err and w first.
+ */
+void update_variance_parameter(Sinogram *SinogramPtr, TomoInputs *TomoInputsPtr, Real_arr_t ***ErrorSino);
+
+int ref_variance_update(const RefProblem *pb, const float *err, float *w, double *var_est)
+{
+    RefState st;
+    Real_arr_t ***E;
+    size_t i, n;
+    if (ref_init(&st, pb)) return -1;
+    n = (size_t)st.S.N_p * st.S.N_r * st.S.N_t;
+    E = (Real_arr_t ***)multialloc(sizeof(Real_arr_t), 3, st.S.N_p, st.S.N_r, st.S.N_t);
+    memcpy(&E[0][0][0], err, n * sizeof(float));
+    memcpy(&st.T.Weight[0][0][0], w, n * sizeof(float));
+    st.T.var_est = *var_est;
+    for (i = 0; i < n; i++)
+        (&st.S.ProjSelect[0][0][0])[i] =
+            fabs((&E[0][0][0])[i] * sqrt((&st.T.Weight[0][0][0])[i])) < st.T.ErrorSinoThresh;
+    update_variance_parameter(&st.S, &st.T, E);
+    memcpy(w, &st.T.Weight[0][0][0], n * sizeof(float));
+    *var_est = st.T.var_est;
+    multifree(E, 3);
+    ref_fini(&st, 0);
+    return 0;
+}

@@ -118,9 +118,7 @@ extern "C" int reconstruct(float **object, float *projections, float *weights, f
     FILE *dbg = debug_msg_ptr;
     if (!object) return fail("object pointer is NULL");
     *object = nullptr;
-    if (remove_rings != 0)
-        return fail("remove_rings = %d: ring correction (projection offset estimation) is not part of this build.",
-                    remove_rings);
+    if (remove_rings < 0 || remove_rings > 3) return fail("remove_rings must be 0, 1, 2 or 3 (got %d)", remove_rings);
     const mbirgpu_options opt = current_options();
     log_info(dbg, "Reconstructing the data ....\n");
 
@@ -183,6 +181,8 @@ extern "C" int reconstruct(float **object, float *projections, float *weights, f
     pb.huber_T = huber_T;
 
     std::vector<float> prev;  // previous stage's object, [T][Z][Y][X]
+    std::vector<float> offset((size_t)proj_cols * proj_rows, 0.0f);  // ring-correction offset d [N_r][N_t]
+    bool have_offset = false;
     int prev_nz = 0, prev_ny = 0, prev_nx = 0;
     std::vector<float> cur;
     int nz = 0, ny = 0, nx = 0;
@@ -221,6 +221,28 @@ extern "C" int reconstruct(float **object, float *projections, float *weights, f
                 return -1;
             }
         }
+        // ring correction: none in the first stage, estimated from zero in the
+        // second, from the previous stage's offset (proj_offset.bin) after that
+        // (updateProjOffset, XT_Init.c:246-255, 345-349)
+        if (remove_rings && si >= 1) {
+            if (si >= 2 && !have_offset) {
+                if (!read_bin("proj_offset", offset.data(), offset.size() * sizeof(float))) {
+                    mbirgpu_session_destroy(sp);
+                    return fail("cannot read proj_offset.bin to initialise stage %d", si);
+                }
+                have_offset = true;
+            }
+            if (mbirgpu_session_set_ring_correction(sp, remove_rings, si >= 2 ? offset.data() : nullptr)) {
+                mbirgpu_session_destroy(sp);
+                return -1;
+            }
+        }
+        // noise-variance re-estimation with the generalised-Huber data term after
+        // the first stage (updateVar, XT_Init.c:270-278)
+        if (!quad_convex && si >= 1 && mbirgpu_session_set_variance_estimation(sp, 1)) {
+            mbirgpu_session_destroy(sp);
+            return -1;
+        }
         // ICD loop with cost log, XT_ICD_update.c:1148-1189
         std::vector<double> costs(opt.max_iterations + 1, 0.0);
         int iters = 0;
@@ -241,15 +263,22 @@ extern "C" int reconstruct(float **object, float *projections, float *weights, f
             mbirgpu_session_destroy(sp);
             return -1;
         }
+        if (remove_rings && si >= 1) {
+            if (mbirgpu_session_get_offset(sp, offset.data())) {
+                mbirgpu_session_destroy(sp);
+                return -1;
+            }
+            have_offset = true;
+        }
         if (opt.write_files) {
             bool ok = true;
             if (opt.compute_cost) ok &= write_bin("cost", costs.data(), (size_t)(iters + 1) * sizeof(double));
             const size_t n = (size_t)nz * ny * nx;
             for (int t = 0; t < recon_num && ok; t++)
                 ok &= write_bin("object_time_" + std::to_string(t), cur.data() + t * n, n * sizeof(float));
-            std::vector<float> offset((size_t)proj_cols * proj_rows, 0.0f);
             ok &= write_bin("proj_offset", offset.data(), offset.size() * sizeof(float));
-            const double var_est = 1.0;
+            double var_est = 1.0;
+            mbirgpu_session_get_variance(sp, &var_est);
             ok &= write_bin("variance_estimate", &var_est, sizeof(var_est));
             std::vector<float> mag((size_t)recon_num * ny * nx);
             if (cudaMemcpy(mag.data(), s->d_mag, mag.size() * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess)

@@ -94,21 +94,28 @@ __global__ void __launch_bounds__(256) forward_project_kernel(Geom g, const uint
 }
 
 __global__ void finish_projection_kernel(size_t n, const double *__restrict__ acc, const float *__restrict__ y,
-                                         float *__restrict__ out)
+                                         float *__restrict__ out, const float *__restrict__ off, int nrt)
 {
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-        out[i] = y ? (float)((double)y[i] - acc[i]) : (float)acc[i];
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        if (!y) {
+            out[i] = (float)acc[i];
+        } else {
+            const float e = (float)((double)y[i] - acc[i]);
+            out[i] = off ? e - off[i % nrt] : e;  // initErrorSinogam, XT_ICD_update.c:689
+        }
+    }
 }
 
 void launch_forward_project(const Geom &g, const uint32_t *d_table, const int32_t *d_view_first,
-                            const float *d_x, const float *d_y, double *d_acc, float *d_out, cudaStream_t st)
+                            const float *d_x, const float *d_y, double *d_acc, float *d_out, cudaStream_t st,
+                            const float *d_off)
 {
     const size_t n = (size_t)g.N_p * g.N_r * g.N_t;
     cudaMemsetAsync(d_acc, 0, n * sizeof(double), st);
     const long long warps = (long long)g.N_time * g.N_x * g.N_y;
     const long long blocks = (warps * 32 + 255) / 256;
     forward_project_kernel<<<(unsigned)blocks, 256, 0, st>>>(g, d_table, d_view_first, d_x, d_acc);
-    finish_projection_kernel<<<148 * 8, 256, 0, st>>>(n, d_acc, d_y, d_out);
+    finish_projection_kernel<<<148 * 8, 256, 0, st>>>(n, d_acc, d_y, d_out, d_off, g.N_r * g.N_t);
 }
 
 // One warp per (frame, column); out is [N_time][N_y][N_x][N_z].

@@ -76,10 +76,26 @@ void launch_count_masked_nnz(const Geom &g, int n_assigned, const int32_t *d_vie
                              const uint8_t *d_mask, const uint32_t *d_table, unsigned long long *d_out,
                              cudaStream_t st);
 
-// e = y - A x (FP64 accumulation in d_acc, N_p*N_r*N_t doubles); when d_y is
-// null the result is A x itself. Rows of views outside every frame get y (or 0).
+// e = y - A x - d (FP64 accumulation in d_acc, N_p*N_r*N_t doubles; d the
+// per-detector-pixel offset [N_r][N_t], may be null); when d_y is null the
+// result is A x itself. Rows of views outside every frame get y - d (or 0).
 void launch_forward_project(const Geom &g, const uint32_t *d_table, const int32_t *d_view_first,
-                            const float *d_x, const float *d_y, double *d_acc, float *d_out, cudaStream_t st);
+                            const float *d_x, const float *d_y, double *d_acc, float *d_out, cudaStream_t st,
+                            const float *d_off = nullptr);
+
+// Ring correction (kernels_offset.cu): one update of the per-detector-pixel
+// offset d (mode 1 unconstrained, 2 zero mean, 3 the reference's window mode,
+// which in its reconstruct has no windows) with e changed by the offset's
+// change in every view. Scratch: d_num, d_lam ([N_r][N_t] doubles), d_gamma
+// (1 double), d_x ([N_r][N_t] floats). Returns 0 or -1.
+int offset_update(const Geom &g, int mode, int N_p, float *d_err, const float *d_w, float *d_off, double *d_num,
+                  double *d_lam, double *d_gamma, float *d_x, cudaStream_t st);
+// Noise variance re-estimation of the generalised-Huber data term: scales the
+// weights in place (W <- W v_old / v_new) and updates *var_est (host);
+// d_scratch holds variance_scratch_doubles() doubles.
+size_t variance_scratch_doubles();
+int variance_update(const Geom &g, int N_p, const float *d_err, float *d_w, double *var_est, double *d_scratch,
+                    cudaStream_t st);
 void launch_back_project(const Geom &g, const uint32_t *d_table, const int32_t *d_view_first,
                          const int32_t *d_views, const float *d_sino, float *d_x, cudaStream_t st);
 

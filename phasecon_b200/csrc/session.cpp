@@ -65,7 +65,8 @@ Session::~Session()
 {
     void *ptrs[] = {d_y, d_w, d_err, d_x, d_tmp, d_table, d_Hr, d_cos, d_sin, d_views, d_view_first, d_view_frame,
                     d_mask, d_mag, d_stats, d_cost_partials, d_cost_out, d_flag, d_acc, d_queue, d_filt, d_sel,
-                    d_nh_items, d_nh_n, d_nh_scratch, d_nh_selstate};
+                    d_nh_items, d_nh_n, d_nh_scratch, d_nh_selstate, d_off, d_offx, d_onum, d_olam, d_ogamma,
+                    d_var};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     for (auto &ev : ev_pairs) {
@@ -281,7 +282,7 @@ int Session::autotune()
 int Session::refresh_error()
 {
     // views outside every frame keep e = y (they never enter the problem)
-    launch_forward_project(hs.g, d_table, d_view_first, d_x, d_y, d_acc, d_err, st);
+    launch_forward_project(hs.g, d_table, d_view_first, d_x, d_y, d_acc, d_err, st, rings ? d_off : nullptr);
     CK(cudaGetLastError());
     return 0;
 }
@@ -313,9 +314,11 @@ int Session::cost(double *total, double *data, double *prior)
     double h[2];
     CK(cudaMemcpyAsync(h, d_cost_out, sizeof(h), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
-    if (data) *data = h[0];
+    // the variance's normalisation N log(var) / 2 (XT_ICD_update.c:307); 0 while var = 1
+    const double lognorm = (double)g.N_p * g.N_r * g.N_t * std::log(var_est) / 2;
+    if (data) *data = h[0] + lognorm;
     if (prior) *prior = h[1];
-    if (total) *total = h[0] + h[1];
+    if (total) *total = h[0] + lognorm + h[1];
     return 0;
 }
 
@@ -352,6 +355,7 @@ int Session::icd_iteration(int iter, mbirgpu_iter_stats *out)
     for (int ph = 0; ph < phases; ph++) {
         L.phase = ph;
         launch_icd_phase(gb, L, d_table, d_view_first, d_mask, d_x, d_err, d_w, d_mag, d_stats, d_queue + ph, st);
+        if (rings && update_offset()) return -1;
     }
     if (timing) CK(cudaEventRecord(ev_pairs[0].second, st));
     int launches = phases;
@@ -386,10 +390,13 @@ int Session::icd_iteration(int iter, mbirgpu_iter_stats *out)
             launch_icd_phase(gb, Ln, d_table, d_view_first, d_mask, d_x, d_err, d_w, d_mag, d_stats,
                              d_queue + kMaxPhases * (pass + 1) + ph, st);
         }
+        if (rings && update_offset()) return -1;
         launches += nh_phases + 11 + (lists ? 3 : 0);  // filter + 10 select launches, 3 list launches
     }
     if (nh > 0 && timing) CK(cudaEventRecord(ev_pairs[1].second, st));
     CK(cudaGetLastError());
+    if (update_var && variance_update(g, g.N_p, d_err, d_w, &var_est, d_var, st))
+        return fail("variance update failed: %s", cudaGetErrorString(cudaGetLastError()));
     if (opt.refresh_every > 0 && iter % opt.refresh_every == 0)
         if (refresh_error()) return -1;
     IcdStats hst;
@@ -553,6 +560,48 @@ int Session::set_object_fbp()
 }
 
 int unet_apply_frames(UNet *u, float *d_vol, int N_time, int N_z, int N_y, int N_x);
+
+// Ring correction of reconstruct (remove_rings 1..3): the offset d enters
+// e = y - Ax - d and is re-estimated after every full-sweep phase and every
+// NH pass (the reference re-estimates after each of its z-block phases,
+// XT_ICD_update.c:983-1043). offset: the starting d (host, [N_r][N_t]), null = 0.
+int Session::set_ring_correction(int mode, const float *offset)
+{
+    const Geom &g = hs.g;
+    if (mode < 0 || mode > 3) return fail("remove_rings must be 0, 1, 2 or 3 (got %d)", mode);
+    const size_t nrt = (size_t)g.N_r * g.N_t;
+    size_t &acc = device_bytes;
+    if (!d_off && (dalloc(&d_off, nrt, &acc) || dalloc(&d_offx, nrt, &acc) || dalloc(&d_onum, nrt, &acc) ||
+                   dalloc(&d_olam, nrt, &acc) || dalloc(&d_ogamma, 1, &acc)))
+        return -1;
+    if (offset) CK(cudaMemcpyAsync(d_off, offset, nrt * sizeof(float), cudaMemcpyHostToDevice, st));
+    else CK(cudaMemsetAsync(d_off, 0, nrt * sizeof(float), st));
+    rings = mode;
+    if (refresh_error()) return -1;
+    CK(cudaStreamSynchronize(st));
+    return 0;
+}
+
+// Noise-variance re-estimation of reconstruct with the generalised-Huber data
+// term (quad_convex = 0) after the first multires stage (updateVar,
+// XT_Init.c:270-278): var starts at 1 and is re-estimated at the end of every
+// iteration, the weights rescaled with it.
+int Session::set_variance_estimation(int on)
+{
+    if (on && !d_var) {
+        size_t &acc = device_bytes;
+        if (dalloc(&d_var, variance_scratch_doubles(), &acc)) return -1;
+    }
+    update_var = on ? 1 : 0;
+    return 0;
+}
+
+int Session::update_offset()
+{
+    if (offset_update(hs.g, rings, hs.g.N_p, d_err, d_w, d_off, d_onum, d_olam, d_ogamma, d_offx, st))
+        return fail("ring correction update failed: %s", cudaGetErrorString(cudaGetLastError()));
+    return 0;
+}
 
 int Session::set_object_unet(UNet *u)
 {
@@ -773,6 +822,64 @@ int mbirgpu_session_set_object_fbp(mbirgpu_session *sp)
 {
     SESSION(sp);
     return s->set_object_fbp();
+}
+
+int mbirgpu_session_set_ring_correction(mbirgpu_session *sp, int32_t remove_rings, const float *offset)
+{
+    SESSION(sp);
+    return s->set_ring_correction(remove_rings, offset);
+}
+
+int mbirgpu_session_set_variance_estimation(mbirgpu_session *sp, int32_t on)
+{
+    SESSION(sp);
+    return s->set_variance_estimation(on);
+}
+
+int mbirgpu_session_get_variance(mbirgpu_session *sp, double *var_est)
+{
+    SESSION(sp);
+    if (!var_est) return fail("NULL argument");
+    *var_est = s->var_est;
+    return 0;
+}
+
+int mbirgpu_session_update_variance(mbirgpu_session *sp)
+{
+    SESSION(sp);
+    if (!s->d_var) {  // allocate the scratch without switching the per-iteration update on
+        const int on = s->update_var;
+        if (s->set_variance_estimation(1)) return -1;
+        s->update_var = on;
+    }
+    const mbirgpu::Geom &g = s->hs.g;
+    if (mbirgpu::variance_update(g, g.N_p, s->d_err, s->d_w, &s->var_est, s->d_var, s->st))
+        return fail("variance update failed: %s", cudaGetErrorString(cudaGetLastError()));
+    return 0;
+}
+
+int mbirgpu_session_update_offset(mbirgpu_session *sp)
+{
+    SESSION(sp);
+    if (!s->rings) return fail("ring correction is off (mbirgpu_session_set_ring_correction)");
+    if (s->update_offset()) return -1;
+    cudaError_t e = cudaStreamSynchronize(s->st);
+    return e == cudaSuccess ? 0 : fail("offset update failed: %s", cudaGetErrorString(e));
+}
+
+int mbirgpu_session_get_offset(mbirgpu_session *sp, float *offset)
+{
+    SESSION(sp);
+    if (!offset) return fail("NULL offset");
+    const mbirgpu::Geom &g = s->hs.g;
+    const size_t nrt = (size_t)g.N_r * g.N_t;
+    if (!s->d_off) {
+        std::memset(offset, 0, nrt * sizeof(float));
+        return 0;
+    }
+    cudaError_t e = cudaMemcpyAsync(offset, s->d_off, nrt * sizeof(float), cudaMemcpyDeviceToHost, s->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
+    return e == cudaSuccess ? 0 : fail("offset download failed: %s", cudaGetErrorString(e));
 }
 
 int mbirgpu_session_set_object_unet(mbirgpu_session *sp, mbirgpu_unet *u)

@@ -46,6 +46,16 @@ struct Session {
     uint64_t *d_nh_selstate = nullptr;  // radix-select state (nh_select_scratch_bytes)
     size_t nh_items_cap = 0, nh_scratch_cap = 0;  // ints allocated
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pairs;
+    // ring correction: offset d [N_r][N_t] of e = y - Ax - d, updated after
+    // every full-sweep phase and every NH pass while rings != 0
+    int rings = 0;
+    float *d_off = nullptr, *d_offx = nullptr;
+    double *d_onum = nullptr, *d_olam = nullptr, *d_ogamma = nullptr;
+    // noise variance of the generalised-Huber data term, re-estimated at the
+    // end of every iteration while update_var (weights scaled in place)
+    int update_var = 0;
+    double var_est = 1.0;
+    double *d_var = nullptr;
 
     ~Session();
     int init(const mbirgpu_problem *pb, const mbirgpu_options *o, int mult_xy, int mult_z, void *stream);
@@ -69,6 +79,9 @@ struct Session {
     int fbp(float *obj);              // host [N_time][N_z][N_y][N_x]
     int set_object_fbp();             // x = FBP, then e = y - A x
     int set_object_unet(UNet *u);     // x = U-Net(FBP) per frame, then e = y - A x
+    int set_ring_correction(int mode, const float *offset);  // mode 0..3, offset host [N_r][N_t] or null
+    int update_offset();
+    int set_variance_estimation(int on);
 };
 
 }  // namespace mbirgpu

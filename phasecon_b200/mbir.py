@@ -28,7 +28,9 @@ EXPORTS = (
     "mbirgpu_session_cost", "mbirgpu_session_icd_iteration", "mbirgpu_session_forward_project",
     "mbirgpu_session_back_project", "mbirgpu_session_get_amatrix", "mbirgpu_session_get_detector_response",
     "mbirgpu_session_run", "mbirgpu_session_forward_project_noalloc", "mbirgpu_session_nh_select",
-    "mbirgpu_session_fbp", "mbirgpu_session_set_object_fbp",
+    "mbirgpu_session_fbp", "mbirgpu_session_set_object_fbp", "mbirgpu_session_set_ring_correction",
+    "mbirgpu_session_get_offset", "mbirgpu_session_update_offset", "mbirgpu_session_set_variance_estimation",
+    "mbirgpu_session_update_variance", "mbirgpu_session_get_variance",
     "mbirgpu_unet_create", "mbirgpu_unet_destroy", "mbirgpu_unet_num_params", "mbirgpu_unet_set_input_scale",
     "mbirgpu_unet_get_input_scale", "mbirgpu_unet_get_params", "mbirgpu_unet_set_params", "mbirgpu_unet_forward",
     "mbirgpu_unet_gradients", "mbirgpu_unet_train_step", "mbirgpu_session_set_object_unet",
@@ -135,6 +137,12 @@ def lib() -> C.CDLL:
         L.mbirgpu_session_nh_select.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         L.mbirgpu_session_fbp.argtypes = [C.c_void_p, C.c_void_p]
         L.mbirgpu_session_set_object_fbp.argtypes = [C.c_void_p]
+        L.mbirgpu_session_set_ring_correction.argtypes = [C.c_void_p, C.c_int32, C.c_void_p]
+        L.mbirgpu_session_update_offset.argtypes = [C.c_void_p]
+        L.mbirgpu_session_get_offset.argtypes = [C.c_void_p, C.c_void_p]
+        L.mbirgpu_session_set_variance_estimation.argtypes = [C.c_void_p, C.c_int32]
+        L.mbirgpu_session_update_variance.argtypes = [C.c_void_p]
+        L.mbirgpu_session_get_variance.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
         L.mbirgpu_batch_create.argtypes = [C.POINTER(C.c_void_p), C.c_void_p, C.c_int32, C.POINTER(Options),
                                            C.c_void_p]
         L.mbirgpu_batch_destroy.argtypes = [C.c_void_p]
@@ -343,6 +351,37 @@ class Session:
 
     def set_object_fbp(self) -> None:
         _check(lib().mbirgpu_session_set_object_fbp(self.h))
+
+    def set_ring_correction(self, remove_rings: int, offset: np.ndarray | None = None) -> None:
+        """Estimate a per-detector-pixel offset d (remove_rings 1, 2, 3; 0 off),
+        starting from offset [proj_cols][proj_rows] (None = zero)."""
+        ptr = None
+        if offset is not None:
+            self._offset_in = np.ascontiguousarray(offset, np.float32)
+            ptr = self._offset_in.ctypes.data
+        _check(lib().mbirgpu_session_set_ring_correction(self.h, remove_rings, ptr))
+
+    def update_offset(self) -> None:
+        _check(lib().mbirgpu_session_update_offset(self.h))
+
+    def set_variance_estimation(self, on: bool) -> None:
+        _check(lib().mbirgpu_session_set_variance_estimation(self.h, 1 if on else 0))
+
+    def update_variance(self) -> float:
+        _check(lib().mbirgpu_session_update_variance(self.h))
+        return self.variance
+
+    @property
+    def variance(self) -> float:
+        v = C.c_double()
+        _check(lib().mbirgpu_session_get_variance(self.h, C.byref(v)))
+        return v.value
+
+    def get_offset(self) -> np.ndarray:
+        """The offset d, [proj_cols][proj_rows]."""
+        a = np.zeros(self.sino_shape[1:], np.float32)
+        _check(lib().mbirgpu_session_get_offset(self.h, a.ctypes.data))
+        return a
 
     def nh_select(self, mag: np.ndarray) -> np.ndarray:
         """NH-ICD voxel-line selection [N_time][N_y][N_x] (uint8) for an
