@@ -59,8 +59,10 @@ def parse():
     ap.add_argument("--workload", default="4d", choices=["4d", "batch", "warmstart"],
                     help="4d: the 4-D benchmark (default); batch: 48 uneven 3-D problems, batched vs sequential; "
                          "warmstart: the learned warm start on the 4-D workload")
-    ap.add_argument("--train-scans", type=int, default=8, help="seeded 4-D training scans (8 frame pairs each)")
-    ap.add_argument("--train-steps", type=int, default=3000)
+    ap.add_argument("--train-scans", type=int, default=16, help="seeded 4-D training scans (8 frame pairs each)")
+    ap.add_argument("--train-steps", type=int, default=6000)
+    ap.add_argument("--average-from", type=float, default=0.7,
+                    help="warm start: average the network weights from this fraction of the training steps on (1 = off)")
     return ap.parse_args()
 
 
@@ -476,7 +478,7 @@ def run_warmstart(args, world, rank, local, pg):
     net = WS.UNet(16, seed=rank)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    hist = WS.train(net, pairs, args.train_steps, lr=1e-3, seed=rank)
+    hist = WS.train(net, pairs, args.train_steps, lr=1e-3, seed=rank, average_from=args.average_from)
     torch.cuda.synchronize()
     t_train = time.perf_counter() - t0
     pb, _, p = W.config_4d(seed=0)

@@ -607,20 +607,18 @@ int Session::set_object_unet(UNet *u)
 {
     const Geom &g = hs.g;
     if (!fbp_supported(g)) return fail("FBP: %d channels x %d rows per view exceed the filter's shared memory", g.N_r, g.N_t);
-    float *d_v = nullptr;
-    size_t acc = 0;
-    if (dalloc(&d_v, n_vox, &acc)) return -1;
+    // d_tmp (max(sinogram, volume) floats) holds the filtered sinogram during
+    // the FBP, then the volume in the network's [T][Z][Y][X] layout
     launch_fbp(g, d_table, d_view_first, d_views, d_y, d_tmp, d_x, st);
-    launch_zfast_to_vol(d_x, d_v, g.N_time, g.N_z, g.N_y, g.N_x, st);
+    launch_zfast_to_vol(d_x, d_tmp, g.N_time, g.N_z, g.N_y, g.N_x, st);
     cudaError_t e = cudaStreamSynchronize(st);  // the network runs on its own stream
-    int rc = e == cudaSuccess ? unet_apply_frames(u, d_v, g.N_time, g.N_z, g.N_y, g.N_x) : -1;
+    int rc = e == cudaSuccess ? unet_apply_frames(u, d_tmp, g.N_time, g.N_z, g.N_y, g.N_x) : -1;
     if (!rc) {
-        launch_vol_to_zfast(d_v, d_x, g.N_time, g.N_z, g.N_y, g.N_x, st);
+        launch_vol_to_zfast(d_tmp, d_x, g.N_time, g.N_z, g.N_y, g.N_x, st);
         launch_mask_object(g, d_mask, d_x, st);
         rc = refresh_error();
         e = cudaStreamSynchronize(st);
     }
-    cudaFree(d_v);
     if (e != cudaSuccess) return fail("warm start failed: %s", cudaGetErrorString(e));
     return rc;
 }

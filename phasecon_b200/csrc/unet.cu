@@ -55,6 +55,17 @@ __device__ __forceinline__ void mma_bf16(float (&c)[4], const uint32_t (&a)[4], 
 
 __device__ __forceinline__ uint32_t ld_pair(const bf16 *p) { return *reinterpret_cast<const uint32_t *>(p); }
 
+// Four 8x8 b16 matrices from shared memory in one instruction
+// (ldmatrix.x4): lane l supplies the address of row l % 8 of matrix l / 8, and
+// receives its fragment of each matrix in r[0..3].
+__device__ __forceinline__ void ldsm_x4(uint32_t (&r)[4], const bf16 *p)
+{
+    const unsigned a = (unsigned)__cvta_generic_to_shared(p);
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0, %1, %2, %3}, [%4];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(a));
+}
+
 constexpr int kPadK = 24;  // shared-memory row stride (16 + 8) in bf16: conflict-free fragment loads
 
 // Output tile of the forward convolution CTA: FZ x FY x FX voxels (256 = 8
@@ -134,6 +145,12 @@ __global__ void __launch_bounds__(kFThreads) conv_tile_kernel(const bf16 *__rest
             }
         }
         __syncthreads();
+        // ldmatrix lane roles: A (16 voxels x 16 channels) matrices are
+        // (voxels 0-7 | 8-15) x (channels 0-7 | 8-15) in the mma fragment order;
+        // B (16 output channels x 16 k) matrices are (outputs 0-7 | 8-15) x (k 0-7 | 8-15)
+        const int lm = lane >> 3, lr = lane & 7;
+        const int a_row = (lm & 1) * 8 + lr, a_k = (lm >> 1) * 8;
+        const int b_row = (lm >> 1) * 8 + lr, b_k = (lm & 1) * 8;
 #pragma unroll 1
         for (int tap = 0; tap < 27; tap++) {
             const int dz = tap / 9, dy = (tap / 3) % 3, dx = tap % 3;  // halo offsets 0..2
@@ -141,14 +158,15 @@ __global__ void __launch_bounds__(kFThreads) conv_tile_kernel(const bf16 *__rest
             for (int i = 0; i < 2; i++) {
                 const int row = warp * 2 + i, tz = row / FY, ty = row % FY;
                 const bf16 *hrow = Hs + (((tz + dz) * FHY + ty + dy) * FHX + dx) * kPadK;
-                const uint32_t a[4] = {ld_pair(hrow + g * kPadK + tig * 2), ld_pair(hrow + (g + 8) * kPadK + tig * 2),
-                                       ld_pair(hrow + g * kPadK + tig * 2 + 8),
-                                       ld_pair(hrow + (g + 8) * kPadK + tig * 2 + 8)};
+                uint32_t a[4];
+                ldsm_x4(a, hrow + a_row * kPadK + a_k);
 #pragma unroll
-                for (int j = 0; j < NT / 8; j++) {
-                    const bf16 *wrow = Ws + (tap * NT + j * 8 + g) * kPadK;
-                    const uint32_t bb[2] = {ld_pair(wrow + tig * 2), ld_pair(wrow + tig * 2 + 8)};
-                    mma_bf16(acc[i][j], a, bb);
+                for (int j = 0; j < NT / 8; j += 2) {
+                    uint32_t b4[4];  // b4[0..1]: outputs j*8.., b4[2..3]: outputs (j+1)*8..
+                    ldsm_x4(b4, Ws + (tap * NT + j * 8 + b_row) * kPadK + b_k);
+                    const uint32_t b0[2] = {b4[0], b4[1]}, b1[2] = {b4[2], b4[3]};
+                    mma_bf16(acc[i][j], a, b0);
+                    mma_bf16(acc[i][j + 1], a, b1);
                 }
             }
         }

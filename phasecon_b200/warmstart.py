@@ -215,21 +215,36 @@ def training_pairs_4d(seed: int, ch_steps: int | None = None, rel: float = 1e-4)
     return [(fbp[f], target[f]) for f in range(fbp.shape[0])]
 
 
-def train(net: UNet, pairs, steps: int, lr: float = 1e-3, seed: int = 0, log_every: int = 0):
-    """Adam steps over randomly drawn (input, target) pairs of host arrays,
-    learning rate on a cosine schedule from `lr` down to lr / 100; returns the
-    loss history. The network's input scale is set so that it sees values of
-    order one."""
+def train(net: UNet, pairs, steps: int, lr: float = 1e-3, seed: int = 0, log_every: int = 0,
+          average_from: float = 1.0, average_every: int = 50):
+    """Adam steps over randomly drawn (input, target) pairs of host arrays;
+    returns the loss history. The network's input scale is set so that it
+    sees values of order one. Learning rate: a cosine schedule from `lr` down
+    to lr / 100 over all steps; with average_from < 1, the cosine runs down to
+    lr / 10 over the first average_from of the steps, the rest run at lr / 10
+    and the network ends as the average of its weights taken every
+    `average_every` steps over that tail (stochastic weight averaging)."""
     import torch
     rng = np.random.default_rng(seed)
     net.input_scale = 1.0 / max(float(np.mean([np.abs(t).max() for _, t in pairs])), 1e-12)
     dev = [(torch.from_numpy(np.ascontiguousarray(x, np.float32)).cuda(),
             torch.from_numpy(np.ascontiguousarray(t, np.float32)).cuda()) for x, t in pairs]
     hist = []
+    tail = int(average_from * steps) if average_from < 1.0 else steps
+    avg, navg = None, 0
     for s in range(steps):
         x, t = dev[int(rng.integers(0, len(dev)))]
-        lr_s = lr * (0.01 + 0.99 * 0.5 * (1.0 + np.cos(np.pi * s / max(1, steps))))
+        if tail < steps:
+            lr_s = lr * 0.1 if s >= tail else lr * (0.1 + 0.9 * 0.5 * (1.0 + np.cos(np.pi * s / max(1, tail))))
+        else:
+            lr_s = lr * (0.01 + 0.99 * 0.5 * (1.0 + np.cos(np.pi * s / max(1, steps))))
         hist.append(net.train_step(x, t, float(lr_s)))
+        if s >= tail and (s - tail) % average_every == average_every - 1:
+            p = net.get_params().astype(np.float64)
+            avg = p if avg is None else avg + p
+            navg += 1
         if log_every and (s + 1) % log_every == 0:
             print(f"step {s + 1}: loss {np.mean(hist[-log_every:]):.4g}", flush=True)
+    if navg:
+        net.set_params((avg / navg).astype(np.float32))
     return hist
