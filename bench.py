@@ -56,6 +56,10 @@ def parse():
     ap.add_argument("--no-converge", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--max-converge-iters", type=int, default=400)
+    ap.add_argument("--schedule", default="",
+                    help="4-D workload: fix the sweep schedule as SV,WARPS,COLORS (super-voxel edge, warps per "
+                         "column, K of the K x K colouring) instead of autotuning it, e.g. for a profiler run whose "
+                         "serialised timings would mislead the autotuner")
     ap.add_argument("--workload", default="4d", choices=["4d", "batch", "warmstart"],
                     help="4d: the 4-D benchmark (default); batch: 48 uneven 3-D problems, batched vs sequential; "
                          "warmstart: the learned warm start on the 4-D workload")
@@ -258,6 +262,8 @@ def run_ours(args, world, rank, local, pg):
     pb, _, p = W.config_4d(seed=0)
     opt = pc.get_options()
     opt.mrf_p = p
+    if args.schedule:
+        opt.sv_size, opt.cta_warps, opt.sv_colors = (int(v) for v in args.schedule.split(","))
     s = pc.Session(pb, options=opt, stream=stream.cuda_stream)
     s.set_timing(True)
     info = s.info

@@ -319,6 +319,12 @@ int mbirgpu_unet_gradients(mbirgpu_unet *u, const float *d_input, const float *d
 /* One Adam step (beta 0.9 / 0.999) on one (input, target) pair. */
 int mbirgpu_unet_train_step(mbirgpu_unet *u, const float *d_input, const float *d_target, int32_t D, int32_t H,
                             int32_t W, float lr, double *loss);
+/* Which tensor-core kernels run the 3x3x3 convolutions: 1 (default) the
+ * tcgen05 kernels (TMEM accumulators, TMA-staged operands) wherever input and
+ * output channel counts are multiples of 16, 0 the mma.sync kernels
+ * everywhere. No counterpart in the reference (the network has none). */
+int mbirgpu_unet_set_tensor_path(mbirgpu_unet *u, int32_t path);
+int32_t mbirgpu_unet_get_tensor_path(const mbirgpu_unet *u);
 /* The session's object becomes the network applied to each frame of the
  * filtered back-projection, zero outside the reconstruction circle; e = y - A x
  * is recomputed. */

@@ -98,17 +98,52 @@ __device__ __forceinline__ Rec<KW> load_rec_smem(const uint32_t *p)
 }
 
 // Copy a column's A records (nwords 32-bit words, a multiple of 4, 16-byte
-// aligned on both sides) into shared memory with cp.async; the copies land
-// while the CTA works on the current column and are waited for (per thread,
-// cp.async.wait_all) before the barrier that precedes their first use.
-__device__ __forceinline__ void stage_records(uint32_t *dst, const uint32_t *src, int nwords)
+// aligned on both sides) into shared memory with one TMA bulk copy, issued by
+// thread 0, that completes on the buffer's mbarrier; the copy lands while the
+// CTA works on the current column.
+__device__ __forceinline__ void stage_records(uint32_t *dst, const uint32_t *src, int nwords,
+                                              unsigned long long *bar)
 {
-    const unsigned base = (unsigned)__cvta_generic_to_shared(dst);
-    for (int i = threadIdx.x * 4; i < nwords; i += blockDim.x * 4)
-        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(base + 4u * i), "l"(src + i) : "memory");
-    asm volatile("cp.async.commit_group;" ::: "memory");
+    if (threadIdx.x != 0) return;
+    const unsigned b = (unsigned)__cvta_generic_to_shared(bar), d = (unsigned)__cvta_generic_to_shared(dst);
+    const unsigned bytes = 4u * (unsigned)nwords;
+    if (bytes == 0) {  // a frame without views: complete the phase with no transfer
+        asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(b) : "memory");
+        return;
+    }
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(bytes) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(d),
+                 "l"(src), "r"(bytes), "r"(b)
+                 : "memory");
 }
-__device__ __forceinline__ void wait_staged() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// Every thread waits for buffer b's copy: the n-th copy into a buffer
+// completes the mbarrier's phase n, so the parity of the wait is the count of
+// earlier waits on that buffer (bit b of `phases`, identical in every thread).
+// The wait is bounded (about 2 s); a copy that never lands is counted and the
+// host reports it.
+__device__ __forceinline__ void wait_staged(unsigned long long *bar, uint32_t &phases, int b, unsigned &timeouts)
+{
+    const unsigned a = (unsigned)__cvta_generic_to_shared(bar);
+    const uint32_t parity = (phases >> b) & 1u;
+    const long long t0 = clock64();
+    for (;;) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred P;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, P;\n\t}"
+            : "=r"(ok)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (ok) break;
+        if (clock64() - t0 > 4000000000LL) {
+            timeouts++;
+            break;
+        }
+    }
+    phases ^= 1u << b;
+}
 
 template <int KW>
 __device__ __forceinline__ float rec_val(const Rec<KW> &r, int q)
@@ -146,6 +181,7 @@ __device__ __forceinline__ void red_add(float *p, const float (&d)[2])
 
 
 struct IcdSmem {
+    unsigned long long stage_bar[2];  // completion of the two record buffers' bulk copies
     float num[kMaxWarps][32], den[kMaxWarps][32];
     float th1[kMaxWarps][32], th2[kMaxWarps][32];
     int pos[kMaxWarps][32];
@@ -157,6 +193,8 @@ struct IcdSmem {
 struct IcdCount {
     unsigned long long upd, skip;
     float sum_dx, sum_x;
+    unsigned timeouts;     // record copies that did not land in time
+    uint32_t phases;       // parity of the next wait on each record buffer
 };
 
 // Warp 0 adds the CTA's counters to the problem's statistics and clears them.
@@ -176,7 +214,10 @@ __device__ __forceinline__ void flush_counts(IcdCount &cnt, IcdStats *stats)
             atomicAdd(&stats->sum_abs_x, (double)cnt.sum_x);
         }
     }
+    if (cnt.timeouts && (threadIdx.x & 31) == 0) atomicAdd(&stats->stage_timeouts, cnt.timeouts);
+    const uint32_t phases = cnt.phases;
     cnt = IcdCount{};
+    cnt.phases = phases;
 }
 
 // Update the voxel columns of super-voxel (sx, sy) of frame f; the whole CTA
@@ -185,7 +226,7 @@ __device__ __forceinline__ void flush_counts(IcdCount &cnt, IcdStats *stats)
 // kUnroll: views whose records and sinogram entries are in flight together;
 // VEC: consecutive detector rows one lane owns (4 when N_t % 4 == 0, else 2);
 // kStaged: the column's records are read from shared memory (srec: two
-// buffers of stage_words words), the next column's copied in with cp.async
+// buffers of stage_words words), the next column's copied in by a TMA bulk copy
 // while the current one is updated, so the theta pass waits on one global
 // round trip per view group instead of two and the apply pass on none.
 template <int KW, int kUnroll, int VEC, bool kStaged>
@@ -251,7 +292,8 @@ __device__ __forceinline__ void icd_update_sv(const Geom &g, const IcdLaunch &L,
     __syncthreads();
     const int ncols = S.ncols;
     const size_t rec_frame = (size_t)fv0 * nxy;
-    if (kStaged && ncols > 0) stage_records(srec, table + (rec_frame + (size_t)S.order[0] * nv) * RW, nv * RW);
+    if (kStaged && ncols > 0)
+        stage_records(srec, table + (rec_frame + (size_t)S.order[0] * nv) * RW, nv * RW, &S.stage_bar[0]);
 
     for (int ci = 0; ci < ncols; ci++) {
         const int c = S.order[ci];
@@ -307,13 +349,13 @@ __device__ __forceinline__ void icd_update_sv(const Geom &g, const IcdLaunch &L,
             // neighbour (in-column neighbours are the column's own values)
             active_pred = !L.zero_skipping || L.iter <= 1 || (zl && V != 0.0f) || pos;
         }
-        if (kStaged) wait_staged();  // this column's records (issued one column earlier)
+        if (kStaged) wait_staged(&S.stage_bar[ci & 1], cnt.phases, ci & 1, cnt.timeouts);  // issued one column earlier
         const int any_active = __syncthreads_or(active_pred);
         // every thread is past the previous column's apply pass: its record
         // buffer may be refilled with the next column's
         if (kStaged && ci + 1 < ncols)
             stage_records(srec + ((ci + 1) & 1) * stage_words,
-                          table + (rec_frame + (size_t)S.order[ci + 1] * nv) * RW, nv * RW);
+                          table + (rec_frame + (size_t)S.order[ci + 1] * nv) * RW, nv * RW, &S.stage_bar[(ci + 1) & 1]);
         if (!any_active) {
             if (warp == 0 && zl) cnt.skip++;
             if (warp == 0 && lane == 0) mag[(size_t)f * nxy + c] = 0.0f;
@@ -512,6 +554,13 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 4) icd_phase_kernel(
     const int hx = (L.n_sv_x + KC - 1) / KC, slots = hx * ((L.n_sv_y + KC - 1) / KC);
     const int n_items = L.items ? *L.n_items : g.N_time * slots;
     IcdCount cnt{};
+    if (kStaged && threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"((unsigned)__cvta_generic_to_shared(&S.stage_bar[0]))
+                     : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"((unsigned)__cvta_generic_to_shared(&S.stage_bar[1]))
+                     : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
     for (;;) {
         __syncthreads();  // S.item / S.order of the previous SV are no longer read
         if (threadIdx.x == 0) S.item = (int)atomicAdd(queue, 1u);

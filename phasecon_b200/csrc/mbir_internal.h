@@ -165,6 +165,7 @@ inline int spread_multiplier(int n)
 struct IcdStats {  // device accumulators
     unsigned long long updates, skipped;
     double sum_abs_dx, sum_abs_x;
+    unsigned int stage_timeouts, pad;  // staged record copies that did not land within the wait limit
 };
 // Per-problem constants of the voxel update, in FP32.
 struct IcdConst {

@@ -402,6 +402,8 @@ int Session::icd_iteration(int iter, mbirgpu_iter_stats *out)
     IcdStats hst;
     CK(cudaMemcpyAsync(&hst, d_stats, sizeof(hst), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
+    if (hst.stage_timeouts)
+        return fail("ICD iteration %d: %u staged A-record copies did not complete", iter, hst.stage_timeouts);
     if (out) {
         std::memset(out, 0, sizeof(*out));
         out->voxel_updates = (int64_t)hst.updates;

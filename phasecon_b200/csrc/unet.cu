@@ -39,6 +39,9 @@
 namespace mbirgpu {
 
 int fail(const char *fmt, ...);
+int conv_tc_launch(const __nv_bfloat16 *in, int Kin, const __nv_bfloat16 *wt, __nv_bfloat16 *wtc, const float *bias,
+                   __nv_bfloat16 *out, int Nout, int d, int h, int w, int df, int relu, cudaStream_t st);
+int conv_tc_status(cudaStream_t st);
 
 namespace {
 
@@ -594,6 +597,9 @@ struct UNet {
     size_t head_w = 0, head_b = 0, n_params = 0;
     float *d_p = nullptr, *d_g = nullptr, *d_m = nullptr, *d_v = nullptr;
     bf16 *d_pb = nullptr, *d_wt = nullptr;  // BF16 copy; flipped weights scratch
+    bf16 *d_wtc = nullptr;                   // weights re-laid for the tcgen05 kernel
+    bool tensor_path = true;                 // tcgen05 convolutions where the shape allows
+    bool conv_err = false;                   // a tcgen05 launch failed
     long long steps = 0;
     float scale = 1.0f;  // input scale: the network sees scale x input
     cudaStream_t st = nullptr;
@@ -617,7 +623,7 @@ struct UNet {
         free_acts();
         for (auto &b : spare) cudaFree(b.second);
         for (void *p : {(void *)d_p, (void *)d_g, (void *)d_m, (void *)d_v, (void *)d_pb, (void *)d_wt,
-                        (void *)d_loss})
+                        (void *)d_wtc, (void *)d_loss})
             if (p) cudaFree(p);
     }
     // Activation blocks go back to a size-keyed pool instead of to the driver:
@@ -685,6 +691,7 @@ int UNet::init(int base, uint64_t seed)
     size_t wt = 0;
     for (auto &k : convs) wt = std::max(wt, (size_t)27 * k.cin * k.cout);
     if (e == cudaSuccess) e = cudaMalloc((void **)&d_wt, wt * sizeof(bf16));
+    if (e == cudaSuccess) e = cudaMalloc((void **)&d_wtc, wt * sizeof(bf16));
     if (e == cudaSuccess) e = cudaMalloc((void **)&d_loss, sizeof(double));
     if (e == cudaSuccess) e = cudaMemcpy(d_p, h.data(), n_params * sizeof(float), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemset(d_m, 0, n_params * sizeof(float));
@@ -768,6 +775,11 @@ void UNet::conv_tiles(const bf16 *in, int Kin, const float *bias, bf16 *o, int N
     const int d = D >> l, h = H >> l, w = W >> l, df = Df >> l;
     const unsigned tiles = (unsigned)(((d + FZ - 1) / FZ) * ((h + FY - 1) / FY) * ((w + FX - 1) / FX));
     const int r = relu ? 1 : 0;
+    if (tensor_path) {
+        const int done = conv_tc_launch(in, Kin, d_wt, d_wtc, bias, o, Nout, d, h, w, df, r, st);
+        if (done < 0) conv_err = true;
+        if (done) return;
+    }
     if (Kin == 1) {
         dim3 grid(tiles, (unsigned)((Nout + 15) / 16));
         conv_first_kernel<16><<<grid, kFThreads, 0, st>>>(in, d_wt, bias, o, Nout, d, h, w, r, df);
@@ -846,6 +858,10 @@ int UNet::forward(const float *d_in)
     }
     head_kernel<<<grid_for(vox(0)), 256, 0, st>>>(y, c, d_p + head_w, d_p + head_b, d_in, vox(0), 1.0f / scale, out);
     cudaError_t e = cudaGetLastError();
+    if (conv_err) {
+        conv_err = false;
+        return -1;
+    }
     return e == cudaSuccess ? 0 : fail("U-Net forward failed: %s", cudaGetErrorString(e));
 }
 
@@ -886,8 +902,14 @@ int UNet::backward(const float *d_target, double *loss)
         conv_back(ia, l > 0 ? pool[l - 1] : x0, act[l][0], gact[l][0], gx, l);
     }
     e = cudaGetLastError();
+    if (conv_err) {
+        conv_err = false;
+        return -1;
+    }
     if (e == cudaSuccess && loss) e = cudaMemcpyAsync(loss, d_loss, sizeof(double), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess && loss) e = cudaStreamSynchronize(st);
+    if (e == cudaSuccess && loss && tensor_path && conv_tc_status(st))
+        return fail("U-Net backward: a tensor-core convolution gave up waiting");
     return e == cudaSuccess ? 0 : fail("U-Net backward failed: %s", cudaGetErrorString(e));
 }
 
@@ -914,6 +936,8 @@ int unet_apply_frames(UNet *u, float *d_vol, int N_time, int N_z, int N_y, int N
         cudaError_t e = cudaMemcpyAsync(d_vol, u->out, N_time * frame * sizeof(float), cudaMemcpyDeviceToDevice,
                                         u->st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(u->st);
+        if (e == cudaSuccess && u->tensor_path && conv_tc_status(u->st))
+            return fail("U-Net inference: a tensor-core convolution gave up waiting");
         return e == cudaSuccess ? 0 : fail("U-Net inference failed: %s", cudaGetErrorString(e));
     }
     if (u->ensure(N_z, N_y, N_x)) return -1;
@@ -924,6 +948,8 @@ int unet_apply_frames(UNet *u, float *d_vol, int N_time, int N_z, int N_y, int N
         if (e != cudaSuccess) return fail("copy failed: %s", cudaGetErrorString(e));
     }
     cudaError_t e = cudaStreamSynchronize(u->st);
+    if (e == cudaSuccess && u->tensor_path && conv_tc_status(u->st))
+        return fail("U-Net inference: a tensor-core convolution gave up waiting");
     return e == cudaSuccess ? 0 : fail("U-Net inference failed: %s", cudaGetErrorString(e));
 }
 
@@ -1008,7 +1034,22 @@ int mbirgpu_unet_forward(mbirgpu_unet *up, const float *d_input, float *d_output
     cudaError_t e = cudaMemcpyAsync(d_output, u->out, (size_t)D * H * W * sizeof(float), cudaMemcpyDeviceToDevice,
                                     u->st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(u->st);
+    if (e == cudaSuccess && u->tensor_path && mbirgpu::conv_tc_status(u->st))
+        return fail("U-Net forward: a tensor-core convolution gave up waiting");
     return e == cudaSuccess ? 0 : fail("U-Net forward failed: %s", cudaGetErrorString(e));
+}
+
+int mbirgpu_unet_set_tensor_path(mbirgpu_unet *up, int32_t path)
+{
+    UNETP(up);
+    if (path != 0 && path != 1) return fail("tensor path must be 0 (mma.sync) or 1 (tcgen05)");
+    u->tensor_path = path == 1;
+    return 0;
+}
+
+int32_t mbirgpu_unet_get_tensor_path(const mbirgpu_unet *up)
+{
+    return up && reinterpret_cast<const UNet *>(up)->tensor_path ? 1 : 0;
 }
 
 int mbirgpu_unet_gradients(mbirgpu_unet *up, const float *d_input, const float *d_target, int32_t D, int32_t H,

@@ -34,6 +34,7 @@ EXPORTS = (
     "mbirgpu_unet_create", "mbirgpu_unet_destroy", "mbirgpu_unet_num_params", "mbirgpu_unet_set_input_scale",
     "mbirgpu_unet_get_input_scale", "mbirgpu_unet_get_params", "mbirgpu_unet_set_params", "mbirgpu_unet_forward",
     "mbirgpu_unet_gradients", "mbirgpu_unet_train_step", "mbirgpu_session_set_object_unet",
+    "mbirgpu_unet_set_tensor_path", "mbirgpu_unet_get_tensor_path",
     "mbirgpu_batch_create", "mbirgpu_batch_destroy", "mbirgpu_batch_run", "mbirgpu_batch_problem_info",
     "mbirgpu_batch_get_object", "mbirgpu_batch_cost", "mbirgpu_reconstruct_batch",
     "phcontomo_reconstruct", "mbirgpu_pc_default_options", "mbirgpu_pc_session_create", "mbirgpu_pc_session_destroy",

@@ -97,6 +97,28 @@ def run_unet(a):
     torch.cuda.synchronize()
     print(f"workload unet: {a.iters} training steps {1e3 * (t1 - t0) / max(a.iters, 1):.1f} ms/step, "
           f"inference {1e3 * (time.perf_counter() - t1):.1f} ms, loss {loss:.4g}")
+    # warm inference of one 32 x 256 x 256 frame on each tensor-core path
+    # (wall time around one synchronous call, median of 5)
+    C = [16, 32, 64, 128]
+    flops = 0.0  # the 3x3x3 convolutions: encoder two per level, decoder three per level
+    for l in range(4):
+        vox = x.numel() / 8 ** l
+        flops += 2 * 27 * vox * ((1 if l == 0 else C[l - 1]) * C[l] + C[l] * C[l])
+        if l < 3:
+            flops += 2 * 27 * vox * (C[l + 1] * C[l] + 2 * C[l] * C[l] + C[l] * C[l])
+    for path in (1, 0):
+        net.tensor_path = path
+        net.forward(x)
+        ts = []
+        for _ in range(5):
+            torch.cuda.synchronize()
+            t2 = time.perf_counter()
+            net.forward(x)
+            ts.append(time.perf_counter() - t2)
+        ms = 1e3 * sorted(ts)[2]
+        print(f"  inference, {'tcgen05' if path else 'mma.sync'} convolutions: {ms:.2f} ms per frame, "
+              f"{flops / ms / 1e9:.1f} TFLOP/s ({flops / 1e12:.3f} TFLOP)")
+    net.tensor_path = 1
 
 
 def run_pcsim(a):

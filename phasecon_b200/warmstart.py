@@ -39,6 +39,9 @@ def lib() -> C.CDLL:
         L.mbirgpu_unet_set_params.argtypes = [vp, vp]
         L.mbirgpu_unet_forward.argtypes = [vp, vp, vp, C.c_int32, C.c_int32, C.c_int32]
         L.mbirgpu_unet_gradients.argtypes = [vp, vp, vp, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_double), vp]
+        L.mbirgpu_unet_set_tensor_path.argtypes = [vp, C.c_int32]
+        L.mbirgpu_unet_get_tensor_path.argtypes = [vp]
+        L.mbirgpu_unet_get_tensor_path.restype = C.c_int32
         L.mbirgpu_unet_train_step.argtypes = [vp, vp, vp, C.c_int32, C.c_int32, C.c_int32, C.c_float,
                                               C.POINTER(C.c_double)]
         L.mbirgpu_session_set_object_unet.argtypes = [vp, vp]
@@ -87,6 +90,17 @@ class UNet:
     @input_scale.setter
     def input_scale(self, s: float) -> None:
         _check(lib().mbirgpu_unet_set_input_scale(self.h, s))
+
+    @property
+    def tensor_path(self) -> int:
+        """1: the 3x3x3 convolutions run on the tcgen05 kernels wherever the
+        channel counts are multiples of 16 (the default); 0: on the mma.sync
+        kernels everywhere."""
+        return int(lib().mbirgpu_unet_get_tensor_path(self.h))
+
+    @tensor_path.setter
+    def tensor_path(self, path: int) -> None:
+        _check(lib().mbirgpu_unet_set_tensor_path(self.h, int(path)))
 
     def save(self, path: str) -> None:
         np.savez_compressed(path, params=self.get_params(), base=self.c, scale=self.input_scale)

@@ -24,8 +24,12 @@ def _dev(x):
     return torch.from_numpy(np.ascontiguousarray(x, np.float32)).cuda()
 
 
-@pytest.mark.parametrize("c,shape", [(4, (8, 8, 8)), (8, (16, 16, 8))])
+@pytest.mark.parametrize("c,shape", [(4, (8, 8, 8)), (8, (16, 16, 8)), (16, (16, 24, 40))])
 def test_unet_gradients_match_fp64_oracle(c, shape):
+    """c = 4 and 8 run the mma.sync convolutions; c = 16 runs every 3x3x3
+    convolution but the first (one input channel) on the tcgen05 kernels,
+    forward and data gradient, on a grid whose y and x are not multiples of
+    the tile at any level."""
     rng = np.random.default_rng(c)
     net = WS.UNet(c, seed=3)
     net.input_scale = 50.0
@@ -118,10 +122,13 @@ def test_trained_warm_start_needs_fewer_iterations():
     assert c_net[0] < c_zero[0]
 
 
-def test_stacked_frame_inference_equals_per_frame():
+@pytest.mark.parametrize("c", [8, 16])
+def test_stacked_frame_inference_equals_per_frame(c):
     """The warm start runs the network on all frames of a 4-D problem in one
     stacked pass (zero padding per frame); every voxel must equal the
-    one-frame-at-a-time network output bit for bit (same tiles, same sums)."""
+    one-frame-at-a-time network output bit for bit (same tiles, same sums).
+    c = 16 runs the tcgen05 convolutions, whose TMA halo loads zero-fill per
+    frame."""
     import torch
     n, nz, frames = 32, 16, 3
     angles, times, rt = P.uniform_views(60)
@@ -133,9 +140,9 @@ def test_stacked_frame_inference_equals_per_frame():
     pb = _measure(pb, obj, 2e4, 0)
     s = pc.Session(pb)
     fbp = s.fbp()
-    net = WS.UNet(8, seed=2)
+    net = WS.UNet(c, seed=2)
     params = net.get_params()
-    params[-9:-1] = np.random.default_rng(0).normal(0, 0.3, 8)  # a head with weight: the network matters
+    params[-c - 1:-1] = np.random.default_rng(0).normal(0, 0.3, c)  # a head with weight: the network matters
     net.set_params(params)
     net.input_scale = 40.0
     WS.warm_start(s, net)
@@ -146,3 +153,32 @@ def test_stacked_frame_inference_equals_per_frame():
         exp = net.forward(torch.from_numpy(np.ascontiguousarray(fbp[f])).cuda()).cpu().numpy()
         np.testing.assert_array_equal(got[f][inside[f]], exp[inside[f]])
     s.close()
+
+
+@pytest.mark.parametrize("shape", [(16, 24, 40), (32, 64, 64)])
+def test_tensor_path_matches_mma_sync(shape):
+    """The tcgen05 convolutions (TMEM accumulators, TMA-staged halo and
+    weights) against the mma.sync kernels on the same BF16 weights and input:
+    both accumulate BF16 products in FP32, in different orders, and round each
+    layer's activations to BF16, so the networks' corrections agree to 1e-2
+    relative L2 (an occasional BF16 rounding flip per layer), and the
+    tcgen05 path is deterministic run to run."""
+    import torch
+    rng = np.random.default_rng(7)
+    net = WS.UNet(16, seed=5)
+    params = net.get_params()
+    params[-17:-1] = rng.normal(0, 0.3, 16)
+    net.set_params(params)
+    net.input_scale = 50.0
+    x = torch.from_numpy((0.01 + 0.01 * rng.random(shape)).astype(np.float32)).cuda()
+    assert net.tensor_path == 1
+    a = net.forward(x).cpu().numpy() - x.cpu().numpy()
+    a2 = net.forward(x).cpu().numpy() - x.cpu().numpy()
+    net.tensor_path = 0
+    b = net.forward(x).cpu().numpy() - x.cpu().numpy()
+    net.tensor_path = 1
+    np.testing.assert_array_equal(a, a2)
+    assert np.abs(b).max() > 0
+    rel = np.linalg.norm(a - b) / np.linalg.norm(b)
+    assert rel < 1e-2, rel
+
