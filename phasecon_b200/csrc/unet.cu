@@ -456,6 +456,24 @@ __global__ void upsample_kernel(const bf16 *__restrict__ in, int C, int d, int h
     }
 }
 
+// the same with 16-byte pieces (C a multiple of 8): thread i copies channels
+// 8 (i mod C/8) .. + 7 of output voxel i / (C/8)
+__global__ void upsample8_kernel(const bf16 *__restrict__ in, int C, int d, int h, int w, bf16 *__restrict__ out)
+{
+    const int H = 2 * h, W = 2 * w, P = C / 8;
+    const long long n = (long long)2 * d * H * W * P;
+    const uint4 *src = reinterpret_cast<const uint4 *>(in);
+    uint4 *dst = reinterpret_cast<uint4 *>(out);
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int p = (int)(i % P);
+        const long long v = i / P;
+        const int x = (int)(v % W);
+        const long long r = v / W;
+        const int y = (int)(r % H), z = (int)(r / H);
+        dst[i] = src[(((long long)(z >> 1) * h + (y >> 1)) * w + (x >> 1)) * P + p];
+    }
+}
+
 __global__ void upsample_grad_kernel(const bf16 *__restrict__ gout, int C, int d, int h, int w, bf16 *__restrict__ gin)
 {
     const int H = 2 * h, W = 2 * w;
@@ -482,6 +500,21 @@ __global__ void concat_kernel(const bf16 *__restrict__ a, int Ca, const bf16 *__
         const int c = (int)(i % C);
         const long long v = i / C;
         cat[i] = c < Ca ? a[v * Ca + c] : b[v * Cb + c - Ca];
+    }
+}
+
+// the same with 16-byte pieces (Ca, Cb multiples of 8)
+__global__ void concat8_kernel(const bf16 *__restrict__ a, int Ca, const bf16 *__restrict__ b, int Cb, long long V,
+                               bf16 *__restrict__ cat)
+{
+    const int Pa = Ca / 8, P = (Ca + Cb) / 8, Pb = P - Pa;
+    const long long n = V * P;
+    const uint4 *sa = reinterpret_cast<const uint4 *>(a), *sb = reinterpret_cast<const uint4 *>(b);
+    uint4 *dst = reinterpret_cast<uint4 *>(cat);
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int p = (int)(i % P);
+        const long long v = i / P;
+        dst[i] = p < Pa ? sa[v * Pa + p] : sb[v * Pb + p - Pa];
     }
 }
 
@@ -848,10 +881,18 @@ int UNet::forward(const float *d_in)
     }
     const bf16 *y = act[3][1];
     for (int l = 2; l >= 0; l--) {
-        upsample_kernel<<<grid_for(vox(l) * C[l + 1]), 256, 0, st>>>(y, C[l + 1], D >> (l + 1), H >> (l + 1),
-                                                                     W >> (l + 1), up[l]);
+        if (C[l + 1] % 8 == 0)
+            upsample8_kernel<<<grid_for(vox(l) * C[l + 1] / 8), 256, 0, st>>>(y, C[l + 1], D >> (l + 1),
+                                                                             H >> (l + 1), W >> (l + 1), up[l]);
+        else
+            upsample_kernel<<<grid_for(vox(l) * C[l + 1]), 256, 0, st>>>(y, C[l + 1], D >> (l + 1), H >> (l + 1),
+                                                                         W >> (l + 1), up[l]);
         conv(ci++, up[l], u[l], l, true);
-        concat_kernel<<<grid_for(vox(l) * 2 * C[l]), 256, 0, st>>>(u[l], C[l], act[l][1], C[l], vox(l), cat[l]);
+        if (C[l] % 8 == 0)
+            concat8_kernel<<<grid_for(vox(l) * 2 * C[l] / 8), 256, 0, st>>>(u[l], C[l], act[l][1], C[l], vox(l),
+                                                                           cat[l]);
+        else
+            concat_kernel<<<grid_for(vox(l) * 2 * C[l]), 256, 0, st>>>(u[l], C[l], act[l][1], C[l], vox(l), cat[l]);
         conv(ci++, cat[l], dec[l][0], l, true);
         conv(ci++, dec[l][0], dec[l][1], l, true);
         y = dec[l][1];

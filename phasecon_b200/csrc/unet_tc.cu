@@ -1,15 +1,15 @@
 // The U-Net's 3x3x3 convolutions on the fifth-generation tensor cores:
-// tcgen05.mma with the accumulators in tensor memory (TMEM), operands staged in
-// shared memory by the TMA engine.
+// tcgen05.mma with the accumulators in tensor memory (TMEM), operands in
+// shared memory.
 //
 //   out[v][n] = act(sum_{tap, k} in[v + off(tap)][k] wt[tap][n][k] + b[n])
 //
 // is an implicit GEMM with M = output voxels, N = output channels, K = 27 taps
 // x input channels. A CTA owns TZ x 16 x 8 output voxels (z, y, x) and NT
-// output channels. For each 16-channel chunk of the input, a TMA tile load
-// brings the (TZ+2) x 18 x 10 halo into shared memory as two 8-channel halves,
-// each [halo voxel][8 channels] (16 bytes a voxel, zero fill outside the
-// grid, which is the convolution's zero padding), and a bulk copy brings the
+// output channels. For each 16-channel chunk of the input, producer warps
+// stage the (TZ+2) x 18 x 10 halo in shared memory as two 8-channel halves,
+// each [halo voxel][8 channels] (16 bytes a voxel, zeros outside the grid,
+// which is the convolution's zero padding), and a TMA bulk copy brings the
 // chunk's weights. The halo needs no im2col: in the canonical K-major layout
 // without swizzle a tcgen05 operand is 8-row core matrices of 16-byte rows,
 // rows 16 bytes apart, core matrices SBO bytes apart along M and LBO bytes
@@ -21,25 +21,33 @@
 // ((zt + dz) * 18 + dy) * 10 + dx voxels: 27 x TZ MMAs (M = 128, N = NT,
 // K = 16) per chunk read the staged halo in place.
 //
-// Persistent, warp-specialised CTA (one per SM), 6 warps:
-//   warp 0 lane 0   TMA producer: per (tile, chunk) item, waits for a free
-//                   shared-memory stage, then issues two tensor tile loads
-//                   (the halo halves) and one bulk copy (the weights) that
-//                   complete on the stage's "full" mbarrier;
-//   warp 1 lane 0   MMA issuer: waits for a full stage and for a free TMEM
+// The halo is staged by threads rather than by a TMA tile load: a tile load
+// whose box rows are 16 bytes (8 channels of one voxel, the row of a core
+// matrix) moved about 8 bytes per cycle per SM, which bound the kernel; 128
+// producer threads with 16-byte loads fill the same tile an order of
+// magnitude faster and then make their shared-memory stores visible to the
+// tensor cores (fence.proxy.async) before arriving on the stage's mbarrier.
+//
+// Persistent, warp-specialised CTA (one per SM), 9 warps:
+//   warps 0-3       producers: per (tile, chunk) item, wait for a free stage;
+//                   thread 0 posts the weight bytes on the stage's "full"
+//                   mbarrier and issues their bulk copy; all 128 threads load
+//                   the halo (16-byte vectors, coalesced), store it, fence and
+//                   arrive;
+//   warps 4-7       epilogue: tcgen05.ld of the accumulator (warp w reads the
+//                   TMEM lanes of its quadrant w % 4 = output rows), bias,
+//                   ReLU, BF16, 32-byte stores; then free the accumulator;
+//   warp 8 lane 0   MMA issuer: waits for a full stage and for a free TMEM
 //                   accumulator, issues the tile's MMAs, and commits them to
 //                   the stage's "empty" mbarrier (the stage is reused once the
 //                   MMAs that read it are done) and, after a tile's last
-//                   chunk, to the accumulator's "full" mbarrier;
-//   warps 2-5       epilogue: tcgen05.ld of the accumulator (warp w reads the
-//                   TMEM lanes of its quadrant w % 4 = output rows), bias,
-//                   ReLU, BF16, 32-byte stores; then free the accumulator.
-// TMEM holds two accumulators (2 x TZ x NT FP32 columns), so the epilogue of
-// one tile overlaps the MMAs of the next. Every wait is bounded: a wait that
-// runs out records an error code that the host reads, and the CTA stops its
-// loops, waits (bounded) for its own MMAs, frees its TMEM and returns.
-#include <cuda.h>
-#include <cudaTypedefs.h>
+//                   chunk, to the accumulator's "full" mbarrier.
+// Every CTA serves one N slice (its weights never change) and walks tiles
+// with a stride of the CTAs per slice. TMEM holds two accumulators (2 x TZ x
+// NT FP32 columns), so the epilogue of one tile overlaps the MMAs of the
+// next. Every wait is bounded: a wait that runs out records an error code
+// that the host reads, and the CTA stops its loops, waits (bounded) for its
+// own MMAs, frees its TMEM and returns.
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -60,7 +68,10 @@ constexpr int TZ = 2, TYY = 16, TXX = 8;                      // output tile (z,
 constexpr int HZ = TZ + 2, HY = TYY + 2, HX = TXX + 2;        // halo 4 x 18 x 10
 constexpr int kHalo = HZ * HY * HX;                           // 720 voxels
 constexpr int kHalfBytes = kHalo * 16;                        // one 8-channel half: 11,520 bytes
-constexpr int kThreads = 192;                                 // producer, MMA, 4 epilogue warps
+constexpr int kProducers = 128;                               // warps 0-3
+constexpr int kThreads = 288;                                 // producers, 4 epilogue warps, MMA warp
+constexpr int kHaloItems = 2 * kHalo;                         // 16-byte halo pieces per chunk
+constexpr int kPerProducer = (kHaloItems + kProducers - 1) / kProducers;  // 12
 constexpr long long kWaitCycles = 4000000000LL;               // about 2 s at the boost clock
 
 __device__ int g_conv_tc_error = 0;
@@ -88,11 +99,6 @@ __device__ __forceinline__ void mbar_arrive(uint32_t bar)
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 
-__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-}
-
 __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity)
 {
     uint32_t ok;
@@ -108,10 +114,11 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity)
 
 // Bounded wait for the phase with the given parity. Returns false (and
 // records `code`) when it runs out or when another role of the CTA gave up.
-__device__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int *abort, int code)
+__device__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int *abort, int code, unsigned sleep_ns = 0)
 {
     const long long t0 = clock64();
     while (!mbar_try_wait(bar, parity)) {
+        if (sleep_ns) __nanosleep(sleep_ns);  // leave the issue slots to the warps doing work
         if (*abort) return false;
         if (clock64() - t0 > kWaitCycles) {
             *abort = 1;
@@ -122,14 +129,9 @@ __device__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int *abort, in
     return true;
 }
 
-__device__ __forceinline__ void tma_load_5d(uint32_t dst, const CUtensorMap *map, int c0, int c1, int c2, int c3,
-                                            int c4, uint32_t bar)
+__device__ __forceinline__ void mbar_expect_tx_only(uint32_t bar, uint32_t bytes)
 {
-    asm volatile(
-        "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
-        "%5, %6}], [%7];" ::"r"(dst),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(bar)
-        : "memory");
+    asm volatile("mbarrier.expect_tx.relaxed.cta.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
 }
 
 __device__ __forceinline__ void bulk_load(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar)
@@ -172,29 +174,31 @@ __device__ __forceinline__ void mma_commit(uint32_t bar)
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16])
+// 16 FP32 columns of this warp's 32 TMEM lanes into v[0..15]. The load and
+// its wait are one asm statement, so no instruction can read the destination
+// registers before the asynchronous load has written them.
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v)
 {
     uint32_t r[16];
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-        "%15}, [%16];"
+        "%15}, [%16];\n\t"
+        "tcgen05.wait::ld.sync.aligned;"
         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
           "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-        : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        : "r"(taddr)
+        : "memory");
 #pragma unroll
     for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
 }
 
 struct Grid {
     int d, h, w, df;         // stacked depth, height, width, frame depth
-    int tiles_x, tiles_y, tiles_z, nsplit, nchunks, units;
+    int tiles_x, tiles_y, tiles, nsplit, nchunks;
 };
 
-__device__ __forceinline__ void unit_coords(const Grid &g, int u, int &ns, int &x0, int &y0, int &z0)
+__device__ __forceinline__ void tile_coords(const Grid &g, int t, int &x0, int &y0, int &z0)
 {
-    ns = u % g.nsplit;
-    int t = u / g.nsplit;
     x0 = (t % g.tiles_x) * TXX;
     t /= g.tiles_x;
     y0 = (t % g.tiles_y) * TYY;
@@ -203,7 +207,7 @@ __device__ __forceinline__ void unit_coords(const Grid &g, int u, int &ns, int &
 
 template <int NT>
 __global__ void __launch_bounds__(kThreads, 1)
-    conv_tc_kernel(const __grid_constant__ CUtensorMap halo_map, const bf16 *__restrict__ wtc,
+    conv_tc_kernel(const bf16 *__restrict__ in, int Kin, const bf16 *__restrict__ wtc,
                    const float *__restrict__ bias, bf16 *__restrict__ out, int Nout, Grid g, int relu)
 {
     using C = Cfg<NT>;
@@ -212,12 +216,16 @@ __global__ void __launch_bounds__(kThreads, 1)
     __shared__ __align__(8) uint64_t bar_acc_full[2], bar_acc_empty[2], bar_done;
     __shared__ uint32_t tmem_base_s;
     __shared__ int abort_s;
+    __shared__ float bias_s[NT];
     const uint32_t base = (smem_u32(smem_raw) + 1023u) & ~1023u;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    // this CTA's N slice and its tiles: tile = slot, slot + stride, ...
+    const int ns = blockIdx.x % g.nsplit, slot = blockIdx.x / g.nsplit, stride = gridDim.x / g.nsplit;
+    const int n0 = ns * NT;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < C::kStages; s++) {
-            mbar_init(smem_u32(&bar_full[s]), 1);
+            mbar_init(smem_u32(&bar_full[s]), kProducers);
             mbar_init(smem_u32(&bar_empty[s]), 1);
         }
         for (int a = 0; a < 2; a++) {
@@ -227,8 +235,8 @@ __global__ void __launch_bounds__(kThreads, 1)
         mbar_init(smem_u32(&bar_done), 1);
         abort_s = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&halo_map)) : "memory");
     }
+    if (threadIdx.x < NT) bias_s[threadIdx.x] = bias ? bias[n0 + threadIdx.x] : 0.0f;
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_s)),
                      "r"(C::kTmemCols)
@@ -241,93 +249,94 @@ __global__ void __launch_bounds__(kThreads, 1)
     const uint32_t tmem = tmem_base_s;
     volatile int *abort = &abort_s;
 
-    if (threadIdx.x == 0) {
-        // ---- TMA producer ----
+    if (warp < 4) {
+        // ---- producers: halo by 128 threads, weights by one bulk copy ----
         int it = 0;
-        for (int u = blockIdx.x; u < g.units && !*abort; u += gridDim.x) {
-            int ns, x0, y0, z0;
-            unit_coords(g, u, ns, x0, y0, z0);
-            const int f = z0 / g.df, zl = z0 - f * g.df;
+        const int tid = threadIdx.x;
+        for (int t = slot; t < g.tiles && !*abort; t += stride) {
+            int x0, y0, z0;
+            tile_coords(g, t, x0, y0, z0);
+            const int zf0 = (z0 / g.df) * g.df, zf1 = zf0 + g.df;  // this tile's frame
+            bool ok = true;
             for (int c = 0; c < g.nchunks; c++, it++) {
                 const int s = it % C::kStages;
                 const uint32_t ph = (uint32_t)(it / C::kStages) & 1u;
-                if (!mbar_wait(smem_u32(&bar_empty[s]), ph ^ 1u, abort, 1)) break;
+                int wok = 0;
+                if (lane == 0) wok = mbar_wait(smem_u32(&bar_empty[s]), ph ^ 1u, abort, 1, 64) ? 1 : 0;
+                if (!__shfl_sync(0xffffffffu, wok, 0)) {
+                    ok = false;
+                    break;
+                }
                 const uint32_t st = base + (uint32_t)s * C::kStage, fb = smem_u32(&bar_full[s]);
-                mbar_expect_tx(fb, (uint32_t)C::kStage);
-                tma_load_5d(st, &halo_map, c * 16, x0 - 1, y0 - 1, zl - 1, f, fb);
-                tma_load_5d(st + kHalfBytes, &halo_map, c * 16 + 8, x0 - 1, y0 - 1, zl - 1, f, fb);
-                bulk_load(st + 2 * kHalfBytes, wtc + ((size_t)ns * g.nchunks + c) * (C::kWBytes / 2),
-                          (uint32_t)C::kWBytes, fb);
-            }
-        }
-    } else if (threadIdx.x == 32) {
-        // ---- MMA issuer ----
-        constexpr uint32_t idesc = idesc_bf16(NT);
-        int it = 0, ut = 0;
-        bool ok = true;
-        for (int u = blockIdx.x; u < g.units && ok; u += gridDim.x, ut++) {
-            const int a = ut & 1;
-            const uint32_t aph = (uint32_t)(ut >> 1) & 1u;
-            if (!(ok = mbar_wait(smem_u32(&bar_acc_empty[a]), aph ^ 1u, abort, 2))) break;
-            tc_fence_after();
-            const uint32_t d0 = tmem + (uint32_t)(a * C::kAcc);
-            for (int c = 0; c < g.nchunks; c++, it++) {
-                const int s = it % C::kStages;
-                const uint32_t ph = (uint32_t)(it / C::kStages) & 1u;
-                if (!(ok = mbar_wait(smem_u32(&bar_full[s]), ph, abort, 3))) break;
-                tc_fence_after();
-                const uint32_t st = base + (uint32_t)s * C::kStage, wb = st + 2 * kHalfBytes;
-#pragma unroll 1
-                for (int tap = 0; tap < 27; tap++) {
-                    const int dz = tap / 9, dy = (tap / 3) % 3, dx = tap % 3;
-                    const uint64_t bdesc = sdesc(wb + (uint32_t)tap * (NT * 32), 128, 256);
+                if (tid == 0) {
+                    mbar_expect_tx_only(fb, (uint32_t)C::kWBytes);
+                    bulk_load(st + 2 * kHalfBytes, wtc + ((size_t)ns * g.nchunks + c) * (C::kWBytes / 2),
+                              (uint32_t)C::kWBytes, fb);
+                }
+                uint4 v[kPerProducer];
 #pragma unroll
-                    for (int zt = 0; zt < TZ; zt++) {
-                        const uint32_t aoff = (uint32_t)((((zt + dz) * HY + dy) * HX + dx) * 16);
-                        const uint64_t adesc = sdesc(st + aoff, kHalfBytes, HX * 16);
-                        mma_bf16_ss(d0 + (uint32_t)(zt * NT), adesc, bdesc, idesc, (c > 0 || tap > 0) ? 1u : 0u);
+                for (int r = 0; r < kPerProducer; r++) {
+                    const int e = tid + r * kProducers;  // piece e: halo voxel e / 2, channel half e % 2
+                    v[r] = make_uint4(0u, 0u, 0u, 0u);
+                    if (e < kHaloItems) {
+                        const int hv = e >> 1, hz = hv / (HY * HX), rr = hv - hz * (HY * HX), hy = rr / HX,
+                                  hx = rr - hy * HX;
+                        const int z = z0 + hz - 1, y = y0 + hy - 1, x = x0 + hx - 1;
+                        if (z >= zf0 && z < zf1 && z < g.d && y >= 0 && y < g.h && x >= 0 && x < g.w)
+                            v[r] = __ldg(reinterpret_cast<const uint4 *>(
+                                in + (((long long)z * g.h + y) * g.w + x) * Kin + c * 16 + (e & 1) * 8));
                     }
                 }
-                mma_commit(smem_u32(&bar_empty[s]));
+#pragma unroll
+                for (int r = 0; r < kPerProducer; r++) {
+                    const int e = tid + r * kProducers;
+                    if (e < kHaloItems) {
+                        const uint32_t dst = st + (uint32_t)((e & 1) * kHalfBytes + (e >> 1) * 16);
+                        asm volatile("st.shared.v4.u32 [%0], {%1, %2, %3, %4};" ::"r"(dst), "r"(v[r].x),
+                                     "r"(v[r].y), "r"(v[r].z), "r"(v[r].w)
+                                     : "memory");
+                    }
+                }
+                // the stores are read by the tensor cores (async proxy)
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                mbar_arrive(fb);
             }
-            if (ok) mma_commit(smem_u32(&bar_acc_full[a]));
+            if (!ok) break;
         }
-        // all MMAs issued by this thread are complete before TMEM is released
-        mma_commit(smem_u32(&bar_done));
-        const long long t0 = clock64();
-        while (!mbar_try_wait(smem_u32(&bar_done), 0u) && clock64() - t0 < kWaitCycles) {
-        }
-    } else if (warp >= 2) {
+    } else if (warp < 8) {
         // ---- epilogue ----
         const int q = warp & 3;             // TMEM lane quadrant = output rows 32q .. 32q + 31
         const int m = q * 32 + lane;        // row of the M = 128 tile
         const int yl = m >> 3, xl = m & 7;
         int ut = 0;
-        for (int u = blockIdx.x; u < g.units; u += gridDim.x, ut++) {
+        for (int t = slot; t < g.tiles; t += stride, ut++) {
             const int a = ut & 1;
             const uint32_t aph = (uint32_t)(ut >> 1) & 1u;
             // lane 0 waits and tells the warp, so the warp stays converged for
             // the warp-wide tcgen05.ld whatever the wait's outcome
-            bool ok = false;
-            if (lane == 0) ok = mbar_wait(smem_u32(&bar_acc_full[a]), aph, abort, 4);
-            if (!__shfl_sync(0xffffffffu, ok ? 1 : 0, 0)) break;
+            int wok = 0;
+            if (lane == 0) wok = mbar_wait(smem_u32(&bar_acc_full[a]), aph, abort, 4, 64) ? 1 : 0;
+            if (!__shfl_sync(0xffffffffu, wok, 0)) break;
             tc_fence_after();
-            int ns, x0, y0, z0;
-            unit_coords(g, u, ns, x0, y0, z0);
-            const int zl = z0 % g.df, y = y0 + yl, x = x0 + xl, n0 = ns * NT;
+            int x0, y0, z0;
+            tile_coords(g, t, x0, y0, z0);
+            const int zl = z0 % g.df, y = y0 + yl, x = x0 + xl;
 #pragma unroll
             for (int zt = 0; zt < TZ; zt++) {
-                const bool inside = zl + zt < g.df && y < g.h && x < g.w;
+                const bool inside = zl + zt < g.df && z0 + zt < g.d && y < g.h && x < g.w;
                 const long long v = (((long long)(z0 + zt) * g.h + y) * g.w + x);
+                float acc[NT];
 #pragma unroll
-                for (int j = 0; j < NT / 16; j++) {
-                    float acc[16];
-                    tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(a * C::kAcc + zt * NT + j * 16), acc);
-                    if (inside) {
+                for (int j = 0; j < NT / 16; j++)
+                    tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(a * C::kAcc + zt * NT + j * 16),
+                              acc + j * 16);
+                if (inside) {
+#pragma unroll
+                    for (int j = 0; j < NT / 16; j++) {
                         alignas(16) bf16 o[16];
 #pragma unroll
                         for (int i = 0; i < 16; i++) {
-                            float val = acc[i] + (bias ? __ldg(bias + n0 + j * 16 + i) : 0.0f);
+                            float val = acc[j * 16 + i] + bias_s[j * 16 + i];
                             if (relu) val = fmaxf(val, 0.0f);
                             o[i] = __float2bfloat16(val);
                         }
@@ -340,6 +349,47 @@ __global__ void __launch_bounds__(kThreads, 1)
             tc_fence_before();
             __syncwarp();
             if (lane == 0) mbar_arrive(smem_u32(&bar_acc_empty[a]));
+        }
+    } else if (lane == 0) {
+        // ---- MMA issuer ----
+        constexpr uint32_t idesc = idesc_bf16(NT);
+        int it = 0, ut = 0;
+        bool ok = true;
+        for (int t = slot; t < g.tiles && ok; t += stride, ut++) {
+            const int a = ut & 1;
+            const uint32_t aph = (uint32_t)(ut >> 1) & 1u;
+            if (!(ok = mbar_wait(smem_u32(&bar_acc_empty[a]), aph ^ 1u, abort, 2))) break;
+            tc_fence_after();
+            const uint32_t d0 = tmem + (uint32_t)(a * C::kAcc);
+            for (int c = 0; c < g.nchunks; c++, it++) {
+                const int s = it % C::kStages;
+                const uint32_t ph = (uint32_t)(it / C::kStages) & 1u;
+                if (!(ok = mbar_wait(smem_u32(&bar_full[s]), ph, abort, 3))) break;
+                tc_fence_after();
+                const uint32_t st = base + (uint32_t)s * C::kStage;
+                // descriptors of tap 0; a tap moves the start address (16-byte
+                // units in the low bits, which cannot carry: the stage lies
+                // below 256 KB) by a compile-time offset
+                const uint64_t a0 = sdesc(st, kHalfBytes, HX * 16);
+                const uint64_t b0 = sdesc(st + 2 * kHalfBytes, 128, 256);
+#pragma unroll
+                for (int tap = 0; tap < 27; tap++) {
+                    const int dz = tap / 9, dy = (tap / 3) % 3, dx = tap % 3;
+#pragma unroll
+                    for (int zt = 0; zt < TZ; zt++) {
+                        const uint32_t aoff = (uint32_t)((((zt + dz) * HY + dy) * HX + dx) * 16);
+                        mma_bf16_ss(d0 + (uint32_t)(zt * NT), a0 + (aoff >> 4), b0 + (uint32_t)(tap * NT * 2), idesc,
+                                    (c > 0 || tap > 0) ? 1u : 0u);
+                    }
+                }
+                mma_commit(smem_u32(&bar_empty[s]));
+            }
+            if (ok) mma_commit(smem_u32(&bar_acc_full[a]));
+        }
+        // all MMAs issued by this thread are complete before TMEM is released
+        mma_commit(smem_u32(&bar_done));
+        const long long t0 = clock64();
+        while (!mbar_try_wait(smem_u32(&bar_done), 0u) && clock64() - t0 < kWaitCycles) {
         }
     }
     tc_fence_before();
@@ -373,20 +423,6 @@ __global__ void tc_weights_kernel(const bf16 *__restrict__ wt, int Kin, int Nout
     }
 }
 
-PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
-{
-    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-    if (!fn) {
-        void *p = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
-                cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-    }
-    return fn;
-}
-
 int sm_count()
 {
     static int n = 0;
@@ -400,7 +436,7 @@ int sm_count()
 }
 
 template <int NT>
-int launch(const CUtensorMap &map, const bf16 *wtc, const float *bias, bf16 *out, int Nout, const Grid &g, int relu,
+int launch(const bf16 *in, int Kin, const bf16 *wtc, const float *bias, bf16 *out, int Nout, const Grid &g, int relu,
            cudaStream_t st)
 {
     static bool attr = false;
@@ -410,8 +446,10 @@ int launch(const CUtensorMap &map, const bf16 *wtc, const float *bias, bf16 *out
             return fail("tensor-core convolution: shared-memory attribute refused");
         attr = true;
     }
-    const unsigned grid = (unsigned)std::max(1, std::min(g.units, sm_count()));
-    conv_tc_kernel<NT><<<grid, kThreads, Cfg<NT>::kSmem, st>>>(map, wtc, bias, out, Nout, g, relu);
+    // CTAs per N slice: one per SM in all, at most one per tile
+    const int per_slice = std::max(1, std::min(g.tiles, sm_count() / g.nsplit));
+    conv_tc_kernel<NT><<<(unsigned)(per_slice * g.nsplit), kThreads, Cfg<NT>::kSmem, st>>>(in, Kin, wtc, bias, out,
+                                                                                          Nout, g, relu);
     const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? 1 : fail("tensor-core convolution launch failed: %s", cudaGetErrorString(e));
 }
@@ -436,8 +474,6 @@ int conv_tc_launch(const __nv_bfloat16 *in, int Kin, const __nv_bfloat16 *wt, __
 {
     const int NT = conv_tc_split(Kin, Nout);
     if (!NT || (d != df && df % TZ) || d % df) return 0;
-    PFN_cuTensorMapEncodeTiled_v12000 encode = encode_fn();
-    if (!encode) return 0;
     Grid g;
     g.d = d;
     g.h = h;
@@ -445,29 +481,18 @@ int conv_tc_launch(const __nv_bfloat16 *in, int Kin, const __nv_bfloat16 *wt, __
     g.df = df;
     g.tiles_x = (w + TXX - 1) / TXX;
     g.tiles_y = (h + TYY - 1) / TYY;
-    g.tiles_z = (d + TZ - 1) / TZ;
+    const long long tiles = (long long)g.tiles_x * g.tiles_y * ((d + TZ - 1) / TZ);
+    if (tiles > (1LL << 30)) return 0;
+    g.tiles = (int)tiles;
     g.nsplit = Nout / NT;
     g.nchunks = Kin / 16;
-    const long long units = (long long)g.tiles_x * g.tiles_y * g.tiles_z * g.nsplit;
-    if (units > (1LL << 30)) return 0;
-    g.units = (int)units;
     tc_weights_kernel<<<(unsigned)std::min<long long>((27LL * Nout * Kin + 255) / 256, 4096), 256, 0, st>>>(wt, Kin,
                                                                                                            Nout, NT,
                                                                                                            wtc);
-    CUtensorMap map;
-    const cuuint64_t dims[5] = {(cuuint64_t)Kin, (cuuint64_t)w, (cuuint64_t)h, (cuuint64_t)df, (cuuint64_t)(d / df)};
-    const cuuint64_t strides[4] = {(cuuint64_t)Kin * 2, (cuuint64_t)w * Kin * 2, (cuuint64_t)h * w * Kin * 2,
-                                   (cuuint64_t)df * h * w * Kin * 2};
-    const cuuint32_t box[5] = {8, HX, HY, HZ, 1};
-    const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
-    const CUresult r = encode(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<__nv_bfloat16 *>(in), dims,
-                              strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (r != CUDA_SUCCESS) return fail("tensor-core convolution: tensor map encoding failed (%d)", (int)r);
     switch (NT) {
-    case 64: return launch<64>(map, wtc, bias, out, Nout, g, relu, st);
-    case 32: return launch<32>(map, wtc, bias, out, Nout, g, relu, st);
-    default: return launch<16>(map, wtc, bias, out, Nout, g, relu, st);
+    case 64: return launch<64>(in, Kin, wtc, bias, out, Nout, g, relu, st);
+    case 32: return launch<32>(in, Kin, wtc, bias, out, Nout, g, relu, st);
+    default: return launch<16>(in, Kin, wtc, bias, out, Nout, g, relu, st);
     }
 }
 
