@@ -497,21 +497,22 @@ def run_warmstart(args, world, rank, local, pg):
     res = {}
     # every start runs once untimed first (device allocations of the FBP and of
     # the network's stacked inference grid, module loading), then timed
-    for name in ("zero", "fbp", "unet") * 2:
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        if name == "zero":
-            s.set_object(np.zeros(s.shape, np.float32))
-        elif name == "fbp":
-            s.set_object_fbp()
-        else:
-            WS.warm_start(s, net)
-        torch.cuda.synchronize()
-        t_init = time.perf_counter() - t0
-        it, costs = WS.iterations_to_cost(s, target, max_iter=400)
-        torch.cuda.synchronize()
-        res[name] = {"time_to_converged_cost_s": time.perf_counter() - t0, "init_s": t_init, "iterations": it,
-                     "initial_cost": costs[0], "final_cost": costs[-1]}
+    with ClockSampler(local) as clk:
+        for name in ("zero", "fbp", "unet") * 2:
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            if name == "zero":
+                s.set_object(np.zeros(s.shape, np.float32))
+            elif name == "fbp":
+                s.set_object_fbp()
+            else:
+                WS.warm_start(s, net)
+            torch.cuda.synchronize()
+            t_init = time.perf_counter() - t0
+            it, costs = WS.iterations_to_cost(s, target, max_iter=400)
+            torch.cuda.synchronize()
+            res[name] = {"time_to_converged_cost_s": time.perf_counter() - t0, "init_s": t_init, "iterations": it,
+                         "initial_cost": costs[0], "final_cost": costs[-1]}
     s.close()
     if rank == 0:
         tz, tu = res["zero"]["time_to_converged_cost_s"], res["unet"]["time_to_converged_cost_s"]
@@ -528,7 +529,8 @@ def run_warmstart(args, world, rank, local, pg):
             "speedup_vs_zero_init": tz / tu if tu else None,
             "speedup_vs_fbp_init": res["fbp"]["time_to_converged_cost_s"] / tu if tu else None,
             "target_cost": target, "starts": res, "train_data_s": t_data, "train_s": t_train,
-            "train_loss_first_last": [float(np.mean(hist[:20])), float(np.mean(hist[-20:]))]}))
+            "train_loss_first_last": [float(np.mean(hist[:20])), float(np.mean(hist[-20:]))],
+            "clocks": clk.summary()}))
 
 
 def main():
