@@ -158,8 +158,8 @@ def converge(session: Session, max_iter: int = 200, rel: float = 1e-4, start_ite
 
 
 def iterations_to_cost(session: Session, target: float, max_iter: int = 300):
-    """Plain ICD iterations until the FP64 cost is at most `target` (the
-    north star's "reaches the plain method's converged cost"); returns
+    """Plain ICD iterations until the FP64 cost is at most `target` (for a
+    warm start: the plain method's converged cost times 1 + 1e-4); returns
     (iterations, cost history) or (None, history) if it never does."""
     costs = [session.cost()[0]]
     if costs[0] <= target:
