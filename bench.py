@@ -58,8 +58,7 @@ def parse():
     ap.add_argument("--max-converge-iters", type=int, default=400)
     ap.add_argument("--schedule", default="",
                     help="4-D workload: fix the sweep schedule as SV,WARPS,COLORS (super-voxel edge, warps per "
-                         "column, K of the K x K colouring) instead of autotuning it, e.g. for a profiler run whose "
-                         "serialised timings would mislead the autotuner")
+                         "column, K of the K x K colouring) instead of the library's shape rule")
     ap.add_argument("--workload", default="4d", choices=["4d", "batch", "warmstart"],
                     help="4d: the 4-D benchmark (default); batch: 48 uneven 3-D problems, batched vs sequential; "
                          "warmstart: the learned warm start on the 4-D workload")
@@ -209,21 +208,44 @@ def cpu_sample_problem(seed: int = 0):
     return pb
 
 
+def reference_parallelism(threads: int, n_time: int, n_z: int) -> int:
+    """Voxel-line updates the reference runs at once: its OpenMP loops go over
+    (frame, every other z block) with num_z_blocks = threads / N_time, at least
+    2, at most N_z, rounded down to even (MBIR_4D/XT_Init.c:379-384,
+    XT_ICD_update.c:964-1046)."""
+    nzb = threads // n_time
+    nzb = 2 if nzb < 2 else min(nzb, n_z)
+    nzb = (nzb // 2) * 2
+    return min(threads, n_time * nzb // 2)
+
+
 def reference_rate(pb, warmup: int, steps: int):
-    """Reference C (single stage, all host threads): voxel-updates/s over
-    `steps` ICD iterations after `warmup`, from two runs (warmup and
-    warmup+steps iterations) so set-up time cancels."""
+    """Reference C as it ships (the build with -DNO_COST_CALCULATE -DNO_DEBUG of
+    MBIR_4D/Makefile:3: no cost pass, no cost-increase abort), single stage,
+    all host threads: voxel-updates/s over `steps` ICD iterations after
+    `warmup`, from two runs (warmup and warmup+steps iterations) so set-up time
+    cancels."""
     import oracle as O
     threads = os.cpu_count() or 1
     t0 = time.perf_counter()
-    _, c1, u1 = O.ref_reconstruct(pb, tempfile.mkdtemp(), max_iter=max(warmup, 1), num_stages=1, threads=threads)
+    _, _, u1 = O.ref_reconstruct(pb, tempfile.mkdtemp(), max_iter=max(warmup, 1), num_stages=1, threads=threads,
+                                 timing=True)
     t1 = time.perf_counter()
-    _, c2, u2 = O.ref_reconstruct(pb, tempfile.mkdtemp(), max_iter=max(warmup, 1) + steps, num_stages=1,
-                                  threads=threads)
+    _, _, u2 = O.ref_reconstruct(pb, tempfile.mkdtemp(), max_iter=max(warmup, 1) + steps, num_stages=1,
+                                 threads=threads, timing=True)
     t2 = time.perf_counter()
     dt = (t2 - t1) - (t1 - t0)
     upd = u2 - u1
     return upd / dt if dt > 0 else float("nan"), dt, upd, threads
+
+
+def reference_sample_text(threads: int, steps: int, warmup: int, upd: int, dt: float) -> str:
+    busy = reference_parallelism(threads, 8, SAMPLE_ROWS)
+    return (f"reference C MBIR_4D built from source as it ships (-DNO_COST_CALCULATE -DNO_DEBUG), single stage, "
+            f"{SAMPLE_ROWS} of 32 detector rows of the same 4-D workload, {steps} ICD iterations after {warmup} "
+            f"(two runs, set-up cancelled; {upd} voxel updates, {dt:.1f} s); {threads} OpenMP threads, of which the "
+            f"reference keeps {busy} busy: it runs (frame, z block) items with num_z_blocks = threads / frames "
+            f"(XT_Init.c:379-384), the same on the full 32-row workload")
 
 
 def run_reference_arm(args, rank):
@@ -231,18 +253,18 @@ def run_reference_arm(args, rank):
         return
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
-    if not oracle.ref_available():
-        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref_mbir4d.so was not built"}))
+    if not oracle.ref_available(timing=True):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref_mbir4d_timing.so was not built"}))
         return
     pb = cpu_sample_problem()
     rate, dt, upd, threads = reference_rate(pb, args.warmup, args.steps)
-    sample = (f"reference C MBIR_4D (built from source), single stage, {SAMPLE_ROWS} of 32 detector rows of the "
-              f"4-D workload, {args.steps} ICD iterations after {args.warmup} (two runs, set-up cancelled)")
+    sample = reference_sample_text(threads, args.steps, args.warmup, upd, dt)
     line = {"metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * dt / max(args.steps, 1), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64/f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "sample_rows": SAMPLE_ROWS}, "impl": "reference",
-            "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference", "sample": sample},
+            "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference", "sample": sample,
+                             "busy_threads": reference_parallelism(threads, 8, SAMPLE_ROWS)},
             "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "voxel_updates": upd}
     print(json.dumps(line))
@@ -371,12 +393,12 @@ def run_ours(args, world, rank, local, pg):
         try:
             sys.path.insert(0, os.path.join(ROOT, "oracle"))
             import oracle
-            if oracle.ref_available():
+            if oracle.ref_available(timing=True):
                 spb = cpu_sample_problem()
                 rate, dt, upd, threads = reference_rate(spb, 1, 2)
                 cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference",
-                       "sample": f"reference C MBIR_4D built from source, {SAMPLE_ROWS} of 32 detector rows of the "
-                                 f"same 4-D workload, 2 ICD iterations after 1 ({upd} voxel updates, {dt:.1f} s)"}
+                       "busy_threads": reference_parallelism(threads, 8, SAMPLE_ROWS),
+                       "sample": reference_sample_text(threads, 2, 1, upd, dt)}
             else:
                 cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
                        "sample": "oracle/_ref not built on this host"}

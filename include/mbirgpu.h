@@ -58,8 +58,8 @@ typedef struct {
     int32_t write_files;     /* reference side-effect files, default 1 */
     int32_t compute_cost;    /* FP64 MAP cost every iteration (cost.bin), default 1 */
     int32_t refresh_every;   /* FP64 recomputation of e = y - Ax every n iterations, default 8 */
-    int32_t sv_size;         /* super-voxel edge in voxel columns; 0 = autotuned */
-    int32_t cta_warps;       /* warps cooperating on one voxel column; 0 = autotuned */
+    int32_t sv_size;         /* super-voxel edge in voxel columns; 0 = by rule or autotuned */
+    int32_t cta_warps;       /* warps cooperating on one voxel column; 0 = by rule or autotuned */
     int32_t icd_unroll;      /* views whose A records and sinogram entries one lane keeps in flight
                                 (1, 2 or 4); 0 = autotuned */
     uint64_t seed;           /* voxel-order seed */
@@ -71,7 +71,7 @@ typedef struct {
                                 NHICD_Iterations, XT_Init.c:406; NO_NHICD is 0) */
     int32_t sv_colors;       /* super-voxel colouring: K x K colour classes, K = 2 (4 phases per
                                 sweep) or 4 (16 phases: same-colour super-voxels twice as far
-                                apart); 0 = autotuned */
+                                apart); 0 = by rule or autotuned */
     int32_t stage_records;   /* 1 (default): the ICD sweep copies each next voxel column's A
                                 records into shared memory while it updates the current one;
                                 0: records are read from global memory where they are used */
@@ -80,6 +80,12 @@ typedef struct {
     int32_t nh_cta_warps;    /* warps cooperating on one voxel column in those passes; 0 = autotuned */
     int32_t nh_work_lists;   /* 1 (default): those passes visit only super-voxels holding selected
                                 columns, the ones with the most first; 0: every super-voxel */
+    int32_t autotune;        /* 0 (default): the schedule fields left at 0 follow a fixed rule of
+                                the problem's shape (super-voxels 4 x 4, K = 2, 4 warps per column
+                                when a frame has >= 64 views, else 2), so the same inputs give the
+                                same schedule and the same image on every run; 1: a single
+                                session measures the candidate schedules on its own problem and
+                                keeps the fastest (timing-dependent); batches always measure */
 } mbirgpu_options;
 
 /* Defaults as listed above. */
@@ -225,8 +231,10 @@ int mbirgpu_session_nh_select(mbirgpu_session *s, const float *mag, uint8_t *sel
  * and sino_dev [N_p][N_r][N_t] are device pointers, and the FP64 scratch is
  * a fixed 16 MiB array in the library (N_p * N_r * N_t <= 2,097,152, larger
  * sessions are rejected). Enqueued on the session's stream, not waited for.
- * Make the first call on each device before any stream capture (it looks the
- * scratch up). The call clears the scratch it uses itself. The scratch is
+ * Runs on the session's device whichever device is current (the caller's
+ * current device is restored). Make the first call on each device before any
+ * stream capture (it looks the scratch up; later calls outside capture look
+ * it up again). The call clears the scratch it uses itself. The scratch is
  * shared by every call on a device: calls in flight at the same time on one
  * device race, so order them. */
 int mbirgpu_session_forward_project_noalloc(mbirgpu_session *s, const float *object_dev, float *sino_dev);

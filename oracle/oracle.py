@@ -100,18 +100,27 @@ class Problem:
                           mult_xy, mult_z)
 
 
+def reference_root() -> str | None:
+    """The phasecon checkout the reference builds read (environment variable
+    PHASECON_REFERENCE_ROOT), or None when it is unset or holds no sources."""
+    root = os.environ.get("PHASECON_REFERENCE_ROOT", "")
+    return root if root and os.path.isdir(os.path.join(root, "Source_Code", "MBIR_4D")) else None
+
+
 def build(with_reference: bool | None = None) -> None:
-    """Build the oracle libraries (the reference only where its sources exist)."""
+    """Build the oracle libraries; the reference builds only where its sources
+    are reachable (PHASECON_REFERENCE_ROOT), else the prebuilt ones under
+    _ref/ are kept as they are."""
     subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
     if with_reference is None:
-        with_reference = os.path.isdir("/root/reference/Source_Code/MBIR_4D")
+        with_reference = reference_root() is not None
     if with_reference:
         subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
         subprocess.run(["make", "-s", "-C", HERE, "ref_pc"], check=True)
 
 
 _orc = None
-_ref = None
+_ref = {}
 
 
 def orc_lib() -> C.CDLL:
@@ -145,14 +154,21 @@ def orc_lib() -> C.CDLL:
     return _orc
 
 
-def ref_available() -> bool:
-    return os.path.exists(os.path.join(REF_DIR, "libref_mbir4d.so"))
+def _ref_name(timing: bool) -> str:
+    return "libref_mbir4d_timing.so" if timing else "libref_mbir4d.so"
 
 
-def ref_lib() -> C.CDLL:
-    global _ref
-    if _ref is None:
-        lib = C.CDLL(os.path.join(REF_DIR, "libref_mbir4d.so"))
+def ref_available(timing: bool = False) -> bool:
+    return os.path.exists(os.path.join(REF_DIR, _ref_name(timing)))
+
+
+def ref_lib(timing: bool = False) -> C.CDLL:
+    """The reference MBIR_4D built from source: the cost-on build (cost.bin per
+    iteration, the "Cost value increased" abort of XT_ICD_update.c:1171), or
+    with timing=True the build with the reference Makefile's own
+    -DNO_COST_CALCULATE -DNO_DEBUG (MBIR_4D/Makefile:3), which has neither."""
+    if timing not in _ref:
+        lib = C.CDLL(os.path.join(REF_DIR, _ref_name(timing)))
         P = C.POINTER(RefProblem)
         lib.ref_set_options.argtypes = [C.c_double, C.c_int, C.c_int]
         lib.ref_geometry.argtypes = [P, _f64p, _f64p, _f32p, _f32p, _i32p, _i32p]
@@ -169,8 +185,8 @@ def ref_lib() -> C.CDLL:
         lib.ref_reconstruct.restype = C.c_int
         lib.ref_free.argtypes = [C.c_void_p]
         lib.ref_vox_updates.restype = C.c_longlong
-        _ref = lib
-    return _ref
+        _ref[timing] = lib
+    return _ref[timing]
 
 
 # --------------------------------------------------------------------------- restatement
@@ -387,14 +403,15 @@ def ref_variance_update(pb: Problem, err: np.ndarray, w: np.ndarray, var_est: fl
 
 
 def ref_reconstruct(pb: Problem, workdir: str, max_iter: int = 1000, num_stages: int = 0, threads: int = 0,
-                    remove_rings: int = 0):
+                    remove_rings: int = 0, timing: bool = False):
     """Run the reference's ``reconstruct`` in ``workdir`` (remove_rings: its
-    ring-correction mode, 0 = off).
+    ring-correction mode, 0 = off; timing: the build without the cost pass).
 
     Returns (object with halo [N_time][N_z+2][N_y][N_x] as the reference
-    returns it, FP64 cost per iteration from cost.bin, voxel updates counted).
+    returns it, FP64 cost per iteration from cost.bin -- None for the timing
+    build, which writes none -- and the voxel updates counted).
     """
-    lib = ref_lib()
+    lib = ref_lib(timing)
     lib.ref_set_options(pb.mrf_p, max_iter, num_stages)
     lib.ref_reset_vox_updates()
     s = pb.ref_struct()
@@ -412,8 +429,25 @@ def ref_reconstruct(pb: Problem, workdir: str, max_iter: int = 1000, num_stages:
     obj = np.ctypeslib.as_array(out, shape=(n,)).copy().reshape(pb.recon_num, pb.proj_rows + 2, pb.proj_cols,
                                                                   pb.proj_cols)
     lib.ref_free(out)
-    cost = np.fromfile(os.path.join(workdir, "cost.bin"), dtype=np.float64)
+    cpath = os.path.join(workdir, "cost.bin")
+    cost = None if timing else np.fromfile(cpath, dtype=np.float64)
     return obj, cost, int(lib.ref_vox_updates())
+
+
+def ref_reconstruct_and_cost(pb: Problem, workdir: str, max_iter: int, num_stages: int = 1, threads: int = 0):
+    """The reference's ``reconstruct`` as it ships (the build without the cost
+    pass, so no rounding-level cost increase can abort it) for max_iter
+    iterations, then the reference's own MAP cost (computeCost,
+    XT_ICD_update.c:185-318) of the object it returned, evaluated on a fresh
+    error sinogram (initErrorSinogam) by the cost-on build.
+
+    Returns (object without halo [N_time][N_z][N_y][N_x], that cost, voxel
+    updates)."""
+    obj, _, upd = ref_reconstruct(pb, workdir, max_iter=max_iter, num_stages=num_stages, threads=threads,
+                                  timing=True)
+    x = np.ascontiguousarray(obj[:, 1:-1])
+    _, _, cost = ref_error_sino_and_cost(pb, x)
+    return x, cost, upd
 
 
 # --------------------------------------------------------------------------- PCMBIR reference (built from source)

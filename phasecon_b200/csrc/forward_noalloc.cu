@@ -13,8 +13,16 @@
 // * the scratch holds kNoallocMaxSinoEntries doubles (16 MiB), so a session
 //   qualifies when N_p * N_r * N_t is at most that (180 views x 128 columns x
 //   16 rows is 368,640); larger sessions are rejected with an error;
-// * the first call on a device looks the scratch up with that device current
-//   (cudaGetSymbolAddress); make that first call before any stream capture;
+// * the call runs on the device the session was created on: it makes that
+//   device current for its duration and restores the caller's current
+//   device before it returns, so a caller that has another GPU current still
+//   gets this session's scratch, table and stream;
+// * the scratch's device address is looked up (cudaGetSymbolAddress, with
+//   the session's device current) on the first call on a device, and looked
+//   up again on every later call whose stream is not capturing, so a module
+//   reloaded after cudaDeviceReset is picked up; a call whose stream is
+//   capturing uses the address found by an earlier call on that device and
+//   fails if there was none: make the first call before any stream capture;
 // * the scratch must be zero where the projection accumulates; every call
 //   clears the part it uses on the session's stream before the projection
 //   kernel runs, so callers do nothing for it; the output is fully written;
@@ -72,23 +80,73 @@ __global__ void round_accumulator_kernel(size_t n, const double *__restrict__ ac
         out[i] = (float)acc[i];
 }
 
-// Address of this device's scratch, looked up once per device.
-int scratch_for_current_device(double **out)
+// Address of device dev's scratch (dev is current). Looked up whenever the
+// stream is not capturing -- the module behind the symbol may have been
+// reloaded (cudaDeviceReset) since the last call -- and taken from the cache
+// of the last lookup while it is.
+int scratch_for_device(int dev, cudaStream_t stream, double **out)
 {
-    int dev = -1;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return fail("cudaGetDevice failed: %s", cudaGetErrorString(e));
     if (dev < 0 || dev >= kMaxDevices) return fail("device %d is beyond the %d devices supported", dev, kMaxDevices);
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaError_t e = cudaStreamIsCapturing(stream, &cs);
+    if (e != cudaSuccess) return fail("cudaStreamIsCapturing failed: %s", cudaGetErrorString(e));
     std::lock_guard<std::mutex> lock(g_scratch_mu);
-    if (!g_scratch_ptr[dev]) {
+    if (cs == cudaStreamCaptureStatusNone) {
         void *p = nullptr;
         e = cudaGetSymbolAddress(&p, g_noalloc_acc);
         if (e != cudaSuccess)
             return fail("cudaGetSymbolAddress of the projection scratch failed on device %d: %s", dev,
                         cudaGetErrorString(e));
         g_scratch_ptr[dev] = static_cast<double *>(p);
+    } else if (!g_scratch_ptr[dev]) {
+        return fail("forward_project_noalloc: the first call on device %d was made while its stream was capturing; "
+                    "make one call before capturing so the scratch address is known",
+                    dev);
     }
     *out = g_scratch_ptr[dev];
+    return 0;
+}
+
+// Makes the session's device current for one call and restores the
+// caller's device afterwards.
+struct DeviceScope {
+    int prev = -1;
+    bool switched = false;
+    int enter(int dev)
+    {
+        cudaError_t e = cudaGetDevice(&prev);
+        if (e != cudaSuccess) return fail("cudaGetDevice failed: %s", cudaGetErrorString(e));
+        if (prev != dev) {
+            e = cudaSetDevice(dev);
+            if (e != cudaSuccess) return fail("cudaSetDevice(%d) failed: %s", dev, cudaGetErrorString(e));
+            switched = true;
+        }
+        return 0;
+    }
+    ~DeviceScope()
+    {
+        if (switched) cudaSetDevice(prev);
+    }
+};
+
+int forward_project_noalloc(Session *s, const float *object_dev, float *sino_dev)
+{
+    const Geom &g = s->hs.g;
+    const size_t n = (size_t)g.N_p * g.N_r * g.N_t;
+    if (n > kNoallocMaxSinoEntries)
+        return fail("forward_project_noalloc: the sinogram has %zu entries (%d views x %d columns x %d rows); "
+                    "the fixed scratch holds at most %zu",
+                    n, g.N_p, g.N_r, g.N_t, kNoallocMaxSinoEntries);
+    double *acc = nullptr;
+    if (scratch_for_device(s->device, s->st, &acc)) return -1;
+    cudaError_t e = cudaMemsetAsync(acc, 0, n * sizeof(double), s->st);
+    if (e != cudaSuccess) return fail("clearing the projection scratch failed: %s", cudaGetErrorString(e));
+    const long long warps = (long long)g.N_time * g.N_x * g.N_y;
+    const long long blocks = (warps * 32 + 255) / 256;
+    forward_project_vol_kernel<<<(unsigned)blocks, 256, 0, s->st>>>(g, s->d_table, s->d_view_first, object_dev, acc);
+    round_accumulator_kernel<<<148 * 8, 256, 0, s->st>>>(n, acc, sino_dev);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return fail("forward_project_noalloc launch failed: %s", cudaGetErrorString(e));
     return 0;
 }
 
@@ -102,21 +160,7 @@ extern "C" int mbirgpu_session_forward_project_noalloc(mbirgpu_session *sp, cons
     if (!sp) return fail("session pointer is NULL");
     if (!object_dev || !sino_dev) return fail("NULL argument");
     Session *s = reinterpret_cast<Session *>(sp);
-    const Geom &g = s->hs.g;
-    const size_t n = (size_t)g.N_p * g.N_r * g.N_t;
-    if (n > kNoallocMaxSinoEntries)
-        return fail("forward_project_noalloc: the sinogram has %zu entries (%d views x %d columns x %d rows); "
-                    "the fixed scratch holds at most %zu",
-                    n, g.N_p, g.N_r, g.N_t, kNoallocMaxSinoEntries);
-    double *acc = nullptr;
-    if (scratch_for_current_device(&acc)) return -1;
-    cudaError_t e = cudaMemsetAsync(acc, 0, n * sizeof(double), s->st);
-    if (e != cudaSuccess) return fail("clearing the projection scratch failed: %s", cudaGetErrorString(e));
-    const long long warps = (long long)g.N_time * g.N_x * g.N_y;
-    const long long blocks = (warps * 32 + 255) / 256;
-    forward_project_vol_kernel<<<(unsigned)blocks, 256, 0, s->st>>>(g, s->d_table, s->d_view_first, object_dev, acc);
-    round_accumulator_kernel<<<148 * 8, 256, 0, s->st>>>(n, acc, sino_dev);
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return fail("forward_project_noalloc launch failed: %s", cudaGetErrorString(e));
-    return 0;
+    DeviceScope scope;
+    if (scope.enter(s->device)) return -1;
+    return forward_project_noalloc(s, object_dev, sino_dev);
 }

@@ -117,15 +117,11 @@ __device__ __forceinline__ void stage_records(uint32_t *dst, const uint32_t *src
                  : "memory");
 }
 
-// Every thread waits for buffer b's copy: the n-th copy into a buffer
-// completes the mbarrier's phase n, so the parity of the wait is the count of
-// earlier waits on that buffer (bit b of `phases`, identical in every thread).
-// The wait is bounded (about 2 s); a copy that never lands is counted and the
-// host reports it.
-__device__ __forceinline__ void wait_staged(unsigned long long *bar, uint32_t &phases, int b, unsigned &timeouts)
+// Bounded wait (about 2 s of clock64) for phase `parity` of mbarrier `bar`;
+// returns false if it ran out.
+__device__ __forceinline__ bool wait_parity_bounded(unsigned long long *bar, uint32_t parity)
 {
     const unsigned a = (unsigned)__cvta_generic_to_shared(bar);
-    const uint32_t parity = (phases >> b) & 1u;
     const long long t0 = clock64();
     for (;;) {
         uint32_t ok;
@@ -136,11 +132,27 @@ __device__ __forceinline__ void wait_staged(unsigned long long *bar, uint32_t &p
             : "=r"(ok)
             : "r"(a), "r"(parity)
             : "memory");
-        if (ok) break;
-        if (clock64() - t0 > 4000000000LL) {
-            timeouts++;
-            break;
-        }
+        if (ok) return true;
+        if (clock64() - t0 > 4000000000LL) return false;
+    }
+}
+
+// Every thread waits for buffer b's copy: the n-th copy into a buffer
+// completes the mbarrier's phase n, so the parity of the wait is the count of
+// earlier waits on that buffer (bit b of `phases`, identical in every thread).
+// The wait is bounded; a copy that never lands is counted (the host turns the
+// count into an error) and raises the CTA's abort flag: the caller stops
+// updating and staging after the next barrier, and the kernel waits for the
+// late copy once more before it exits (abort_bar / abort_parity).
+__device__ __forceinline__ void wait_staged(unsigned long long *bar, uint32_t &phases, int b, unsigned &timeouts,
+                                            int &abort, int &abort_bar, uint32_t &abort_parity)
+{
+    const uint32_t parity = (phases >> b) & 1u;
+    if (!wait_parity_bounded(bar, parity)) {
+        timeouts++;
+        abort = 1;  // every writer stores the same values
+        abort_bar = b;
+        abort_parity = parity;
     }
     phases ^= 1u << b;
 }
@@ -188,6 +200,9 @@ struct IcdSmem {
     float dx[32];
     int order[kMaxSvCols];
     int ncols, item;
+    int abort;              // a record copy did not land in time: stop updating
+    int abort_bar;          // the buffer whose copy was late, and the wait's parity
+    uint32_t abort_parity;
 };
 
 struct IcdCount {
@@ -349,8 +364,12 @@ __device__ __forceinline__ void icd_update_sv(const Geom &g, const IcdLaunch &L,
             // neighbour (in-column neighbours are the column's own values)
             active_pred = !L.zero_skipping || L.iter <= 1 || (zl && V != 0.0f) || pos;
         }
-        if (kStaged) wait_staged(&S.stage_bar[ci & 1], cnt.phases, ci & 1, cnt.timeouts);  // issued one column earlier
+        if (kStaged)  // issued one column earlier
+            wait_staged(&S.stage_bar[ci & 1], cnt.phases, ci & 1, cnt.timeouts, S.abort, S.abort_bar, S.abort_parity);
         const int any_active = __syncthreads_or(active_pred);
+        // a late copy leaves this column's records undefined: no update, no
+        // further copies (S.abort is read after the barrier, so uniformly)
+        if (kStaged && S.abort) return;
         // every thread is past the previous column's apply pass: its record
         // buffer may be refilled with the next column's
         if (kStaged && ci + 1 < ncols)
@@ -554,6 +573,7 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 4) icd_phase_kernel(
     const int hx = (L.n_sv_x + KC - 1) / KC, slots = hx * ((L.n_sv_y + KC - 1) / KC);
     const int n_items = L.items ? *L.n_items : g.N_time * slots;
     IcdCount cnt{};
+    if (threadIdx.x == 0) S.abort = 0;
     if (kStaged && threadIdx.x == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"((unsigned)__cvta_generic_to_shared(&S.stage_bar[0]))
                      : "memory");
@@ -563,6 +583,7 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 4) icd_phase_kernel(
     }
     for (;;) {
         __syncthreads();  // S.item / S.order of the previous SV are no longer read
+        if (kStaged && S.abort) break;  // uniform: written before the barrier
         if (threadIdx.x == 0) S.item = (int)atomicAdd(queue, 1u);
         __syncthreads();
         const int item = S.item;
@@ -584,6 +605,9 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 4) icd_phase_kernel(
         icd_update_sv<KW, kUnroll, VEC, kStaged>(g, L, K, table, view_first, mask, x, err, wgt, mag, f, sx, sy, S,
                                                  cnt, s_rec, stage_words);
     }
+    // after an abort, the late copy may still write into this CTA's shared
+    // memory: give it one more bounded wait before the CTA exits
+    if (kStaged && S.abort && threadIdx.x == 0) wait_parity_bounded(&S.stage_bar[S.abort_bar], S.abort_parity);
     flush_counts(cnt, stats);
 }
 

@@ -79,6 +79,7 @@ int Session::init(const mbirgpu_problem *pb, const mbirgpu_options *o, int mult_
 {
     opt = o ? *o : current_options();
     st = (cudaStream_t)stream;
+    CK(cudaGetDevice(&device));
     ProblemDesc pd{};
     pd.proj_rows = pb->proj_rows;
     pd.proj_cols = pb->proj_cols;
@@ -189,7 +190,21 @@ int Session::init(const mbirgpu_problem *pb, const mbirgpu_options *o, int mult_
     if (refresh_error()) return -1;
     return autotune();
 }
-// Schedule autotuner. Candidates: (super-voxel edge sv, colours K) in
+// Default schedule, a function of the problem's shape only (autotune = 0):
+// 4 x 4 super-voxels in K = 2 colours (the 4-D workload's measured best,
+// and the concurrency cap sv_max_concurrent keeps it convergent on any
+// frame size), 4 warps per column when a frame has at least 64 views to
+// split over them, else 2. Fields the user fixed are kept.
+void Session::choose_schedule()
+{
+    const Geom &g = hs.g;
+    sv = opt.sv_size > 0 ? std::min(opt.sv_size, 16) : 4;
+    colors = opt.sv_colors > 0 ? opt.sv_colors : 2;
+    warps = opt.cta_warps > 0 ? std::min(opt.cta_warps, 8) : (g.max_views >= 64 ? 4 : 2);
+    sync_nh_schedule();
+}
+
+// Schedule autotuner (opt-in, autotune = 1). Candidates: (super-voxel edge sv, colours K) in
 // {(4, 2), (4, 4), (8, 2), (8, 4), (16, 2)} and warps per CTA in {2, 4}, each
 // with its grid capped at sv_max_concurrent CTAs. Each candidate runs one
 // iteration as the run will (the second one when non-homogeneous passes are
@@ -197,17 +212,9 @@ int Session::init(const mbirgpu_problem *pb, const mbirgpu_options *o, int mult_
 // its time is scaled by the relative number of iterations its same-colour
 // spacing needs to converge (sv_convergence_factor). The smallest estimated
 // time to convergence wins. User-fixed sv_size / cta_warps / sv_colors
-// restrict the search; with all three fixed there is none.
-void Session::choose_schedule()
-{
-    const Geom &g = hs.g;
-    int ntp = 4;
-    while (ntp < g.N_t) ntp <<= 1;
-    sv = opt.sv_size > 0 ? std::min(opt.sv_size, 16) : 8;
-    colors = opt.sv_colors > 0 ? opt.sv_colors : 2;
-    warps = opt.cta_warps > 0 ? std::min(opt.cta_warps, 8) : std::max(2, std::min(8, g.max_views / (16 * (32 / ntp))));
-    sync_nh_schedule();
-}
+// restrict the search; with all three fixed there is none. The result
+// depends on measured times, so two runs on the same inputs can pick
+// different schedules and end on (equally converged) different images.
 
 // Schedule of the non-homogeneous passes: the user's, else the full sweep's
 // super-voxels and colours with twice its warps per column (up to 8). Those
@@ -224,6 +231,7 @@ void Session::sync_nh_schedule()
 
 int Session::autotune()
 {
+    if (!opt.autotune) return 0;
     if (opt.sv_size > 0 && opt.cta_warps > 0 && opt.sv_colors > 0) return 0;
     const Geom &g = hs.g;
     // snapshot x and e into the scratch buffers (d_tmp holds a volume, d_acc a sinogram)
@@ -656,6 +664,7 @@ void mbirgpu_default_options(mbirgpu_options *o)
     o->nh_sv_colors = 0;
     o->nh_cta_warps = 0;
     o->nh_work_lists = 1;
+    o->autotune = 0;
 }
 
 int mbirgpu_set_options(const mbirgpu_options *o)
@@ -673,6 +682,7 @@ int mbirgpu_set_options(const mbirgpu_options *o)
     if (o->nh_sv_colors != 0 && o->nh_sv_colors != 2 && o->nh_sv_colors != 4)
         return fail("nh_sv_colors must be 0 (auto), 2 or 4");
     if (o->nh_cta_warps < 0 || o->nh_cta_warps > 8) return fail("nh_cta_warps must be 0 (auto) or 1..8");
+    if (o->autotune != 0 && o->autotune != 1) return fail("autotune must be 0 (schedule by rule) or 1 (measured)");
     mbirgpu_options cur = mbirgpu::current_options();
     (void)cur;
     std::lock_guard<std::mutex> lk(mbirgpu::g_opt_mu);

@@ -15,6 +15,7 @@ struct Session {
     HostSetup hs;
     mbirgpu_options opt{};
     cudaStream_t st = nullptr;
+    int device = 0;  // the CUDA device that was current when the session was created
     float convg_thresh = 0;
     size_t n_sino = 0, n_vox = 0, device_bytes = 0;
     int n_assigned = 0;  // views that belong to some frame

@@ -3,7 +3,7 @@
 Run in a container that has the phasecon sources (the reference C is built from
 them by ``make -C oracle ref``):
 
-    python tests/golden/gen_golden.py [/path/to/phasecon]
+    PHASECON_REFERENCE_ROOT=/path/to/phasecon python tests/golden/gen_golden.py
 
 Every array saved here is an OUTPUT OF THE REFERENCE C code, built from source
 with a single-rank MPI shim (oracle/Makefile), or a vector shipped with the
@@ -102,4 +102,7 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PHASECON_REFERENCE_ROOT", "")
+    if not root:
+        sys.exit("set PHASECON_REFERENCE_ROOT (or pass the path) to the phasecon checkout")
+    main(root)

@@ -1,0 +1,139 @@
+"""Parity at the benchmark configurations: the CUDA path (through the C ABI)
+against the reference C run here on the same inputs.
+
+The reference is the MBIR_4D library built from its own sources as it ships
+(oracle/_ref/libref_mbir4d_timing.so: -DNO_COST_CALCULATE -DNO_DEBUG, so a
+rounding-level cost increase cannot abort it); its MAP cost is the
+reference's own computeCost (MBIR_4D/XT_ICD_update.c:185-318) of the object
+it returns.
+
+Tolerances (the method's, since the voxel update order differs): converged
+MAP cost within 1e-4 relative, image RMSE within 0.5 % of the reference
+image's dynamic range.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+import phasecon_b200 as pc
+from phasecon_b200 import phantoms as P
+from problems import to_gpu_problem
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not (O.ref_available() and O.ref_available(timing=True)),
+                                 reason="reference build not present")]
+
+THREADS = os.cpu_count() or 1
+
+
+def _rmse_frac(x, xr):
+    return float(np.sqrt(np.mean((x.astype(np.float64) - xr) ** 2)) / (xr.max() - xr.min()))
+
+
+def config1_problem(seed: int = 0):
+    """The 3-D configuration: a 10-ellipsoid Shepp-Logan-type phantom
+    (attenuation 0-0.02 /mm) on 128 x 128 x 16 voxels at 1 mm, 180 parallel-beam
+    views over 180 deg, a 128 x 16 detector, y = -log(N / 1e4), w = N with
+    N ~ Poisson(1e4 exp(-Ax)) (A applied by the oracle's restatement of the
+    reference projector), qGGMRF p = 1.1, q = 2, T = 1 (c_s = 1), sigma_x = 0.01."""
+    views, n, nz = 180, 128, 16
+    angles, times, rt = P.uniform_views(views)
+    obj = P.ellipsoid_phantom(n, nz, seed)[None]
+    pb = O.Problem(np.zeros((views, nz, n), np.float32), np.ones((views, nz, n), np.float32), angles, times, rt, nz,
+                   n, views, 1, rot_center=n / 2, sig_s=0.01, sig_t=1.0, c_s=1.0, c_t=1.0, mrf_p=1.1,
+                   convg_thresh=0.0)
+    ax = O.Oracle(pb).forward(obj)
+    y, w = P.poisson_measurements(ax, 1e4, seed)
+    pb.projections = np.ascontiguousarray(y.transpose(0, 2, 1))
+    pb.weights = np.ascontiguousarray(w.transpose(0, 2, 1))
+    return pb
+
+
+def test_config1_shepp_logan_dropin_matches_reference(tmp_path):
+    """20 ICD iterations from zero, one stage, through reconstruct() on both
+    sides. The reference's own run has settled to 1e-9 relative by then."""
+    pb = config1_problem()
+    ref_x, ref_cost, ref_upd = O.ref_reconstruct_and_cost(pb, str(tmp_path / "ref"), 20, num_stages=1,
+                                                          threads=THREADS)
+    args = (pb.projections, pb.weights, pb.proj_angles, pb.proj_times, pb.recon_times, pb.proj_rows,
+            pb.proj_cols, pb.proj_num, pb.recon_num, pb.vox_wid, pb.rot_center, pb.sig_s, pb.sig_t, pb.c_s,
+            pb.c_t)
+    cwd = os.getcwd()
+    os.makedirs(tmp_path / "gpu")
+    os.chdir(tmp_path / "gpu")
+    saved = pc.get_options()
+    try:
+        pc.set_options(mrf_p=1.1, max_iterations=20, num_stages=1, cost_rel_tol=0.0)
+        out = pc.reconstruct(*args, convg_thresh=0.0, remove_rings=0, quad_convex=1)
+        cost = np.fromfile("cost.bin", np.float64)
+    finally:
+        os.chdir(cwd)
+        import ctypes
+        pc.lib().mbirgpu_set_options(ctypes.byref(saved))
+    assert len(cost) == 21  # the cost before iteration 1 and after each of the 20
+    x = out[:, 1:-1]
+    assert abs(cost[-1] - ref_cost) / ref_cost < 1e-4, (cost[-3:], ref_cost)
+    assert _rmse_frac(x, ref_x) <= 0.005
+    # the oracle (FP64 restatement) agrees with the GPU's FP64 cost of its own state
+    orc = O.Oracle(pb)
+    x = np.ascontiguousarray(x)
+    c_orc = orc.cost(orc.error_sino(x), x)[0]
+    assert abs(cost[-1] - c_orc) / c_orc < 1e-6
+
+
+def test_config2_4d_sample_converges_to_reference(tmp_path):
+    """The 4-D Cahn-Hilliard workload (8 frames, 1,024 interlaced views, 256
+    detector columns, p = 1.2) restricted to its first 4 detector rows / voxel
+    slices -- the sample the benchmark's CPU baseline times. The reference runs
+    15 iterations from zero (its cost settles to 1e-9 relative by iteration 12);
+    the GPU runs plain SV-ICD from zero to a relative cost change below 1e-7."""
+    import bench
+    pb = bench.cpu_sample_problem()
+    ref_x, ref_cost, _ = O.ref_reconstruct_and_cost(pb, str(tmp_path / "ref"), 15, num_stages=1, threads=THREADS)
+    o = pc.get_options()
+    o.mrf_p = 1.2
+    s = pc.Session(to_gpu_problem(pb), options=o)
+    costs = [s.cost()[0]]
+    for it in range(1, 61):
+        s.icd_iteration(it)
+        costs.append(s.cost()[0])
+        if it > 2 and abs(costs[-2] - costs[-1]) < 1e-7 * costs[-1]:
+            break
+    x = s.get_object()
+    s.close()
+    assert abs(costs[-1] - ref_cost) / ref_cost < 1e-4, (costs[-3:], ref_cost)
+    assert _rmse_frac(x, ref_x) <= 0.005
+
+
+def test_schedule_is_a_function_of_the_shape_and_results_repeat(tmp_path):
+    """With the default options (no timing-based autotuning) two reconstruct()
+    calls on the same inputs pick the same schedule and end on the same image
+    and cost, up to the order of the FP32 atomic error-sinogram updates."""
+    pb = config1_problem(seed=3)
+    args = (pb.projections, pb.weights, pb.proj_angles, pb.proj_times, pb.recon_times, pb.proj_rows,
+            pb.proj_cols, pb.proj_num, pb.recon_num, pb.vox_wid, pb.rot_center, pb.sig_s, pb.sig_t, pb.c_s,
+            pb.c_t)
+    cwd = os.getcwd()
+    saved = pc.get_options()
+    outs, costs = [], []
+    try:
+        pc.set_options(mrf_p=1.1, max_iterations=8, cost_rel_tol=0.0)
+        for i in range(2):
+            os.makedirs(tmp_path / f"r{i}")
+            os.chdir(tmp_path / f"r{i}")
+            outs.append(pc.reconstruct(*args, convg_thresh=0.0, remove_rings=0, quad_convex=1))
+            costs.append(np.fromfile("cost.bin", np.float64))
+            os.chdir(cwd)
+        o = pc.get_options()
+        o.mrf_p = 1.1
+        infos = [pc.Session(to_gpu_problem(pb), options=o).info for _ in range(2)]
+    finally:
+        os.chdir(cwd)
+        import ctypes
+        pc.lib().mbirgpu_set_options(ctypes.byref(saved))
+    assert [(i.sv_size, i.cta_warps, i.sv_colors) for i in infos] == [(4, 4, 2)] * 2
+    a, b = outs
+    assert np.abs(a - b).max() <= 1e-4 * (a.max() - a.min())
+    assert np.allclose(costs[0], costs[1], rtol=1e-6, atol=0)

@@ -166,9 +166,15 @@ def test_error_sinogram_drift_is_bounded():
     assert np.abs(e_run - e_exact).max() <= 1e-4 * np.abs(e_exact).max()
 
 
-@pytest.mark.skipif(not O.ref_available(), reason="reference build not present")
+@pytest.mark.skipif(not (O.ref_available() and O.ref_available(timing=True)), reason="reference build not present")
 def test_reconstruct_dropin_matches_reference(tmp_path):
+    """reconstruct() through the C ABI against the reference's reconstruct()
+    (multi-resolution plan, both stopping on the reference's own test
+    100 sum|dx| / sum|x| < 0.005): final cost within 1e-4, image RMSE within
+    0.5 % of the range. The reference is the build as it ships (no cost pass);
+    its cost is its own computeCost of the object it returns."""
     pb, _ = make_problem(ncol=128, nrow=8, nview=90, nframe=1, seed=4)
+    pb.convg_thresh = 0.005
     args = (pb.projections, pb.weights, pb.proj_angles, pb.proj_times, pb.recon_times, pb.proj_rows,
             pb.proj_cols, pb.proj_num, pb.recon_num, pb.vox_wid, pb.rot_center, pb.sig_s, pb.sig_t, pb.c_s,
             pb.c_t)
@@ -176,8 +182,8 @@ def test_reconstruct_dropin_matches_reference(tmp_path):
     os.chdir(tmp_path)
     saved = pc.get_options()
     try:
-        pc.set_options(mrf_p=pb.mrf_p, max_iterations=60, cost_rel_tol=0.0)
-        out = pc.reconstruct(*args, convg_thresh=0.05, remove_rings=0, quad_convex=1)
+        pc.set_options(mrf_p=pb.mrf_p, max_iterations=200, cost_rel_tol=0.0)
+        out = pc.reconstruct(*args, convg_thresh=pb.convg_thresh, remove_rings=0, quad_convex=1)
         cost = np.fromfile("cost.bin", np.float64)
         assert os.path.exists("object_time_0.bin") and os.path.exists("status.bin")
     finally:
@@ -186,18 +192,19 @@ def test_reconstruct_dropin_matches_reference(tmp_path):
         pc.lib().mbirgpu_set_options(ctypes.byref(saved))
     assert out.shape == (1, pb.proj_rows + 2, pb.proj_cols, pb.proj_cols)
     assert np.all(out[:, 0] == 0) and np.all(out[:, -1] == 0)
-    pb.convg_thresh = 0.05
-    ref_obj, ref_cost, _ = O.ref_reconstruct(pb, str(tmp_path / "ref"), max_iter=60)
-    x, xr = out[:, 1:-1], ref_obj[:, 1:-1]
+    xr, ref_cost, _ = O.ref_reconstruct_and_cost(pb, str(tmp_path / "ref"), 200, num_stages=0,
+                                                 threads=os.cpu_count() or 1)
+    x = out[:, 1:-1]
     assert np.sqrt(np.mean((x - xr) ** 2)) <= 0.005 * (xr.max() - xr.min())
-    assert abs(cost[-1] - ref_cost[-1]) / ref_cost[-1] < 1e-3
+    assert abs(cost[-1] - ref_cost) / ref_cost < 1e-4, (cost[-3:], ref_cost)
 
 
-@pytest.mark.parametrize("schedule", [dict(), dict(sv_size=4, sv_colors=2, cta_warps=2)])
+@pytest.mark.parametrize("schedule", [dict(), dict(autotune=1), dict(sv_size=4, sv_colors=2, cta_warps=2)])
 def test_concurrent_sv_updates_stay_convergent_on_a_large_single_frame(schedule):
     """A 256 x 256 x 24 single-frame scan with 331 views: with every super-voxel
     of a colour in flight at once (sv 4, 2 colours) the over-relaxed updates
-    diverged; the grid cap keeps the cost monotone (autotuned and forced)."""
+    diverged; the grid cap keeps the cost monotone (shape rule, autotuned and
+    forced)."""
     from phasecon_b200 import phantoms as P
     from phasecon_b200.workloads import _measure
     nv, n, nz = 331, 256, 24
