@@ -59,10 +59,20 @@ def parse():
     ap.add_argument("--schedule", default="",
                     help="4-D workload: fix the sweep schedule as SV,WARPS,COLORS (super-voxel edge, warps per "
                          "column, K of the K x K colouring) instead of the library's shape rule")
-    ap.add_argument("--workload", default="4d", choices=["4d", "batch", "warmstart"],
+    ap.add_argument("--workload", default="4d", choices=["4d", "batch", "warmstart", "pc"],
                     help="4d: the 4-D benchmark (default); batch: 48 uneven 3-D problems, batched vs sequential; "
-                         "warmstart: the learned warm start on the 4-D workload")
+                         "warmstart: the learned warm start on the 4-D workload; pc: the phase-contrast scan "
+                         "(180 views of 256 x 256), phase-retrieval ADMM iterations")
+    ap.add_argument("--nms-order", type=int, default=-1,
+                    help="pc workload: Nelder-Mead sweep order, 0 raster (the reference's), 1 colour classes; "
+                         "-1: the library default")
+    ap.add_argument("--pc-cpu-views", type=int, default=0,
+                    help="pc workload: views of the reference CPU sample (0: one per host thread, at most 32)")
     ap.add_argument("--train-scans", type=int, default=16, help="seeded 4-D training scans (8 frame pairs each)")
+    ap.add_argument("--train-ellipsoids", type=int, default=32,
+                    help="seeded single-frame ellipsoid-phantom training pairs added to the Cahn-Hilliard scans")
+    ap.add_argument("--ws-seeds", type=int, default=3, help="warm start: independent trainings (network seeds)")
+    ap.add_argument("--no-warmstart", action="store_true", help="4-D workload: skip the learned warm start")
     ap.add_argument("--train-steps", type=int, default=6000)
     ap.add_argument("--average-from", type=float, default=0.7,
                     help="warm start: average the network weights from this fraction of the training steps on (1 = off)")
@@ -405,6 +415,10 @@ def run_ours(args, world, rank, local, pg):
         except Exception as ex:
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"failed: {ex}"}
 
+    ws = None
+    if not args.no_warmstart and not args.no_converge:
+        ws = warmstart_section(args, rank, local, pb, p)
+
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
@@ -420,6 +434,9 @@ def run_ours(args, world, rank, local, pg):
                 "voxel_updates_per_step": updates / args.steps, "roofline": roofline, "cpu_baseline": cpu,
                 "e2e": e2e, "clocks": clk.summary(), "gpu_launches": launches}
         line.update(conv)
+        if ws is not None:
+            line["warm_start"] = ws
+            line["speedup_vs_zero_init"] = ws["speedup_vs_zero_init"]
         print(json.dumps(line))
 
 
@@ -485,74 +502,234 @@ def run_batch(args, world, rank, local, pg):
             "clocks": clk.summary()}))
 
 
-def run_warmstart(args, world, rank, local, pg):
-    """The learned warm start on the 4-D workload: train the U-Net on seeded
-    4-D scans other than the benchmark's (FBP frame -> converged plain GPU ICD
-    frame), then time plain ICD on the 4-D problem to the plain method's
-    converged cost (within 1e-4 relative) from zero, from FBP and from the
-    network's output (the FBP and network time included)."""
+def warmstart_section(args, rank: int, local: int, pb, p: float) -> dict:
+    """The learned warm start on the 4-D workload `pb`: one training set (the
+    8 frame pairs of each of `--train-scans` seeded 4-D Cahn-Hilliard scans and
+    `--train-ellipsoids` seeded single-frame ellipsoid phantoms scanned with one
+    frame's views; input = the GPU FBP, target = plain GPU ICD to rel 1e-4;
+    seeds other than the benchmark's), `--ws-seeds` networks trained on it from
+    different seeds, then plain ICD on the benchmark scan timed to the plain
+    method's converged cost (x (1 + 1e-4)) from zero, from FBP and from each
+    network's output; each time includes its initialisation (FBP, network,
+    error sinogram) and follows one untimed run of the same start."""
     import torch
 
     import phasecon_b200 as pc
     from phasecon_b200 import warmstart as WS
-    from phasecon_b200 import workloads as W
 
-    torch.cuda.set_device(local)
     t0 = time.perf_counter()
     pairs = []
     for i in range(args.train_scans):
         pairs += WS.training_pairs_4d(1000 + rank * 100000 + i)
+    n_ch = len(pairs)
+    for i in range(args.train_ellipsoids):
+        x, t, _ = WS.training_pair(5000 + rank * 100000 + i, kind="ellipsoids")
+        pairs.append((x, t))
     t_data = time.perf_counter() - t0
-    net = WS.UNet(16, seed=rank)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    hist = WS.train(net, pairs, args.train_steps, lr=1e-3, seed=rank, average_from=args.average_from)
-    torch.cuda.synchronize()
-    t_train = time.perf_counter() - t0
-    pb, _, p = W.config_4d(seed=0)
     opt = pc.get_options()
     opt.mrf_p = p
     s = pc.Session(pb, options=opt)
     s.set_object(np.zeros(s.shape, np.float32))
     _, c_conv = WS.converge(s, rel=1e-7, max_iter=400)
     target = c_conv[-1] * (1 + 1e-4)
-    res = {}
-    # every start runs once untimed first (device allocations of the FBP and of
-    # the network's stacked inference grid, module loading), then timed
+
+    def timed_start(start):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        start()
+        torch.cuda.synchronize()
+        t_init = time.perf_counter() - t0
+        it, costs = WS.iterations_to_cost(s, target, max_iter=400)
+        torch.cuda.synchronize()
+        return {"time_to_converged_cost_s": time.perf_counter() - t0, "init_s": t_init, "iterations": it,
+                "initial_cost": costs[0], "final_cost": costs[-1]}
+
+    starts = {"zero": lambda: s.set_object(np.zeros(s.shape, np.float32)), "fbp": s.set_object_fbp}
+    res, seeds, train_s, losses = {}, [], [], []
     with ClockSampler(local) as clk:
-        for name in ("zero", "fbp", "unet") * 2:
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            if name == "zero":
-                s.set_object(np.zeros(s.shape, np.float32))
-            elif name == "fbp":
-                s.set_object_fbp()
-            else:
-                WS.warm_start(s, net)
-            torch.cuda.synchronize()
-            t_init = time.perf_counter() - t0
-            it, costs = WS.iterations_to_cost(s, target, max_iter=400)
-            torch.cuda.synchronize()
-            res[name] = {"time_to_converged_cost_s": time.perf_counter() - t0, "init_s": t_init, "iterations": it,
-                         "initial_cost": costs[0], "final_cost": costs[-1]}
+        for name, fn in starts.items():
+            timed_start(fn)  # untimed: module loading, the FBP's allocations
+            res[name] = timed_start(fn)
+    clocks = [clk.summary()]
+    for k in range(args.ws_seeds):
+        net = WS.UNet(16, seed=rank * 1000 + k)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        hist = WS.train(net, pairs, args.train_steps, lr=1e-3, seed=rank * 1000 + k, average_from=args.average_from)
+        torch.cuda.synchronize()
+        train_s.append(time.perf_counter() - t0)
+        losses.append([float(np.mean(hist[:20])), float(np.mean(hist[-20:]))])
+        with ClockSampler(local) as clk:
+            timed_start(lambda: WS.warm_start(s, net))  # untimed: the stacked grid's activation blocks
+            r = timed_start(lambda: WS.warm_start(s, net))
+        clocks.append(clk.summary())
+        r["seed"] = rank * 1000 + k
+        seeds.append(r)
+        net.close()
     s.close()
+    tz, tf = res["zero"]["time_to_converged_cost_s"], res["fbp"]["time_to_converged_cost_s"]
+    sp = [tz / r["time_to_converged_cost_s"] for r in seeds]
+    return {"speedup_vs_zero_init": min(sp) if sp else None, "speedup_vs_zero_init_per_seed": sp,
+            "speedup_vs_zero_init_median": float(np.median(sp)) if sp else None,
+            "speedup_vs_fbp_init_per_seed": [tf / r["time_to_converged_cost_s"] for r in seeds],
+            "target_cost": target, "starts": res, "unet_starts": seeds,
+            "train": {"pairs": len(pairs), "cahn_hilliard_pairs": n_ch, "ellipsoid_pairs": len(pairs) - n_ch,
+                      "steps": args.train_steps, "seeds": args.ws_seeds, "data_s": t_data, "train_s": train_s,
+                      "loss_first_last": losses},
+            "unet": "4 levels 16/32/64/128, 3x3x3, BF16 weights and activations, FP32 accumulation",
+            "timing": "wall time per start (init + ICD to the target cost), each after one untimed run of the "
+                      "same start; speedup_vs_zero_init is the smallest over the seeds",
+            "clocks": clocks}
+
+
+def run_warmstart(args, world, rank, local, pg):
+    """The learned warm start alone (the same section the default 4-D line
+    carries), as its own JSON line."""
+    import torch
+
+    from phasecon_b200 import workloads as W
+
+    torch.cuda.set_device(local)
+    pb, _, p = W.config_4d(seed=0)
+    ws = warmstart_section(args, rank, local, pb, p)
     if rank == 0:
-        tz, tu = res["zero"]["time_to_converged_cost_s"], res["unet"]["time_to_converged_cost_s"]
+        tu = max(r["time_to_converged_cost_s"] for r in ws["unet_starts"]) if ws["unet_starts"] else None
         print(json.dumps({
             "metric": "warm start: wall time to the plain method's converged cost (rel 1e-4), 4-D workload",
             "value": tu, "unit": "s", "n_gpus": world, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "bf16 network / f32 ICD", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "unet": "4 levels 16/32/64/128, 3x3x3, BF16, FP32 accumulation",
-                       "train_pairs": len(pairs), "train_steps": args.train_steps,
-                       "timing": "each start timed after one untimed run of all three",
-                       "train_phantoms": f"{args.train_scans} seeded 4-D Cahn-Hilliard scans (2,000-8,000 steps, "
-                                         "seeds other than the benchmark's), 8 frame pairs each; targets: plain GPU "
-                                         "ICD of the whole 4-D scan to rel 1e-4"},
-            "speedup_vs_zero_init": tz / tu if tu else None,
-            "speedup_vs_fbp_init": res["fbp"]["time_to_converged_cost_s"] / tu if tu else None,
-            "target_cost": target, "starts": res, "train_data_s": t_data, "train_s": t_train,
-            "train_loss_first_last": [float(np.mean(hist[:20])), float(np.mean(hist[-20:]))],
-            "clocks": clk.summary()}))
+            "config": {"workload": WORKLOAD}, **ws}))
+
+
+def pc_reference_rate(pb, views: int, threads: int, workdir: str):
+    """The reference's phcontomo_reconstruct (PCMBIR_3D, built from source with
+    the FP64 FFT shim, all host threads, OpenMP over views) on the first
+    `views` views of the scan: Paganin (recon_type 1), then recon_type 2 with
+    1 and with 2 phase-retrieval iterations; the difference of the two times is
+    one PRet iteration of every sampled view. Returns view-PRet-iterations/s."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    meas = np.ascontiguousarray(pb.measurements[:views])
+    V, rows, cols = meas.shape
+    args = dict(measurements=meas, brights=pb.brights, proj_angles=np.zeros(V, np.float32),
+                proj_times=np.arange(V, dtype=np.float32), recon_times=np.array([0, V], np.float32),
+                proj_rows=rows, proj_cols=cols, proj_num=V, recon_num=1, vox_wid=pb.vox_wid, rot_center=cols / 2,
+                mag_sig_s=pb.mag_sig_s, mag_sig_t=1.0, mag_c_s=pb.mag_c_s, mag_c_t=1.0, phase_sig_s=pb.phase_sig_s,
+                phase_sig_t=1.0, phase_c_s=pb.phase_c_s, phase_c_t=1.0, convg_thresh=0.0,
+                obj2det_dist=pb.obj2det_dist, light_energy=pb.light_energy, pag_regparam=pb.pag_regparam)
+    O.ref_pc_reconstruct(workdir, **args, recon_type=1, threads=threads)
+    t = []
+    for n in (1, 2):
+        t0 = time.perf_counter()
+        O.ref_pc_reconstruct(workdir, **args, recon_type=2, pret_max_iter=n, threads=threads)
+        t.append(time.perf_counter() - t0)
+    dt = t[1] - t[0]
+    return V / dt if dt > 0 else float("nan"), dt, V
+
+
+def run_pc(args, world, rank, local, pg):
+    """Phase-contrast configuration: 40 random spheres in a 256 um cube, 180
+    views of 256 x 256 at 20 keV and 50 mm (phasecon_b200/workloads.py
+    config_pc). A step is one phase-retrieval ADMM iteration (Nelder-Mead
+    proximal sweep, steepest descent on the exit wave to its stop rule, dual
+    update, cost) of every view, batched over the views; the state starts from
+    Paganin retrieval. Warm-up runs W iterations in a session of its own; the
+    timed session runs K iterations (CUDA events on its stream)."""
+    import torch
+
+    from phasecon_b200 import pcmbir as PC
+    from phasecon_b200 import workloads as W
+
+    torch.cuda.set_device(local)
+    stream = torch.cuda.current_stream()
+    pb, _ = W.config_pc(seed=rank)
+    V, rows, cols = pb.dims
+    N = rows * cols
+    kw = {} if args.nms_order < 0 else {"nms_order": args.nms_order}
+    warm = PC.PcSession(pb, PC.default_options(pret_max_iter=max(args.warmup, 1), **kw),
+                        stream=stream.cuda_stream)
+    warm.paganin()
+    warm.init_admm()
+    warm.run()
+    warm.close()
+    opts = PC.default_options(pret_max_iter=args.steps, **kw)
+    s = PC.PcSession(pb, opts, stream=stream.cuda_stream)
+    s.paganin()
+    s.init_admm()
+    barrier(pg)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        costs, iters, st = s.run()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    barrier(pg)
+    ms = max_over_ranks(pg, ev0.elapsed_time(ev1))
+    view_iters = int(iters.sum())
+    value = sum_over_ranks(pg, float(view_iters)) / (ms / 1e3)
+    # dominant memory-side kernel family: the Fresnel-type transform (3 launches
+    # per transform of all views), 16 B per pixel (read + write complex FP32)
+    n_tr = 20
+    s.time_fresnel(2)
+    tr_ms = s.time_fresnel(n_tr)
+    alg_bytes = 16.0 * V * N
+    achieved = alg_bytes / (tr_ms / n_tr / 1e3) / 1e9
+    peak, peak_kind = measured_peaks()
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": None, "peak_source": peak_kind, "kernel": "pc_rows_fft + pc_cols_filter + pc_rows_fft",
+                "algorithmic_bytes_per_launch": alg_bytes, "avg_transform_ms": tr_ms / n_tr,
+                "transforms_per_step": st.fresnel_transforms / max(args.steps, 1)}
+    zr, zi, _, _, _ = s.get_state()
+    s.close()
+    # end to end through the session API with host buffers: session from host
+    # measurements (H2D), Paganin, K iterations, D2H of the retrieved z
+    torch.cuda.synchronize()
+    barrier(pg)
+    t0 = time.perf_counter()
+    s2 = PC.PcSession(pb, opts, stream=stream.cuda_stream)
+    s2.paganin()
+    s2.init_admm()
+    _, it2, _ = s2.run()
+    out = s2.get_state()
+    torch.cuda.synchronize()
+    t_e2e = max_over_ranks(pg, time.perf_counter() - t0)
+    s2.close()
+    e2e = {"value": sum_over_ranks(pg, float(it2.sum())) / t_e2e, "unit": "view-iterations/s",
+           "h2d_bytes_per_step": (pb.measurements.nbytes + pb.brights.nbytes) / args.steps,
+           "d2h_bytes_per_step": sum(a.nbytes for a in out[:2]) / args.steps, "steps_per_call": args.steps,
+           "note": "session from host arrays, Paganin start, K iterations, D2H of the retrieved z (r, i)"}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            sys.path.insert(0, os.path.join(ROOT, "oracle"))
+            import oracle
+            if oracle.ref_pc_available():
+                threads = os.cpu_count() or 1
+                nv = args.pc_cpu_views or min(threads, 32)
+                rate, dt, nv = pc_reference_rate(pb, nv, threads, tempfile.mkdtemp())
+                cpu = {"value": rate, "unit": "view-iterations/s", "cores": threads, "kind": "reference",
+                       "sample": f"reference PCMBIR_3D phcontomo_reconstruct built from source (FFTW replaced by an "
+                                 f"FP64 radix-2 FFT with tabulated twiddles), recon_type 2 on the first {nv} views "
+                                 f"of the same scan, one phase-retrieval iteration each (1- and 2-iteration runs "
+                                 f"differenced, {dt:.1f} s), OpenMP over views"}
+        except Exception as ex:
+            cpu = {"value": None, "unit": "view-iterations/s", "cores": 0, "kind": "reference",
+                   "sample": f"failed: {ex}"}
+    if rank == 0:
+        print(json.dumps({
+            "metric": "phase-retrieval ADMM iterations x views per second (config 3 phase contrast)",
+            "value": value, "unit": "view-iterations/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 (FP64 per-view sums)", "data": "synthetic",
+            "config": {"workload": "pc_spheres_256cube_180views_256x256", "views": V, "detector": [rows, cols],
+                       "nms_order": int(opts.nms_order), "sd_max_iter": int(opts.sd_max_iter),
+                       "nms_max_iter": int(opts.nms_max_iter), "parallelism": f"replicas{world}",
+                       "l2": "inputs larger than L2: 14 per-view complex/real FP32 arrays of 180 x 256^2 (~1 GB)"},
+            "sd_steps_per_view_iteration": st.sd_steps / max(view_iters, 1),
+            "final_cost_mean": float(np.nanmean([c[np.isfinite(c)][-1] for c in costs])),
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(),
+            "gpu_launches": int(st.kernel_launches)}))
 
 
 def main():
@@ -565,6 +742,8 @@ def main():
             run_batch(args, world, rank, local, pg)
         elif args.workload == "warmstart":
             run_warmstart(args, world, rank, local, pg)
+        elif args.workload == "pc":
+            run_pc(args, world, rank, local, pg)
         else:
             run_ours(args, world, rank, local, pg)
     finally:

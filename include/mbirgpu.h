@@ -394,6 +394,7 @@ typedef struct {
     int64_t sd_steps;          /* steepest-descent steps run, summed over views */
     int64_t fresnel_transforms;/* Fresnel transforms run, summed over views */
     double kernel_ms;          /* device time of the run (CUDA events) */
+    int64_t kernel_launches;   /* kernels the run launched */
 } mbirgpu_pc_stats;
 
 void mbirgpu_pc_default_options(mbirgpu_pc_options *opt);
@@ -410,6 +411,11 @@ int mbirgpu_pc_session_destroy(mbirgpu_pc_session *s);
 /* Batched Fresnel transform of every view (herm = 0: compute_FresnelTran,
  * herm = 1: compute_HermFresnelTran). */
 int mbirgpu_pc_fresnel(mbirgpu_pc_session *s, const float *in, float *out, int32_t herm);
+/* No counterpart in the reference (a measurement aid). n Fresnel-type
+ * transforms (herm: the Hermitian one) of every view of the session, on its
+ * resident buffers (whatever they hold), enqueued back to back on the
+ * session's stream; *ms receives their device time (CUDA events). */
+int mbirgpu_pc_time_fresnel(mbirgpu_pc_session *s, int32_t n, int32_t herm, double *ms);
 /* Paganin retrieval of every view into the session's z (and, if not NULL, zr/zi). */
 int mbirgpu_pc_paganin(mbirgpu_pc_session *s, float *zr, float *zi);
 int mbirgpu_pc_set_z(mbirgpu_pc_session *s, const float *zr, const float *zi);

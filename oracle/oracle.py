@@ -551,6 +551,52 @@ def ref_pc_estimate(g, y, om, D, zr, zi, lam, w, workdir, pret_iters=100, sd_ite
     return z_r[..., 1].copy(), z_i[..., 1].copy(), w_r + 1j * w_i, v_r + 1j * v_i, om_r + 1j * om_i, cost
 
 
+def ref_pc_reconstruct(workdir: str, measurements, brights, proj_angles, proj_times, recon_times, proj_rows,
+                       proj_cols, proj_num, recon_num, vox_wid, rot_center, mag_sig_s, mag_sig_t, mag_c_s, mag_c_t,
+                       phase_sig_s, phase_sig_t, phase_c_s, phase_c_t, convg_thresh, obj2det_dist, light_energy,
+                       pag_regparam, restart=0, recon_type=1, pret_max_iter: int = 100, mrf_p: float = 1.2,
+                       threads: int = 0) -> None:
+    """The reference's own phcontomo_reconstruct (PCMBIR_3D/XT_Engine.c:82-197)
+    run in `workdir`, where it leaves its output files (pag_*_ret.bin for
+    recon_type 1; *_pret_aux, *_pret_dual, omega_*, pret_cost_proj_<i> ... for
+    recon_type 2). pret_max_iter sets PRet_MaxIter (XT_Init.c:516, 100 as
+    shipped); threads sets the OpenMP thread count (0: the default)."""
+    lib = ref_pc_lib()
+    C.c_int.in_dll(lib, "oracle_ref_pret_max_iter").value = int(pret_max_iter)
+    C.c_double.in_dll(lib, "oracle_ref_pc_mrf_p").value = float(mrf_p)
+    fp = C.POINTER(C.c_float)
+    lib.phcontomo_reconstruct.argtypes = [C.POINTER(fp), C.POINTER(fp)] + [C.c_void_p] * 5 + [C.c_int32] * 4 + \
+        [C.c_float] * 14 + [C.c_uint8, C.c_uint8, C.c_void_p]
+    lib.phcontomo_reconstruct.restype = C.c_int
+    arrs = [np.ascontiguousarray(a, dtype=np.float32) for a in
+            (measurements, brights, proj_angles, proj_times, recon_times)]
+    libc = C.CDLL(None)
+    libc.fopen.restype = C.c_void_p
+    libc.fopen.argtypes = [C.c_char_p, C.c_char_p]
+    libc.fclose.argtypes = [C.c_void_p]
+    if threads > 0:
+        try:
+            omp = C.CDLL("libgomp.so.1")
+            omp.omp_set_num_threads(int(threads))
+        except OSError:
+            pass
+    mag, ph = fp(), fp()
+    cwd = os.getcwd()
+    os.makedirs(workdir, exist_ok=True)
+    os.chdir(workdir)
+    dbg = libc.fopen(b"debug.txt", b"a")
+    try:
+        rc = lib.phcontomo_reconstruct(C.byref(mag), C.byref(ph), *(a.ctypes.data for a in arrs), proj_rows, proj_cols,
+                                       proj_num, recon_num, vox_wid, rot_center, mag_sig_s, mag_sig_t, mag_c_s, mag_c_t,
+                                       phase_sig_s, phase_sig_t, phase_c_s, phase_c_t, convg_thresh, obj2det_dist,
+                                       light_energy, pag_regparam, restart, recon_type, dbg)
+    finally:
+        libc.fclose(dbg)
+        os.chdir(cwd)
+    if rc != 0:
+        raise RuntimeError(f"reference phcontomo_reconstruct returned {rc}")
+
+
 def ref_pc_paganin(g, meas, D):
     zr, zi = np.zeros(meas.shape), np.zeros(meas.shape)
     ref_pc_lib().ref_pc_paganin(C.byref(pc_params(g)), _c(meas), _c(D.real), _c(D.imag), g.wavenumber, zr, zi)

@@ -28,6 +28,7 @@ double oracle_ref_pc_mrf_p = 1.2;
 /* phantom sizes of the data simulator (PHANTOM_XY_SIZE / PHANTOM_Z_SIZE) */
 int oracle_ref_phantom_xy = 512;
 int oracle_ref_phantom_z = 128;
+int oracle_ref_pret_max_iter = 100; /* PRet_MaxIter of XT_Init.c:516 */
 
 void initFilter(ScannedObject *ScannedObjectPtr, TomoInputs *TomoInputsPtr);
 void create_FresnelTranWindow(Real_arr_t **Freq_Window, int32_t rows, int32_t cols, Real_t delta_rows, Real_t delta_cols, Real_t sigma);

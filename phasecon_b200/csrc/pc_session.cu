@@ -150,7 +150,10 @@ struct PcSession {
                    int acc_slot)
     {
         pc_transform(d, A, smem_rows, smem_cols, prologue, in, table, epilogue, out, acc_slot, st);
+        launches += 3;
     }
+
+    int64_t launches = 0;  // kernels this session has launched
 
     dim3 pointwise_grid() const { return dim3(std::max(1, std::min(64, d.N / 1024)), d.V); }
 
@@ -166,10 +169,12 @@ struct PcSession {
     {
         if (opt.nms_order == 0) {
             pc_nms_wavefront<<<d.V, 128, 0, st>>>(d, A, prior, opt.nms_max_iter, (float)opt.nms_threshold);
+            launches += 1;
             return;
         }
         for (int color = 0; color < 4; color++)
             pc_nms<<<pointwise_grid(), 256, 0, st>>>(d, A, prior, color, opt.nms_max_iter, (float)opt.nms_threshold);
+        launches += 4;
     }
 };
 
@@ -304,6 +309,7 @@ void PcSession::sd_step(int *active, int step)
     pc_sd_update<<<pointwise_grid(), 256, 0, st>>>(d, A);
     transform(A, PC_IN_DW, d_w, d_Hf, PC_OUT_OMEGA, nullptr, 0);
     pc_sd_finish<<<(d.V + 127) / 128, 128, 0, st>>>(d, A, step, (float)opt.sd_threshold);
+    launches += 2;
 }
 
 int PcSession::omega_from_w(int *active)
@@ -318,6 +324,7 @@ void PcSession::pret_cost(int *active)
     PcArgs A = args(active);
     transform(A, PC_IN_DEZ, nullptr, d_Hf, PC_OUT_PCOST, nullptr, PC_ACC_PCOST);
     pc_prior_cost<<<pointwise_grid(), 256, 0, st>>>(d, A, prior);
+    launches += 1;
 }
 
 int PcSession::any_active(const int *flags, bool *any)
@@ -335,6 +342,7 @@ int PcSession::any_active(const int *flags, bool *any)
 int PcSession::run(double *costs, int32_t *iters, mbirgpu_pc_stats *stats)
 {
     const int V = d.V, P = opt.pret_max_iter;
+    const int64_t launches0 = launches;
     if (!ev0) PCK(cudaEventCreate(&ev0));
     if (!ev1) PCK(cudaEventCreate(&ev1));
     PCK(cudaEventRecord(ev0, st));
@@ -351,12 +359,14 @@ int PcSession::run(double *costs, int32_t *iters, mbirgpu_pc_stats *stats)
     // cost before the first iteration (:111)
     pret_cost(d_act_pret);
     pc_pret_finish<<<(V + 127) / 128, 128, 0, st>>>(d, args(d_act_pret), -1, (float)opt.pret_threshold, d_costs);
+    launches += 1;
     PCK(cudaGetLastError());
     int it = 0;
     for (; it < P; it++) {
         PcArgs A = args(d_act_pret);
         nms_sweep(A);
         pc_pret_prepare<<<pointwise_grid(), 256, 0, st>>>(d, A);
+        launches += 1;
         PCK(cudaMemcpyAsync(d_act_sd, d_act_pret, V * sizeof(int), cudaMemcpyDeviceToDevice, st));
         for (int j = 0; j < opt.sd_max_iter; j++) {
             sd_step(d_act_sd, j);
@@ -368,9 +378,11 @@ int PcSession::run(double *costs, int32_t *iters, mbirgpu_pc_stats *stats)
             }
         }
         pc_pret_dual<<<pointwise_grid(), 256, 0, st>>>(d, A);
+        launches += 1;
         pret_cost(d_act_pret);
         pc_pret_finish<<<(V + 127) / 128, 128, 0, st>>>(d, A, it, (float)opt.pret_threshold,
                                                          d_costs + (size_t)(it + 1) * V);
+        launches += 1;
         PCK(cudaGetLastError());
         bool any = false;
         if (any_active(d_act_pret, &any)) return -1;
@@ -400,6 +412,7 @@ int PcSession::run(double *costs, int32_t *iters, mbirgpu_pc_stats *stats)
             stats->fresnel_transforms += 5LL * steps[v] + pit[v] + 1;
         }
         stats->kernel_ms = ms;
+        stats->kernel_launches = launches - launches0;
     }
     return 0;
 }
@@ -503,6 +516,30 @@ int mbirgpu_pc_fresnel(mbirgpu_pc_session *sp, const float *in, float *out, int3
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return fail("Fresnel transform launch failed: %s", cudaGetErrorString(e));
     return download(s, reinterpret_cast<float2 *>(out), s->d_buf, NV);
+}
+
+int mbirgpu_pc_time_fresnel(mbirgpu_pc_session *sp, int32_t n, int32_t herm, double *ms)
+{
+    PCSESSION(sp);
+    if (!ms || n < 1) return fail("need n >= 1 and a result pointer");
+    cudaEvent_t a = nullptr, b = nullptr;
+    if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess) {
+        if (a) cudaEventDestroy(a);
+        return fail("cudaEventCreate failed");
+    }
+    cudaEventRecord(a, s->st);
+    for (int i = 0; i < n; i++)
+        s->transform(s->args(nullptr), mbirgpu::PC_IN_PLAIN, s->d_T1, herm ? s->d_Hh : s->d_Hf,
+                     mbirgpu::PC_OUT_PLAIN, s->d_buf, 0);
+    cudaEventRecord(b, s->st);
+    cudaError_t e = cudaEventSynchronize(b);
+    float t = 0.f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&t, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (e != cudaSuccess) return fail("timing the Fresnel transforms failed: %s", cudaGetErrorString(e));
+    *ms = t;
+    return 0;
 }
 
 int mbirgpu_pc_paganin(mbirgpu_pc_session *sp, float *zr, float *zi)

@@ -38,7 +38,7 @@ EXPORTS = (
     "mbirgpu_batch_create", "mbirgpu_batch_destroy", "mbirgpu_batch_run", "mbirgpu_batch_problem_info",
     "mbirgpu_batch_get_object", "mbirgpu_batch_cost", "mbirgpu_reconstruct_batch",
     "phcontomo_reconstruct", "mbirgpu_pc_default_options", "mbirgpu_pc_session_create", "mbirgpu_pc_session_destroy",
-    "mbirgpu_pc_fresnel", "mbirgpu_pc_paganin", "mbirgpu_pc_set_z", "mbirgpu_pc_init_admm", "mbirgpu_pc_set_state",
+    "mbirgpu_pc_fresnel", "mbirgpu_pc_time_fresnel", "mbirgpu_pc_paganin", "mbirgpu_pc_set_z", "mbirgpu_pc_init_admm", "mbirgpu_pc_set_state",
     "mbirgpu_pc_get_state", "mbirgpu_pc_sd_step", "mbirgpu_pc_nms_sweep", "mbirgpu_pc_run",
     "phcontomo_forward_project", "mbirgpu_pc_sim_default_options", "mbirgpu_pc_sim_set_options",
     "mbirgpu_pc_sim_get_options", "mbirgpu_pc_simulate",

@@ -42,7 +42,8 @@ class PcOptions(C.Structure):
 
 
 class PcStats(C.Structure):
-    _fields_ = [("sd_steps", C.c_int64), ("fresnel_transforms", C.c_int64), ("kernel_ms", C.c_double)]
+    _fields_ = [("sd_steps", C.c_int64), ("fresnel_transforms", C.c_int64), ("kernel_ms", C.c_double),
+                ("kernel_launches", C.c_int64)]
 
 
 class SimOptions(C.Structure):
@@ -70,6 +71,7 @@ def lib() -> C.CDLL:
         L.mbirgpu_pc_session_destroy.argtypes = [vp]
         L.mbirgpu_pc_fresnel.argtypes = [vp, vp, vp, C.c_int32]
         L.mbirgpu_pc_paganin.argtypes = [vp, vp, vp]
+        L.mbirgpu_pc_time_fresnel.argtypes = [vp, C.c_int32, C.c_int32, C.POINTER(C.c_double)]
         L.mbirgpu_pc_set_z.argtypes = [vp, vp, vp]
         L.mbirgpu_pc_init_admm.argtypes = [vp]
         L.mbirgpu_pc_set_state.argtypes = [vp, vp, vp, vp]
@@ -166,6 +168,12 @@ class PcSession:
         out = np.zeros_like(a)
         _check(lib().mbirgpu_pc_fresnel(self.h, a.ctypes.data, out.ctypes.data, 1 if herm else 0))
         return _f2c(out)
+
+    def time_fresnel(self, n: int, herm: bool = False) -> float:
+        """Device milliseconds of n back-to-back transforms of every view."""
+        ms = C.c_double()
+        _check(lib().mbirgpu_pc_time_fresnel(self.h, n, 1 if herm else 0, C.byref(ms)))
+        return ms.value
 
     def paganin(self):
         zr = np.zeros(self.shape, np.float32)
