@@ -48,20 +48,25 @@ double *g_scratch_ptr[kMaxDevices] = {};
 
 // The forward projector with the object read in the ABI's volume layout
 // [N_time][N_z][N_y][N_x] (no conversion pass, so no staging buffer): one warp
-// per (frame, voxel column), lane = detector row, FP64 reductions into acc.
+// per (frame, voxel column, chunk of 32 detector rows), lane = detector row,
+// FP64 reductions into acc.
 __global__ void __launch_bounds__(256) forward_project_vol_kernel(Geom g, const uint32_t *__restrict__ table,
                                                                  const int32_t *__restrict__ view_first,
                                                                  const float *__restrict__ vol,
                                                                  double *__restrict__ acc)
 {
     const int nxy = g.N_x * g.N_y;
+    const int n_chunks = (g.N_t + kRowChunk - 1) / kRowChunk;
     const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
-    if (gw >= (long long)g.N_time * nxy) return;
-    const int f = (int)(gw / nxy), c = (int)(gw - (long long)f * nxy);
-    const bool row_ok = lane < g.N_t;
+    if (gw >= (long long)g.N_time * nxy * n_chunks) return;
+    const int ch = (int)(gw % n_chunks);
+    const long long fc = gw / n_chunks;
+    const int f = (int)(fc / nxy), c = (int)(fc - (long long)f * nxy);
+    const int t = ch * kRowChunk + lane;  // this lane's detector row
+    const bool row_ok = t < g.N_t;
     const double xv =
-        row_ok ? (double)__ldg(vol + ((size_t)f * g.N_z + lane / g.z_overlap) * nxy + c) : 0.0;
+        row_ok ? (double)__ldg(vol + ((size_t)f * g.N_z + t / g.z_overlap) * nxy + c) : 0.0;
     if (__all_sync(0xffffffffu, xv == 0.0)) return;
     const int fv0 = view_first[f], nv = view_first[f + 1] - fv0;
     const uint32_t *rec = table + ((size_t)fv0 * nxy + (size_t)c * nv) * g.rec_words;
@@ -70,7 +75,7 @@ __global__ void __launch_bounds__(256) forward_project_vol_kernel(Geom g, const 
         const uint32_t hdr = __ldg(rec);
         const int cnt = hdr >> 24, row = hdr & 0xFFFFFF;
         for (int q = 0; q < cnt; q++)
-            atomicAdd(acc + (size_t)(row + q) * g.N_t + lane, xv * (double)__uint_as_float(__ldg(rec + 1 + q)));
+            atomicAdd(acc + (size_t)(row + q) * g.N_t + t, xv * (double)__uint_as_float(__ldg(rec + 1 + q)));
     }
 }
 
@@ -141,7 +146,7 @@ int forward_project_noalloc(Session *s, const float *object_dev, float *sino_dev
     if (scratch_for_device(s->device, s->st, &acc)) return -1;
     cudaError_t e = cudaMemsetAsync(acc, 0, n * sizeof(double), s->st);
     if (e != cudaSuccess) return fail("clearing the projection scratch failed: %s", cudaGetErrorString(e));
-    const long long warps = (long long)g.N_time * g.N_x * g.N_y;
+    const long long warps = (long long)g.N_time * g.N_x * g.N_y * ((g.N_t + kRowChunk - 1) / kRowChunk);
     const long long blocks = (warps * 32 + 255) / 256;
     forward_project_vol_kernel<<<(unsigned)blocks, 256, 0, s->st>>>(g, s->d_table, s->d_view_first, object_dev, acc);
     round_accumulator_kernel<<<148 * 8, 256, 0, s->st>>>(n, acc, sino_dev);

@@ -142,8 +142,8 @@ std::string build_setup(HostSetup &hs, const ProblemDesc &pd, const float *angle
         g.huber_T = pd.huber_T;
         g.huber_delta = pd.huber_delta;
     }
-    if (g.N_t > kMaxNt) return "More than 32 detector rows per problem is not supported by this build.";
     if ((long long)g.N_p * g.N_r >= (1LL << 24)) return "proj_num * proj_cols must stay below 2^24.";
+    if ((long long)g.N_p * g.N_r * g.N_t >= (1LL << 32)) return "proj_num * proj_cols * proj_rows must stay below 2^32.";
 
     // view -> frame map (initRandomAngles / initSparseAnglesOfObject, XT_Init.c:69-131)
     for (int i = 0; i + 1 < g.N_p; i++)

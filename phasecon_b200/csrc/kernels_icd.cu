@@ -244,7 +244,9 @@ __device__ __forceinline__ void flush_counts(IcdCount &cnt, IcdStats *stats)
 // buffers of stage_words words), the next column's copied in by a TMA bulk copy
 // while the current one is updated, so the theta pass waits on one global
 // round trip per view group instead of two and the apply pass on none.
-template <int KW, int kUnroll, int VEC, bool kStaged>
+// kHuber: 0 the quadratic data term, 1 the generalised Huber one
+// (XT_VoxUpdate.c:68-82), 2 decided per problem at run time (K.huber).
+template <int KW, int kUnroll, int VEC, bool kStaged, int kHuber>
 __device__ __forceinline__ void icd_update_sv(const Geom &g, const IcdLaunch &L, const IcdConst &K,
                                               const uint32_t *__restrict__ table,
                                               const int32_t *__restrict__ view_first,
@@ -257,19 +259,22 @@ __device__ __forceinline__ void icd_update_sv(const Geom &g, const IcdLaunch &L,
     const int NX = g.N_x, NY = g.N_y, NZ = g.N_z, NT = g.N_t, MZ = g.z_overlap;
     const int nxy = NX * NY;
     const int RW = g.rec_words;
+    // A voxel column is updated in chunks of at most 32 detector rows (32 / MZ
+    // voxel slices, one per lane of warp 0); chunk k covers rows [32k, 32k + 32)
+    // and slices [k CZ, k CZ + CZ). Columns of up to 32 rows are one chunk.
+    const int CT = NT < 32 ? NT : 32, CZ = CT / MZ;
+    const int n_chunks = (NT + 31) / 32;
 
     // lane -> (view group, run of VEC detector rows) for the theta / apply passes
     using VT = typename VecF<VEC>::T;
-    const int lpr = NT / VEC;  // lanes per sinogram row
+    const int lpr = CT / VEC;  // lanes per sinogram row of a full chunk
     int lprp = 1;
     while (lprp < lpr) lprp <<= 1;
     const int G = 32 / lprp;  // view groups per warp
     const int grp = lane / lprp, tq = lane % lprp;
-    const bool row_ok = tq < lpr;
-    const int t0 = tq * VEC;  // first detector row of this lane
+    const int t0 = tq * VEC;  // first detector row of this lane within the chunk
     const int gstride = W * G;
     const int gfirst = warp * G + grp;
-    const bool zl = lane < NZ;
     const int fv0 = view_first[f], nv = view_first[f + 1] - fv0;
 
     // ---- the SV's columns inside the reconstruction circle, shuffled ----------
@@ -316,237 +321,265 @@ __device__ __forceinline__ void icd_update_sv(const Geom &g, const IcdLaunch &L,
         const size_t col_off = ((size_t)f * nxy + c) * NZ;
         const uint32_t *col_rec = kStaged ? srec + (ci & 1) * stage_words : table + (rec_frame + (size_t)c * nv) * RW;
 
-        // ---- 1. neighbourhood (sources split over warps) + column activity ------
-        int active_pred;
-        const float V = zl ? x[col_off + lane] : 0.0f;  // the column itself (warp 0 reuses it in the solve)
-        {
-            float num = 0.0f, den = 0.0f;
-            int pos = 0;
-            for (int s = warp; s < 10; s += W) {
-                if (s < 8) {
-                    const int o = s < 4 ? s : s + 1;  // skip the centre of the 3x3
-                    const int dy = o / 3 - 1, dx = o % 3 - 1;
-                    const int jj = j + dy, kk = k + dx;
-                    const bool valid = jj >= 0 && jj < NY && kk >= 0 && kk < NX;
-                    const float nz0 = (valid && zl) ? x[((size_t)f * nxy + jj * NX + kk) * NZ + lane] : 0.0f;
-                    const float nzm = __shfl_up_sync(0xffffffffu, nz0, 1);
-                    const float nzp = __shfl_down_sync(0xffffffffu, nz0, 1);
-                    if (valid && zl) {
-                        const float nb[3] = {nzm, nz0, nzp};
+        for (int ch = 0; ch < n_chunks; ch++) {
+            const int z0 = ch * CZ;                                  // first slice of the chunk
+            const int cz = NZ - z0 < CZ ? NZ - z0 : CZ;              // slices in the chunk
+            const int ct = cz * MZ;                                  // detector rows in the chunk
+            const int rbase = ch * 32;                               // first detector row of the chunk
+            const bool zl = lane < cz;
+            const int z = z0 + lane;                                 // this lane's slice
+            const bool row_ok = tq < ct / VEC;
+
+            // ---- 1. neighbourhood (sources split over warps) + column activity ------
+            int active_pred;
+            const float V = zl ? x[col_off + z] : 0.0f;  // the column itself (warp 0 reuses it in the solve)
+            {
+                float num = 0.0f, den = 0.0f;
+                int pos = 0;
+                for (int s = warp; s < 10; s += W) {
+                    if (s < 8) {
+                        const int o = s < 4 ? s : s + 1;  // skip the centre of the 3x3
+                        const int dy = o / 3 - 1, dx = o % 3 - 1;
+                        const int jj = j + dy, kk = k + dx;
+                        const bool valid = jj >= 0 && jj < NY && kk >= 0 && kk < NX;
+                        const size_t noff = ((size_t)f * nxy + jj * NX + kk) * NZ;
+                        const float nz0 = (valid && zl) ? x[noff + z] : 0.0f;
+                        float nzm = __shfl_up_sync(0xffffffffu, nz0, 1);
+                        float nzp = __shfl_down_sync(0xffffffffu, nz0, 1);
+                        // across chunk edges the z +- 1 neighbours are outside the warp
+                        if (lane == 0 && z > 0 && valid) nzm = x[noff + z - 1];
+                        if (lane == cz - 1 && z + 1 < NZ && valid) nzp = x[noff + z + 1];
+                        if (valid && zl) {
+                            const float nb[3] = {nzm, nz0, nzp};
 #pragma unroll
-                        for (int dz = -1; dz <= 1; dz++) {
-                            const int zz = lane + dz;
-                            if (zz < 0 || zz >= NZ) continue;
-                            const float n = nb[dz + 1];
-                            const float b = qg_weight(V - n, K.q, K.qmp, K.issq, K.issqp, K.cs, K.bs0);
-                            const float cf = K.sf[(dz + 1) * 9 + (dy + 1) * 3 + (dx + 1)] * b;
+                            for (int dz = -1; dz <= 1; dz++) {
+                                const int zz = z + dz;
+                                if (zz < 0 || zz >= NZ) continue;
+                                const float n = nb[dz + 1];
+                                const float b = qg_weight(V - n, K.q, K.qmp, K.issq, K.issqp, K.cs, K.bs0);
+                                const float cf = K.sf[(dz + 1) * 9 + (dy + 1) * 3 + (dx + 1)] * b;
+                                num += cf * n;
+                                den += cf;
+                                pos |= n > 0.0f;
+                            }
+                        }
+                    } else {
+                        const int ff = f + (s == 8 ? -1 : 1);
+                        if (ff >= 0 && ff < g.N_time && zl) {
+                            const float n = x[((size_t)ff * nxy + c) * NZ + z];
+                            const float b = qg_weight(V - n, K.q, K.qmp, K.istq, K.istqp, K.ct, K.bt0);
+                            const float cf = K.tf * b;
                             num += cf * n;
                             den += cf;
                             pos |= n > 0.0f;
                         }
                     }
-                } else {
-                    const int ff = f + (s == 8 ? -1 : 1);
-                    if (ff >= 0 && ff < g.N_time && zl) {
-                        const float n = x[((size_t)ff * nxy + c) * NZ + lane];
-                        const float b = qg_weight(V - n, K.q, K.qmp, K.istq, K.istqp, K.ct, K.bt0);
-                        const float cf = K.tf * b;
-                        num += cf * n;
-                        den += cf;
-                        pos |= n > 0.0f;
-                    }
                 }
+                S.num[warp][lane] = num;
+                S.den[warp][lane] = den;
+                S.pos[warp][lane] = pos;
+                // a column is skipped only if every slice is zero with no positive
+                // neighbour (in-column neighbours are the column's own values)
+                active_pred = !L.zero_skipping || L.iter <= 1 || (zl && V != 0.0f) || pos;
             }
-            S.num[warp][lane] = num;
-            S.den[warp][lane] = den;
-            S.pos[warp][lane] = pos;
-            // a column is skipped only if every slice is zero with no positive
-            // neighbour (in-column neighbours are the column's own values)
-            active_pred = !L.zero_skipping || L.iter <= 1 || (zl && V != 0.0f) || pos;
-        }
-        if (kStaged)  // issued one column earlier
-            wait_staged(&S.stage_bar[ci & 1], cnt.phases, ci & 1, cnt.timeouts, S.abort, S.abort_bar, S.abort_parity);
-        const int any_active = __syncthreads_or(active_pred);
-        // a late copy leaves this column's records undefined: no update, no
-        // further copies (S.abort is read after the barrier, so uniformly)
-        if (kStaged && S.abort) return;
-        // every thread is past the previous column's apply pass: its record
-        // buffer may be refilled with the next column's
-        if (kStaged && ci + 1 < ncols)
-            stage_records(srec + ((ci + 1) & 1) * stage_words,
-                          table + (rec_frame + (size_t)S.order[ci + 1] * nv) * RW, nv * RW, &S.stage_bar[(ci + 1) & 1]);
-        if (!any_active) {
-            if (warp == 0 && zl) cnt.skip++;
-            if (warp == 0 && lane == 0) mag[(size_t)f * nxy + c] = 0.0f;
-            continue;  // uniform across the CTA
-        }
+            if (kStaged && ch == 0)  // issued one column earlier
+                wait_staged(&S.stage_bar[ci & 1], cnt.phases, ci & 1, cnt.timeouts, S.abort, S.abort_bar,
+                            S.abort_parity);
+            const int any_active = __syncthreads_or(active_pred);
+            if (ch == 0) {
+                // a late copy leaves this column's records undefined: no update, no
+                // further copies (S.abort is read after the barrier, so uniformly)
+                if (kStaged && S.abort) return;
+                // every thread is past the previous column's apply pass: its record
+                // buffer may be refilled with the next column's
+                if (kStaged && ci + 1 < ncols)
+                    stage_records(srec + ((ci + 1) & 1) * stage_words,
+                                  table + (rec_frame + (size_t)S.order[ci + 1] * nv) * RW, nv * RW,
+                                  &S.stage_bar[(ci + 1) & 1]);
+            }
+            if (!any_active) {
+                if (warp == 0 && zl) cnt.skip++;
+                if (warp == 0 && lane == 0 && ch == 0) mag[(size_t)f * nxy + c] = 0.0f;
+                continue;  // uniform across the CTA
+            }
 
-        // ---- 2. theta over the column's views -----------------------------------
-        {
-            float th1[VEC], th2[VEC];
+            // ---- 2. theta over the column's views -----------------------------------
+            {
+                float th1[VEC], th2[VEC];
 #pragma unroll
-            for (int i = 0; i < VEC; i++) th1[i] = th2[i] = 0.0f;
-            if (row_ok) {
-                for (int v0 = gfirst; v0 < nv; v0 += kUnroll * gstride) {
-                    Rec<KW> R[kUnroll];
+                for (int i = 0; i < VEC; i++) th1[i] = th2[i] = 0.0f;
+                if (row_ok) {
+                    for (int v0 = gfirst; v0 < nv; v0 += kUnroll * gstride) {
+                        Rec<KW> R[kUnroll];
 #pragma unroll
-                    for (int u = 0; u < kUnroll; u++) {
-                        const int v = v0 + u * gstride;
-                        if (v < nv) R[u] = kStaged ? load_rec_smem<KW>(col_rec + (size_t)v * RW)
-                                               : load_rec<KW>(col_rec + (size_t)v * RW);
-                        else R[u].w[0].x = 0u;
-                    }
+                        for (int u = 0; u < kUnroll; u++) {
+                            const int v = v0 + u * gstride;
+                            if (v < nv) R[u] = kStaged ? load_rec_smem<KW>(col_rec + (size_t)v * RW)
+                                                   : load_rec<KW>(col_rec + (size_t)v * RW);
+                            else R[u].w[0].x = 0u;
+                        }
 #pragma unroll
-                    for (int u = 0; u < kUnroll; u++) {
-                        const uint32_t hdr = R[u].w[0].x;
-                        const int cnt_q = hdr >> 24;
-                        // sinogram rows stay below 2^24 and N_t <= 32: 32-bit offsets
-                        const unsigned sb = (hdr & 0xFFFFFFu) * (unsigned)NT + (unsigned)t0;
+                        for (int u = 0; u < kUnroll; u++) {
+                            const uint32_t hdr = R[u].w[0].x;
+                            const int cnt_q = hdr >> 24;
+                            // sinogram rows stay below 2^24 and N_t rows each: 32-bit offsets
+                            const unsigned sb = (hdr & 0xFFFFFFu) * (unsigned)NT + (unsigned)(rbase + t0);
 #pragma unroll
-                        for (int q = 0; q < 4 * KW - 1; q++) {
-                            if (q < cnt_q) {
-                                float ev[VEC], wv[VEC];
-                                VecF<VEC>::get(__ldcg(reinterpret_cast<const VT *>(err + (sb + (unsigned)(q * NT)))), ev);
-                                VecF<VEC>::get(__ldg(reinterpret_cast<const VT *>(wgt + (sb + (unsigned)(q * NT)))), wv);
-                                const float a = rec_val<KW>(R[u], q) * K.dt;
+                            for (int q = 0; q < 4 * KW - 1; q++) {
+                                if (q < cnt_q) {
+                                    float ev[VEC], wv[VEC];
+                                    VecF<VEC>::get(__ldcg(reinterpret_cast<const VT *>(err + (sb + (unsigned)(q * NT)))), ev);
+                                    VecF<VEC>::get(__ldg(reinterpret_cast<const VT *>(wgt + (sb + (unsigned)(q * NT)))), wv);
+                                    const float a = rec_val<KW>(R[u], q) * K.dt;
 #pragma unroll
-                                for (int i = 0; i < VEC; i++) {
-                                    float ww = wv[i];
-                                    if (K.huber) {
-                                        const float sw = sqrtf(ww);
-                                        if (!(fabsf(ev[i] * sw) < K.huber_T)) ww = K.huber_T * K.huber_delta * sw / fabsf(ev[i]);
+                                    for (int i = 0; i < VEC; i++) {
+                                        float ww = wv[i];
+                                        if (kHuber == 1 || (kHuber == 2 && K.huber)) {
+                                            const float sw = sqrtf(ww);
+                                            if (!(fabsf(ev[i] * sw) < K.huber_T)) ww = K.huber_T * K.huber_delta * sw / fabsf(ev[i]);
+                                        }
+                                        const float aw = a * ww;
+                                        th2[i] += a * aw;
+                                        th1[i] -= ev[i] * aw;
                                     }
-                                    const float aw = a * ww;
-                                    th2[i] += a * aw;
-                                    th1[i] -= ev[i] * aw;
                                 }
                             }
                         }
                     }
                 }
-            }
-            // fold the view groups of the warp onto group 0
-            for (int off = lprp; off < 32; off <<= 1) {
+                // fold the view groups of the warp onto group 0
+                for (int off = lprp; off < 32; off <<= 1) {
 #pragma unroll
-                for (int i = 0; i < VEC; i++) {
-                    th1[i] += __shfl_xor_sync(0xffffffffu, th1[i], off);
-                    th2[i] += __shfl_xor_sync(0xffffffffu, th2[i], off);
+                    for (int i = 0; i < VEC; i++) {
+                        th1[i] += __shfl_xor_sync(0xffffffffu, th1[i], off);
+                        th2[i] += __shfl_xor_sync(0xffffffffu, th2[i], off);
+                    }
+                }
+                if (grp == 0 && row_ok) {
+#pragma unroll
+                    for (int i = 0; i < VEC; i++) {
+                        S.th1[warp][t0 + i] = th1[i];
+                        S.th2[warp][t0 + i] = th2[i];
+                    }
                 }
             }
-            if (grp == 0 && row_ok) {
-#pragma unroll
-                for (int i = 0; i < VEC; i++) {
-                    S.th1[warp][t0 + i] = th1[i];
-                    S.th2[warp][t0 + i] = th2[i];
-                }
-            }
-        }
-        __syncthreads();
+            __syncthreads();
 
-        // ---- 3. zero-skipping and solve (warp 0, lane = slice) -------------------
-        if (warp == 0) {
-            const float V0 = V;
-            float numA = 0.0f, denA = 0.0f, t1 = 0.0f, t2 = 0.0f;
-            int pos = 0;
-            for (int w = 0; w < W; w++) {
-                numA += S.num[w][lane];
-                denA += S.den[w][lane];
-                pos |= S.pos[w][lane];
-                if (lane < NT) {
-                    t1 += S.th1[w][lane];
-                    t2 += S.th2[w][lane];
+            // ---- 3. zero-skipping and solve (warp 0, lane = slice of the chunk) ------
+            if (warp == 0) {
+                const float V0 = V;
+                float numA = 0.0f, denA = 0.0f, t1 = 0.0f, t2 = 0.0f;
+                int pos = 0;
+                for (int w = 0; w < W; w++) {
+                    numA += S.num[w][lane];
+                    denA += S.den[w][lane];
+                    pos |= S.pos[w][lane];
+                    if (lane < ct) {
+                        t1 += S.th1[w][lane];
+                        t2 += S.th2[w][lane];
+                    }
+                }
+                // in-column z - 1 / z + 1: the chunk below is already updated
+                // (Gauss-Seidel over the chunks), the chunk above not yet
+                const float edge_m = (z0 > 0) ? x[col_off + z0 - 1] : 0.0f;
+                const float edge_p = (z0 + cz < NZ) ? x[col_off + z0 + cz] : 0.0f;
+                {
+                    float vm = __shfl_up_sync(0xffffffffu, V0, 1);
+                    float vp = __shfl_down_sync(0xffffffffu, V0, 1);
+                    if (lane == 0) vm = edge_m;
+                    if (lane == cz - 1) vp = edge_p;
+                    if (z >= 1 && vm > 0.0f) pos = 1;
+                    if (z + 1 < NZ && vp > 0.0f) pos = 1;
+                }
+                const bool skip = !zl || (L.zero_skipping && L.iter > 1 && V0 == 0.0f && !pos);
+                __syncwarp();
+                S.th1[0][lane] = t1;
+                S.th2[0][lane] = t2;
+                __syncwarp();
+                float th1 = 0.0f, th2 = 0.0f;
+                if (zl)
+                    for (int r = 0; r < MZ; r++) {
+                        th1 += S.th1[0][lane * MZ + r];
+                        th2 += S.th2[0][lane * MZ + r];
+                    }
+                float cur = V0;
+#pragma unroll
+                for (int parity = 0; parity < 2; parity++) {
+                    float vm = __shfl_up_sync(0xffffffffu, cur, 1);
+                    float vp = __shfl_down_sync(0xffffffffu, cur, 1);
+                    if (lane == 0) vm = edge_m;
+                    if (lane == cz - 1) vp = edge_p;
+                    if (!skip && (z & 1) == parity) {
+                        float num = numA, den = denA;
+                        if (z >= 1) {
+                            const float cf = K.sf[0 * 9 + 4] * qg_weight(V0 - vm, K.q, K.qmp, K.issq, K.issqp, K.cs, K.bs0);
+                            num += cf * vm;
+                            den += cf;
+                        }
+                        if (z + 1 < NZ) {
+                            const float cf = K.sf[2 * 9 + 4] * qg_weight(V0 - vp, K.q, K.qmp, K.issq, K.issqp, K.cs, K.bs0);
+                            num += cf * vp;
+                            den += cf;
+                        }
+                        const float u = (num + th2 * V0 - th1) / (den + th2);
+                        cur = V0 + K.alpha * (u - V0);
+                    }
+                }
+                const float dx = skip ? 0.0f : cur - V0;
+                S.dx[lane] = dx;
+                if (zl) {
+                    if (!skip) {
+                        x[col_off + z] = cur;
+                        cnt.upd++;
+                        cnt.sum_dx += fabsf(dx);
+                        cnt.sum_x += fabsf(cur);
+                    } else {
+                        cnt.skip++;
+                    }
+                }
+                float m = fabsf(dx);
+                for (int off = 16; off > 0; off >>= 1) m += __shfl_xor_sync(0xffffffffu, m, off);
+                if (lane == 0) {
+                    float *mp = mag + (size_t)f * nxy + c;
+                    *mp = ch == 0 ? m : *mp + m;
                 }
             }
+            __syncthreads();
+
+            // ---- 4. apply e -= a dx (the next chunk's or column's barrier orders
+            //         these reductions before its theta loads) ---------------------------
             {
-                const float vm = __shfl_up_sync(0xffffffffu, V0, 1);
-                const float vp = __shfl_down_sync(0xffffffffu, V0, 1);
-                if (lane >= 1 && vm > 0.0f) pos = 1;
-                if (lane + 1 < NZ && vp > 0.0f) pos = 1;
-            }
-            const bool skip = !zl || (L.zero_skipping && L.iter > 1 && V0 == 0.0f && !pos);
-            __syncwarp();
-            S.th1[0][lane] = t1;
-            S.th2[0][lane] = t2;
-            __syncwarp();
-            float th1 = 0.0f, th2 = 0.0f;
-            if (zl)
-                for (int r = 0; r < MZ; r++) {
-                    th1 += S.th1[0][lane * MZ + r];
-                    th2 += S.th2[0][lane * MZ + r];
+                float dxv[VEC];
+                bool any = false;
+#pragma unroll
+                for (int i = 0; i < VEC; i++) {
+                    dxv[i] = row_ok ? S.dx[(t0 + i) / MZ] : 0.0f;
+                    any |= dxv[i] != 0.0f;
                 }
-            float cur = V0;
+                if (any) {
+                    for (int v0 = gfirst; v0 < nv; v0 += kUnroll * gstride) {
+                        Rec<KW> R[kUnroll];
 #pragma unroll
-            for (int parity = 0; parity < 2; parity++) {
-                const float vm = __shfl_up_sync(0xffffffffu, cur, 1);
-                const float vp = __shfl_down_sync(0xffffffffu, cur, 1);
-                if (!skip && (lane & 1) == parity) {
-                    float num = numA, den = denA;
-                    if (lane >= 1) {
-                        const float cf = K.sf[0 * 9 + 4] * qg_weight(V0 - vm, K.q, K.qmp, K.issq, K.issqp, K.cs, K.bs0);
-                        num += cf * vm;
-                        den += cf;
-                    }
-                    if (lane + 1 < NZ) {
-                        const float cf = K.sf[2 * 9 + 4] * qg_weight(V0 - vp, K.q, K.qmp, K.issq, K.issqp, K.cs, K.bs0);
-                        num += cf * vp;
-                        den += cf;
-                    }
-                    const float u = (num + th2 * V0 - th1) / (den + th2);
-                    cur = V0 + K.alpha * (u - V0);
-                }
-            }
-            const float dx = skip ? 0.0f : cur - V0;
-            S.dx[lane] = dx;
-            if (zl) {
-                if (!skip) {
-                    x[col_off + lane] = cur;
-                    cnt.upd++;
-                    cnt.sum_dx += fabsf(dx);
-                    cnt.sum_x += fabsf(cur);
-                } else {
-                    cnt.skip++;
-                }
-            }
-            float m = fabsf(dx);
-            for (int off = 16; off > 0; off >>= 1) m += __shfl_xor_sync(0xffffffffu, m, off);
-            if (lane == 0) mag[(size_t)f * nxy + c] = m;
-        }
-        __syncthreads();
-
-        // ---- 4. apply e -= a dx (the next column's barrier orders these
-        //         reductions before its theta loads) --------------------------------
-        {
-            float dxv[VEC];
-            bool any = false;
+                        for (int u = 0; u < kUnroll; u++) {
+                            const int v = v0 + u * gstride;
+                            if (v < nv) R[u] = kStaged ? load_rec_smem<KW>(col_rec + (size_t)v * RW)
+                                                   : load_rec<KW>(col_rec + (size_t)v * RW);
+                            else R[u].w[0].x = 0u;
+                        }
 #pragma unroll
-            for (int i = 0; i < VEC; i++) {
-                dxv[i] = row_ok ? S.dx[(t0 + i) / MZ] : 0.0f;
-                any |= dxv[i] != 0.0f;
-            }
-            if (any) {
-                for (int v0 = gfirst; v0 < nv; v0 += kUnroll * gstride) {
-                    Rec<KW> R[kUnroll];
+                        for (int u = 0; u < kUnroll; u++) {
+                            const uint32_t hdr = R[u].w[0].x;
+                            const int cnt_q = hdr >> 24;
+                            const unsigned sb = (hdr & 0xFFFFFFu) * (unsigned)NT + (unsigned)(rbase + t0);
 #pragma unroll
-                    for (int u = 0; u < kUnroll; u++) {
-                        const int v = v0 + u * gstride;
-                        if (v < nv) R[u] = kStaged ? load_rec_smem<KW>(col_rec + (size_t)v * RW)
-                                               : load_rec<KW>(col_rec + (size_t)v * RW);
-                        else R[u].w[0].x = 0u;
-                    }
+                            for (int q = 0; q < 4 * KW - 1; q++) {
+                                if (q < cnt_q) {
+                                    const float a = -(rec_val<KW>(R[u], q) * K.dt);
+                                    float d[VEC];
 #pragma unroll
-                    for (int u = 0; u < kUnroll; u++) {
-                        const uint32_t hdr = R[u].w[0].x;
-                        const int cnt_q = hdr >> 24;
-                        // sinogram rows stay below 2^24 and N_t <= 32: 32-bit offsets
-                        const unsigned sb = (hdr & 0xFFFFFFu) * (unsigned)NT + (unsigned)t0;
-#pragma unroll
-                        for (int q = 0; q < 4 * KW - 1; q++) {
-                            if (q < cnt_q) {
-                                const float a = -(rec_val<KW>(R[u], q) * K.dt);
-                                float d[VEC];
-#pragma unroll
-                                for (int i = 0; i < VEC; i++) d[i] = a * dxv[i];
-                                red_add(err + (sb + (unsigned)(q * NT)), d);
+                                    for (int i = 0; i < VEC; i++) d[i] = a * dxv[i];
+                                    red_add(err + (sb + (unsigned)(q * NT)), d);
+                                }
                             }
                         }
                     }
@@ -561,7 +594,7 @@ __device__ __forceinline__ void icd_update_sv(const Geom &g, const IcdLaunch &L,
 // One colour phase of one problem: persistent CTAs drain the phase's SV queue.
 // With kStaged, the dynamic shared memory holds two record buffers of
 // stage_words words each (the current and the next column's A records).
-template <int KW, int kUnroll, int VEC, bool kStaged>
+template <int KW, int kUnroll, int VEC, bool kStaged, int kHuber>
 __global__ void __launch_bounds__(kMaxWarps * 32, 4) icd_phase_kernel(
     Geom g, IcdLaunch L, IcdConst K, const uint32_t *__restrict__ table, const int32_t *__restrict__ view_first,
     const uint8_t *__restrict__ mask, float *__restrict__ x, float *__restrict__ err, const float *__restrict__ wgt,
@@ -602,7 +635,7 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 4) icd_phase_kernel(
             sy = KC * (rem / hx) + color / KC;
         }
         if (sx >= L.n_sv_x || sy >= L.n_sv_y) continue;  // uniform
-        icd_update_sv<KW, kUnroll, VEC, kStaged>(g, L, K, table, view_first, mask, x, err, wgt, mag, f, sx, sy, S,
+        icd_update_sv<KW, kUnroll, VEC, kStaged, kHuber>(g, L, K, table, view_first, mask, x, err, wgt, mag, f, sx, sy, S,
                                                  cnt, s_rec, stage_words);
     }
     // after an abort, the late copy may still write into this CTA's shared
@@ -615,7 +648,7 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 4) icd_phase_kernel(
 // above this size the sweep reads records from global memory instead.
 constexpr int kMaxStageBytes = 16 * 1024;
 
-template <int KW, int U, int VEC, bool kStaged>
+template <int KW, int U, int VEC, bool kStaged, int kHuber>
 static void launch_staged(const Geom &g, const IcdLaunch &L, const IcdConst &K, const uint32_t *d_table,
                           const int32_t *d_view_first, const uint8_t *d_mask, float *d_x, float *d_err,
                           const float *d_w, float *d_mag, IcdStats *d_stats, unsigned int *d_queue, int stage_words,
@@ -626,12 +659,13 @@ static void launch_staged(const Geom &g, const IcdLaunch &L, const IcdConst &K, 
     int dev = 0, sms = 148, per_sm = 1;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, icd_phase_kernel<KW, U, VEC, kStaged>, threads, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, icd_phase_kernel<KW, U, VEC, kStaged, kHuber>, threads,
+                                                  smem);
     const long long items = (long long)g.N_time * sv_slots(g.N_x, g.N_y, L.sv, L.colors_k);
     long long grid = (long long)sms * (per_sm > 0 ? per_sm : 1);
     if (grid > items) grid = items;
     if (L.max_ctas > 0 && grid > L.max_ctas) grid = L.max_ctas;
-    icd_phase_kernel<KW, U, VEC, kStaged><<<(unsigned)grid, threads, smem, st>>>(
+    icd_phase_kernel<KW, U, VEC, kStaged, kHuber><<<(unsigned)grid, threads, smem, st>>>(
         g, L, K, d_table, d_view_first, d_mask, d_x, d_err, d_w, d_mag, d_stats, d_queue, stage_words);
 }
 
@@ -641,12 +675,18 @@ static void launch_kw(const Geom &g, const IcdLaunch &L, const IcdConst &K, cons
                       float *d_mag, IcdStats *d_stats, unsigned int *d_queue, cudaStream_t st)
 {
     const int stage_words = g.max_views * g.rec_words;  // a multiple of 4 words: 16-byte aligned buffers
-    if (L.stage_records && 2 * (size_t)stage_words * sizeof(uint32_t) <= (size_t)kMaxStageBytes)
-        launch_staged<KW, U, VEC, true>(g, L, K, d_table, d_view_first, d_mask, d_x, d_err, d_w, d_mag, d_stats,
-                                        d_queue, stage_words, st);
-    else
-        launch_staged<KW, U, VEC, false>(g, L, K, d_table, d_view_first, d_mask, d_x, d_err, d_w, d_mag, d_stats,
-                                         d_queue, 0, st);
+    const bool staged = L.stage_records && 2 * (size_t)stage_words * sizeof(uint32_t) <= (size_t)kMaxStageBytes;
+#define MBIR_STAGED(S, H)                                                                                         \
+    launch_staged<KW, U, VEC, S, H>(g, L, K, d_table, d_view_first, d_mask, d_x, d_err, d_w, d_mag, d_stats, d_queue, \
+                                    S ? stage_words : 0, st)
+    if (staged) {
+        if (K.huber) MBIR_STAGED(true, 1);
+        else MBIR_STAGED(true, 0);
+    } else {
+        if (K.huber) MBIR_STAGED(false, 1);
+        else MBIR_STAGED(false, 0);
+    }
+#undef MBIR_STAGED
 }
 
 IcdConst make_icd_const(const Geom &g)
@@ -746,7 +786,7 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 4) icd_batch_kernel(const Batc
         const int sx = K * (rem % hx) + color % K;
         const int sy = K * (rem / hx) + color / K;
         if (sx >= P.L.n_sv_x || sy >= P.L.n_sv_y) continue;
-        icd_update_sv<KW, kUnroll, VEC, false>(P.g, P.L, P.K, P.table, P.view_first, P.mask, P.x, P.err, P.w, P.mag,
+        icd_update_sv<KW, kUnroll, VEC, false, 2>(P.g, P.L, P.K, P.table, P.view_first, P.mask, P.x, P.err, P.w, P.mag,
                                                f, sx, sy, S, cnt, nullptr, 0);
     }
     if (cur >= 0) flush_counts(cnt, P.stats);
@@ -798,7 +838,7 @@ int icd_grid(int warps)
     int dev = 0, sms = 148, per_sm = 1;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, icd_phase_kernel<1, 2, 4, false>, warps * 32, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, icd_phase_kernel<1, 2, 4, false, 0>, warps * 32, 0);
     return sms * (per_sm > 0 ? per_sm : 1);
 }
 

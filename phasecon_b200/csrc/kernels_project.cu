@@ -59,21 +59,26 @@ void launch_zfast_to_vol(const float *in, float *out, int N_time, int N_z, int N
     transpose_rows_cols<<<grid, block, 0, st>>>(in, out, nxy, N_z);
 }
 
-// One warp per (frame, voxel column), lane = detector row: every A entry of
-// the column adds a * x into an FP64 accumulator image of the sinogram with a
-// global FP64 reduction (red.global.add.f64, performed in L2). Columns whose
-// voxels are all zero are skipped.
+// One warp per (frame, voxel column, chunk of 32 detector rows), lane =
+// detector row: every A entry of the column adds a * x into an FP64
+// accumulator image of the sinogram with a global FP64 reduction
+// (red.global.add.f64, performed in L2). Columns whose voxels are all zero are
+// skipped.
 __global__ void __launch_bounds__(256) forward_project_kernel(Geom g, const uint32_t *__restrict__ table,
                                                              const int32_t *__restrict__ view_first,
                                                              const float *__restrict__ x, double *__restrict__ acc)
 {
     const int nxy = g.N_x * g.N_y;
+    const int n_chunks = (g.N_t + kRowChunk - 1) / kRowChunk;
     const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
-    if (gw >= (long long)g.N_time * nxy) return;
-    const int f = (int)(gw / nxy), c = (int)(gw - (long long)f * nxy);
-    const bool row_ok = lane < g.N_t;
-    const double xv = row_ok ? (double)__ldg(x + ((size_t)f * nxy + c) * g.N_z + lane / g.z_overlap) : 0.0;
+    if (gw >= (long long)g.N_time * nxy * n_chunks) return;
+    const int ch = (int)(gw % n_chunks);
+    const long long fc = gw / n_chunks;
+    const int f = (int)(fc / nxy), c = (int)(fc - (long long)f * nxy);
+    const int t = ch * kRowChunk + lane;  // this lane's detector row
+    const bool row_ok = t < g.N_t;
+    const double xv = row_ok ? (double)__ldg(x + ((size_t)f * nxy + c) * g.N_z + t / g.z_overlap) : 0.0;
     if (__all_sync(0xffffffffu, xv == 0.0)) return;
     const int fv0 = view_first[f], nv = view_first[f + 1] - fv0;
     const uint32_t *rec = table + ((size_t)fv0 * nxy + (size_t)c * nv) * g.rec_words;
@@ -88,7 +93,7 @@ __global__ void __launch_bounds__(256) forward_project_kernel(Geom g, const uint
             const int cnt = hdr[u] >> 24, row = hdr[u] & 0xFFFFFF;
             const uint32_t *r = rec + (size_t)(v0 + u) * g.rec_words + 1;
             for (int q = 0; q < cnt; q++)
-                atomicAdd(acc + (size_t)(row + q) * g.N_t + lane, xv * (double)__uint_as_float(__ldg(r + q)));
+                atomicAdd(acc + (size_t)(row + q) * g.N_t + t, xv * (double)__uint_as_float(__ldg(r + q)));
         }
     }
 }
@@ -112,7 +117,7 @@ void launch_forward_project(const Geom &g, const uint32_t *d_table, const int32_
 {
     const size_t n = (size_t)g.N_p * g.N_r * g.N_t;
     cudaMemsetAsync(d_acc, 0, n * sizeof(double), st);
-    const long long warps = (long long)g.N_time * g.N_x * g.N_y;
+    const long long warps = (long long)g.N_time * g.N_x * g.N_y * ((g.N_t + kRowChunk - 1) / kRowChunk);
     const long long blocks = (warps * 32 + 255) / 256;
     forward_project_kernel<<<(unsigned)blocks, 256, 0, st>>>(g, d_table, d_view_first, d_x, d_acc);
     finish_projection_kernel<<<148 * 8, 256, 0, st>>>(n, d_acc, d_y, d_out, d_off, g.N_r * g.N_t);
@@ -240,38 +245,44 @@ bool launch_forward_project_views(const Geom &g, const uint32_t *d_table, const 
     return launch_views_g<1>(g, d_table, d_view_first, d_views, d_view_frame, n_assigned, d_x, d_y, d_out, st, d_off);
 }
 
-// One warp per (frame, column); out is [N_time][N_y][N_x][N_z].
+// One warp per (frame, column, chunk of 32 detector rows); out is
+// [N_time][N_y][N_x][N_z].
 __global__ void back_project_kernel(Geom g, const uint32_t *__restrict__ table,
                                     const int32_t *__restrict__ view_first, const int32_t *__restrict__ views,
                                     const float *__restrict__ sino, float *__restrict__ out)
 {
     const int nxy = g.N_x * g.N_y;
+    const int n_chunks = (g.N_t + kRowChunk - 1) / kRowChunk;
     const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
-    if (gw >= (long long)g.N_time * nxy) return;
-    const int f = (int)(gw / nxy), c = (int)(gw - (long long)f * nxy);
+    if (gw >= (long long)g.N_time * nxy * n_chunks) return;
+    const int ch = (int)(gw % n_chunks);
+    const long long fc = gw / n_chunks;
+    const int f = (int)(fc / nxy), c = (int)(fc - (long long)f * nxy);
+    const int t = ch * kRowChunk + lane;  // this lane's detector row
     const int fv0 = view_first[f], nv = view_first[f + 1] - fv0;
     const uint32_t *rec = table + ((size_t)fv0 * nxy + (size_t)c * nv) * g.rec_words;
     double acc = 0.0;
-    if (lane < g.N_t) {
+    if (t < g.N_t) {
         for (int v = 0; v < nv; v++, rec += g.rec_words) {
             const uint32_t hdr = __ldg(rec);
             const int cnt = hdr >> 24, row = hdr & 0xFFFFFF;
             for (int q = 0; q < cnt; q++) {
                 const double a = (double)__uint_as_float(__ldg(rec + 1 + q));
-                acc += a * (double)__ldg(sino + ((size_t)row + q) * g.N_t + lane);
+                acc += a * (double)__ldg(sino + ((size_t)row + q) * g.N_t + t);
             }
         }
     }
+    // rows of one voxel slice are z_overlap consecutive lanes (32 is a multiple of z_overlap)
     for (int off = 1; off < g.z_overlap; off <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
-    if (lane < g.N_t && lane % g.z_overlap == 0)
-        out[((size_t)f * nxy + c) * g.N_z + lane / g.z_overlap] = (float)acc;
+    if (t < g.N_t && t % g.z_overlap == 0)
+        out[((size_t)f * nxy + c) * g.N_z + t / g.z_overlap] = (float)acc;
 }
 
 void launch_back_project(const Geom &g, const uint32_t *d_table, const int32_t *d_view_first,
                          const int32_t *d_views, const float *d_sino, float *d_x, cudaStream_t st)
 {
-    const long long warps = (long long)g.N_time * g.N_x * g.N_y;
+    const long long warps = (long long)g.N_time * g.N_x * g.N_y * ((g.N_t + kRowChunk - 1) / kRowChunk);
     const int threads = 256;
     const long long blocks = (warps * 32 + threads - 1) / threads;
     back_project_kernel<<<(unsigned)blocks, threads, 0, st>>>(g, d_table, d_view_first, d_views, d_sino, d_x);

@@ -12,7 +12,7 @@ namespace mbirgpu {
 
 constexpr int kRespBins = 64;  // DETECTOR_RESPONSE_BINS, MBIR_4D/XT_Constants.h:79
 constexpr int kMaxKmax = 9;    // channels per (column, view) at voxel scale 4: 2*4+1
-constexpr int kMaxNt = 32;     // detector rows handled by the lane-per-row kernels
+constexpr int kRowChunk = 32;  // detector rows one warp covers (lane = row); taller columns are chunked
 
 // One stage's geometry and prior constants, passed by value to kernels.
 // Field meanings follow Sinogram / ScannedObject / TomoInputs of

@@ -235,3 +235,24 @@ def test_phcontomo_reconstruct_matches_reference_files(tmp_path):
         a, b = load(gdir, name), load(rdir, name)
         assert a.shape == b.shape, name
         assert np.sqrt(np.mean((a - b) ** 2)) <= 1e-3 * (b.max() - b.min()), name
+
+
+def test_colour_class_sweep_reaches_the_raster_cost():
+    """The Nelder-Mead proximal sweep in colour classes (four launches, no two
+    8-neighbours in one class) against the reference's raster order (the
+    wavefront kernel): the full per-view ADMM, 20 phase-retrieval iterations
+    from the Paganin start on 6 views of 64 x 64, ends at the same
+    phase-retrieval cost per view within 1e-3 relative (the orders differ, so
+    the cost -- the quantity the method minimises -- is the parity measure)."""
+    V, R, C = 6, 64, 64
+    pb, g, y, D, zt = scan(V, R, C, seed=61)
+    finals = []
+    for order in (0, 1):
+        s = PcSession(pb, default_options(pret_max_iter=20, nms_order=order))
+        s.paganin()
+        s.init_admm()
+        costs, iters, _ = s.run()
+        finals.append(np.array([c[np.isfinite(c)][-1] for c in costs]))
+        s.close()
+    raster, colour = finals
+    assert np.all(np.abs(colour - raster) / np.abs(raster) < 1e-3), (raster, colour)
