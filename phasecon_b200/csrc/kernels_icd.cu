@@ -235,6 +235,54 @@ __device__ __forceinline__ void flush_counts(IcdCount &cnt, IcdStats *stats)
     cnt.phases = phases;
 }
 
+// theta1 / theta2 partial sums of one lane (VEC detector rows starting at
+// sinogram row offset `row0` within each A entry's row, views gfirst,
+// gfirst + gstride, ... of the column): theta1 = -sum a w e,
+// theta2 = sum a^2 w with a = A value x delta_t (XT_VoxUpdate.c:56-85).
+template <int KW, int kUnroll, int VEC, bool kStaged, int kHuber>
+__device__ __forceinline__ void theta_pass(const IcdConst &K, const uint32_t *col_rec, const float *__restrict__ err,
+                                           const float *__restrict__ wgt, int gfirst, int gstride, int nv, int RW,
+                                           int NT, int row0, float (&th1)[VEC], float (&th2)[VEC])
+{
+    using VT = typename VecF<VEC>::T;
+    for (int v0 = gfirst; v0 < nv; v0 += kUnroll * gstride) {
+        Rec<KW> R[kUnroll];
+#pragma unroll
+        for (int u = 0; u < kUnroll; u++) {
+            const int v = v0 + u * gstride;
+            if (v < nv) R[u] = kStaged ? load_rec_smem<KW>(col_rec + (size_t)v * RW) : load_rec<KW>(col_rec + (size_t)v * RW);
+            else R[u].w[0].x = 0u;
+        }
+#pragma unroll
+        for (int u = 0; u < kUnroll; u++) {
+            const uint32_t hdr = R[u].w[0].x;
+            const int cnt_q = hdr >> 24;
+            // sinogram rows stay below 2^24 and N_t rows each: 32-bit offsets
+            const unsigned sb = (hdr & 0xFFFFFFu) * (unsigned)NT + (unsigned)row0;
+#pragma unroll
+            for (int q = 0; q < 4 * KW - 1; q++) {
+                if (q < cnt_q) {
+                    float ev[VEC], wv[VEC];
+                    VecF<VEC>::get(__ldcg(reinterpret_cast<const VT *>(err + (sb + (unsigned)(q * NT)))), ev);
+                    VecF<VEC>::get(__ldg(reinterpret_cast<const VT *>(wgt + (sb + (unsigned)(q * NT)))), wv);
+                    const float a = rec_val<KW>(R[u], q) * K.dt;
+#pragma unroll
+                    for (int i = 0; i < VEC; i++) {
+                        float ww = wv[i];
+                        if (kHuber == 1 || (kHuber == 2 && K.huber)) {
+                            const float sw = sqrtf(ww);
+                            if (!(fabsf(ev[i] * sw) < K.huber_T)) ww = K.huber_T * K.huber_delta * sw / fabsf(ev[i]);
+                        }
+                        const float aw = a * ww;
+                        th2[i] += a * aw;
+                        th1[i] -= ev[i] * aw;
+                    }
+                }
+            }
+        }
+    }
+}
+
 // Update the voxel columns of super-voxel (sx, sy) of frame f; the whole CTA
 // cooperates (see the file comment for the four passes per column).
 // KW: 16-byte words per A record (1, 2, 3 for voxel scale 1, 2, 4);
@@ -246,7 +294,9 @@ __device__ __forceinline__ void flush_counts(IcdCount &cnt, IcdStats *stats)
 // round trip per view group instead of two and the apply pass on none.
 // kHuber: 0 the quadratic data term, 1 the generalised Huber one
 // (XT_VoxUpdate.c:68-82), 2 decided per problem at run time (K.huber).
-template <int KW, int kUnroll, int VEC, bool kStaged, int kHuber>
+// kOverlap: warp 0 gathers the prior neighbourhood while warps 1..W-1 run the
+// theta pass (used when the launch has at least 2 warps).
+template <int KW, int kUnroll, int VEC, bool kStaged, int kHuber, bool kOverlap>
 __device__ __forceinline__ void icd_update_sv(const Geom &g, const IcdLaunch &L, const IcdConst &K,
                                               const uint32_t *__restrict__ table,
                                               const int32_t *__restrict__ view_first,
@@ -273,8 +323,13 @@ __device__ __forceinline__ void icd_update_sv(const Geom &g, const IcdLaunch &L,
     const int G = 32 / lprp;  // view groups per warp
     const int grp = lane / lprp, tq = lane % lprp;
     const int t0 = tq * VEC;  // first detector row of this lane within the chunk
-    const int gstride = W * G;
-    const int gfirst = warp * G + grp;
+    // overlap mode: warp 0 gathers the prior neighbourhood of the column while
+    // warps 1..W-1 run the theta pass (independent work), so theta is split
+    // over W - 1 warps and the neighbourhood needs no cross-warp sum
+    const bool ovl = kOverlap && W >= 2;
+    const int tw = ovl ? W - 1 : W, twarp = ovl ? warp - 1 : warp;  // theta warps, this warp's rank
+    const int gstride = tw * G;
+    const int gfirst = twarp * G + grp;
     const int fv0 = view_first[f], nv = view_first[f + 1] - fv0;
 
     // ---- the SV's columns inside the reconstruction circle, shuffled ----------
@@ -330,13 +385,28 @@ __device__ __forceinline__ void icd_update_sv(const Geom &g, const IcdLaunch &L,
             const int z = z0 + lane;                                 // this lane's slice
             const bool row_ok = tq < ct / VEC;
 
-            // ---- 1. neighbourhood (sources split over warps) + column activity ------
+            // overlap mode: the previous chunk's / column's apply pass is complete
+            // before this theta pass reads e (the neighbourhood barrier below
+            // comes after theta in that mode)
+            if (ovl) __syncthreads();
+
+            // ---- 1. neighbourhood (sources split over warps, or all on warp 0) ----
             int active_pred;
             const float V = zl ? x[col_off + z] : 0.0f;  // the column itself (warp 0 reuses it in the solve)
+            float th1[VEC], th2[VEC];
+#pragma unroll
+            for (int i = 0; i < VEC; i++) th1[i] = th2[i] = 0.0f;
+            if (kStaged && ch == 0 && ovl)  // issued one column earlier; theta reads it next
+                wait_staged(&S.stage_bar[ci & 1], cnt.phases, ci & 1, cnt.timeouts, S.abort, S.abort_bar,
+                            S.abort_parity);
+            if (ovl && warp > 0 && row_ok)
+                theta_pass<KW, kUnroll, VEC, kStaged, kHuber>(K, col_rec, err, wgt, gfirst, gstride, nv, RW, NT,
+                                                             rbase + t0, th1, th2);
             {
                 float num = 0.0f, den = 0.0f;
                 int pos = 0;
-                for (int s = warp; s < 10; s += W) {
+                const int s_first = ovl ? (warp == 0 ? 0 : 10) : warp, s_step = ovl ? 1 : W;
+                for (int s = s_first; s < 10; s += s_step) {
                     if (s < 8) {
                         const int o = s < 4 ? s : s + 1;  // skip the centre of the 3x3
                         const int dy = o / 3 - 1, dx = o % 3 - 1;
@@ -381,8 +451,9 @@ __device__ __forceinline__ void icd_update_sv(const Geom &g, const IcdLaunch &L,
                 // a column is skipped only if every slice is zero with no positive
                 // neighbour (in-column neighbours are the column's own values)
                 active_pred = !L.zero_skipping || L.iter <= 1 || (zl && V != 0.0f) || pos;
+                if (ovl && warp > 0) active_pred = 0;  // only warp 0 saw the neighbourhood
             }
-            if (kStaged && ch == 0)  // issued one column earlier
+            if (kStaged && ch == 0 && !ovl)  // issued one column earlier
                 wait_staged(&S.stage_bar[ci & 1], cnt.phases, ci & 1, cnt.timeouts, S.abort, S.abort_bar,
                             S.abort_parity);
             const int any_active = __syncthreads_or(active_pred);
@@ -403,50 +474,11 @@ __device__ __forceinline__ void icd_update_sv(const Geom &g, const IcdLaunch &L,
                 continue;  // uniform across the CTA
             }
 
-            // ---- 2. theta over the column's views -----------------------------------
+            // ---- 2. theta over the column's views (already done in overlap mode) ---
             {
-                float th1[VEC], th2[VEC];
-#pragma unroll
-                for (int i = 0; i < VEC; i++) th1[i] = th2[i] = 0.0f;
-                if (row_ok) {
-                    for (int v0 = gfirst; v0 < nv; v0 += kUnroll * gstride) {
-                        Rec<KW> R[kUnroll];
-#pragma unroll
-                        for (int u = 0; u < kUnroll; u++) {
-                            const int v = v0 + u * gstride;
-                            if (v < nv) R[u] = kStaged ? load_rec_smem<KW>(col_rec + (size_t)v * RW)
-                                                   : load_rec<KW>(col_rec + (size_t)v * RW);
-                            else R[u].w[0].x = 0u;
-                        }
-#pragma unroll
-                        for (int u = 0; u < kUnroll; u++) {
-                            const uint32_t hdr = R[u].w[0].x;
-                            const int cnt_q = hdr >> 24;
-                            // sinogram rows stay below 2^24 and N_t rows each: 32-bit offsets
-                            const unsigned sb = (hdr & 0xFFFFFFu) * (unsigned)NT + (unsigned)(rbase + t0);
-#pragma unroll
-                            for (int q = 0; q < 4 * KW - 1; q++) {
-                                if (q < cnt_q) {
-                                    float ev[VEC], wv[VEC];
-                                    VecF<VEC>::get(__ldcg(reinterpret_cast<const VT *>(err + (sb + (unsigned)(q * NT)))), ev);
-                                    VecF<VEC>::get(__ldg(reinterpret_cast<const VT *>(wgt + (sb + (unsigned)(q * NT)))), wv);
-                                    const float a = rec_val<KW>(R[u], q) * K.dt;
-#pragma unroll
-                                    for (int i = 0; i < VEC; i++) {
-                                        float ww = wv[i];
-                                        if (kHuber == 1 || (kHuber == 2 && K.huber)) {
-                                            const float sw = sqrtf(ww);
-                                            if (!(fabsf(ev[i] * sw) < K.huber_T)) ww = K.huber_T * K.huber_delta * sw / fabsf(ev[i]);
-                                        }
-                                        const float aw = a * ww;
-                                        th2[i] += a * aw;
-                                        th1[i] -= ev[i] * aw;
-                                    }
-                                }
-                            }
-                        }
-                    }
-                }
+                if (!ovl && row_ok)
+                    theta_pass<KW, kUnroll, VEC, kStaged, kHuber>(K, col_rec, err, wgt, gfirst, gstride, nv, RW, NT,
+                                                                 rbase + t0, th1, th2);
                 // fold the view groups of the warp onto group 0
                 for (int off = lprp; off < 32; off <<= 1) {
 #pragma unroll
@@ -455,7 +487,7 @@ __device__ __forceinline__ void icd_update_sv(const Geom &g, const IcdLaunch &L,
                         th2[i] += __shfl_xor_sync(0xffffffffu, th2[i], off);
                     }
                 }
-                if (grp == 0 && row_ok) {
+                if (grp == 0 && row_ok && !(ovl && warp == 0)) {
 #pragma unroll
                     for (int i = 0; i < VEC; i++) {
                         S.th1[warp][t0 + i] = th1[i];
@@ -463,7 +495,7 @@ __device__ __forceinline__ void icd_update_sv(const Geom &g, const IcdLaunch &L,
                     }
                 }
             }
-            __syncthreads();
+            if (!ovl) __syncthreads();  // in overlap mode theta finished before the neighbourhood barrier
 
             // ---- 3. zero-skipping and solve (warp 0, lane = slice of the chunk) ------
             if (warp == 0) {
@@ -471,10 +503,12 @@ __device__ __forceinline__ void icd_update_sv(const Geom &g, const IcdLaunch &L,
                 float numA = 0.0f, denA = 0.0f, t1 = 0.0f, t2 = 0.0f;
                 int pos = 0;
                 for (int w = 0; w < W; w++) {
-                    numA += S.num[w][lane];
-                    denA += S.den[w][lane];
-                    pos |= S.pos[w][lane];
-                    if (lane < ct) {
+                    if (!ovl || w == 0) {
+                        numA += S.num[w][lane];
+                        denA += S.den[w][lane];
+                        pos |= S.pos[w][lane];
+                    }
+                    if (lane < ct && !(ovl && w == 0)) {
                         t1 += S.th1[w][lane];
                         t2 += S.th2[w][lane];
                     }
@@ -594,8 +628,8 @@ __device__ __forceinline__ void icd_update_sv(const Geom &g, const IcdLaunch &L,
 // One colour phase of one problem: persistent CTAs drain the phase's SV queue.
 // With kStaged, the dynamic shared memory holds two record buffers of
 // stage_words words each (the current and the next column's A records).
-template <int KW, int kUnroll, int VEC, bool kStaged, int kHuber>
-__global__ void __launch_bounds__(kMaxWarps * 32, 4) icd_phase_kernel(
+template <int KW, int kUnroll, int VEC, bool kStaged, int kHuber, bool kOverlap>
+__global__ void __launch_bounds__(kMaxWarps * 32, kOverlap ? 3 : 4) icd_phase_kernel(
     Geom g, IcdLaunch L, IcdConst K, const uint32_t *__restrict__ table, const int32_t *__restrict__ view_first,
     const uint8_t *__restrict__ mask, float *__restrict__ x, float *__restrict__ err, const float *__restrict__ wgt,
     float *__restrict__ mag, IcdStats *__restrict__ stats, unsigned int *__restrict__ queue, int stage_words)
@@ -635,7 +669,8 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 4) icd_phase_kernel(
             sy = KC * (rem / hx) + color / KC;
         }
         if (sx >= L.n_sv_x || sy >= L.n_sv_y) continue;  // uniform
-        icd_update_sv<KW, kUnroll, VEC, kStaged, kHuber>(g, L, K, table, view_first, mask, x, err, wgt, mag, f, sx, sy, S,
+        icd_update_sv<KW, kUnroll, VEC, kStaged, kHuber, kOverlap>(g, L, K, table, view_first, mask, x, err, wgt, mag, f,
+                                                                   sx, sy, S,
                                                  cnt, s_rec, stage_words);
     }
     // after an abort, the late copy may still write into this CTA's shared
@@ -648,7 +683,7 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 4) icd_phase_kernel(
 // above this size the sweep reads records from global memory instead.
 constexpr int kMaxStageBytes = 16 * 1024;
 
-template <int KW, int U, int VEC, bool kStaged, int kHuber>
+template <int KW, int U, int VEC, bool kStaged, int kHuber, bool kOverlap>
 static void launch_staged(const Geom &g, const IcdLaunch &L, const IcdConst &K, const uint32_t *d_table,
                           const int32_t *d_view_first, const uint8_t *d_mask, float *d_x, float *d_err,
                           const float *d_w, float *d_mag, IcdStats *d_stats, unsigned int *d_queue, int stage_words,
@@ -659,13 +694,14 @@ static void launch_staged(const Geom &g, const IcdLaunch &L, const IcdConst &K, 
     int dev = 0, sms = 148, per_sm = 1;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, icd_phase_kernel<KW, U, VEC, kStaged, kHuber>, threads,
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, icd_phase_kernel<KW, U, VEC, kStaged, kHuber, kOverlap>,
+                                                  threads,
                                                   smem);
     const long long items = (long long)g.N_time * sv_slots(g.N_x, g.N_y, L.sv, L.colors_k);
     long long grid = (long long)sms * (per_sm > 0 ? per_sm : 1);
     if (grid > items) grid = items;
     if (L.max_ctas > 0 && grid > L.max_ctas) grid = L.max_ctas;
-    icd_phase_kernel<KW, U, VEC, kStaged, kHuber><<<(unsigned)grid, threads, smem, st>>>(
+    icd_phase_kernel<KW, U, VEC, kStaged, kHuber, kOverlap><<<(unsigned)grid, threads, smem, st>>>(
         g, L, K, d_table, d_view_first, d_mask, d_x, d_err, d_w, d_mag, d_stats, d_queue, stage_words);
 }
 
@@ -676,15 +712,20 @@ static void launch_kw(const Geom &g, const IcdLaunch &L, const IcdConst &K, cons
 {
     const int stage_words = g.max_views * g.rec_words;  // a multiple of 4 words: 16-byte aligned buffers
     const bool staged = L.stage_records && 2 * (size_t)stage_words * sizeof(uint32_t) <= (size_t)kMaxStageBytes;
-#define MBIR_STAGED(S, H)                                                                                         \
-    launch_staged<KW, U, VEC, S, H>(g, L, K, d_table, d_view_first, d_mask, d_x, d_err, d_w, d_mag, d_stats, d_queue, \
-                                    S ? stage_words : 0, st)
-    if (staged) {
-        if (K.huber) MBIR_STAGED(true, 1);
-        else MBIR_STAGED(true, 0);
+#define MBIR_STAGED(S, H, O)                                                                                      \
+    launch_staged<KW, U, VEC, S, H, O>(g, L, K, d_table, d_view_first, d_mask, d_x, d_err, d_w, d_mag, d_stats,       \
+                                       d_queue, S ? stage_words : 0, st)
+    // the overlapped column update is built for the staged single-record-word
+    // sweep (voxel scale 1, the common case)
+    if (staged && KW == 1 && L.overlap && L.warps >= 2) {
+        if (K.huber) MBIR_STAGED(true, 1, true);
+        else MBIR_STAGED(true, 0, true);
+    } else if (staged) {
+        if (K.huber) MBIR_STAGED(true, 1, false);
+        else MBIR_STAGED(true, 0, false);
     } else {
-        if (K.huber) MBIR_STAGED(false, 1);
-        else MBIR_STAGED(false, 0);
+        if (K.huber) MBIR_STAGED(false, 1, false);
+        else MBIR_STAGED(false, 0, false);
     }
 #undef MBIR_STAGED
 }
@@ -786,7 +827,7 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 4) icd_batch_kernel(const Batc
         const int sx = K * (rem % hx) + color % K;
         const int sy = K * (rem / hx) + color / K;
         if (sx >= P.L.n_sv_x || sy >= P.L.n_sv_y) continue;
-        icd_update_sv<KW, kUnroll, VEC, false, 2>(P.g, P.L, P.K, P.table, P.view_first, P.mask, P.x, P.err, P.w, P.mag,
+        icd_update_sv<KW, kUnroll, VEC, false, 2, false>(P.g, P.L, P.K, P.table, P.view_first, P.mask, P.x, P.err, P.w, P.mag,
                                                f, sx, sy, S, cnt, nullptr, 0);
     }
     if (cur >= 0) flush_counts(cnt, P.stats);
@@ -838,7 +879,7 @@ int icd_grid(int warps)
     int dev = 0, sms = 148, per_sm = 1;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, icd_phase_kernel<1, 2, 4, false, 0>, warps * 32, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, icd_phase_kernel<1, 2, 4, false, 0, false>, warps * 32, 0);
     return sms * (per_sm > 0 ? per_sm : 1);
 }
 

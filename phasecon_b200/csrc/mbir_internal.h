@@ -140,6 +140,7 @@ struct IcdLaunch {
     int colors_k;         // K x K colour classes; phase p updates colour (p + frame) mod K^2
     long long max_ctas;   // cap on the persistent grid (sv_max_concurrent); 0 = none
     int stage_records;    // prefetch each next column's A records into shared memory (cp.async)
+    int overlap;          // warp 0 gathers the prior neighbourhood while the other warps run theta
     // optional explicit work list of the phase (non-homogeneous passes): items[i]
     // = frame << 22 | sv_y << 11 | sv_x, *n_items of them (device memory);
     // null = every SV slot of the phase's colour in every frame
