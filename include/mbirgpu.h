@@ -90,6 +90,13 @@ typedef struct {
                                 while the CTA's other warps accumulate theta1 / theta2 (the two
                                 are independent); 0 (default): every warp takes part in both,
                                 one after the other */
+    int32_t graph_iterations;/* 1 (default): a session on a stream of its own (not the legacy
+                                default stream) replays each ICD iteration -- colour phases,
+                                non-homogeneous passes, FP64 refresh -- from a CUDA graph captured
+                                on first use (one graph per kind of iteration; the kernels read the
+                                iteration number from device memory); iterations with ring
+                                correction or variance re-estimation, and the legacy default
+                                stream, launch directly. 0: always launch directly */
 } mbirgpu_options;
 
 /* Defaults as listed above. */

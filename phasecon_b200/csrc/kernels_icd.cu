@@ -38,6 +38,9 @@
 //      prior pair), x <- V + alpha (u - V);
 //   4. apply: e[view][r][t] -= a dx(slice of t) with atomic adds.
 // All arithmetic is FP32; the host refreshes e in FP64 periodically.
+#include <mutex>
+#include <vector>
+
 #include "mbir_internal.h"
 
 namespace mbirgpu {
@@ -331,6 +334,7 @@ __device__ __forceinline__ void icd_update_sv(const Geom &g, const IcdLaunch &L,
     const int gstride = tw * G;
     const int gfirst = twarp * G + grp;
     const int fv0 = view_first[f], nv = view_first[f + 1] - fv0;
+    const int iter = L.iter_dev ? *L.iter_dev : L.iter;  // 1-based iteration number
 
     // ---- the SV's columns inside the reconstruction circle, shuffled ----------
     if (warp == 0) {
@@ -352,7 +356,7 @@ __device__ __forceinline__ void icd_update_sv(const Geom &g, const IcdLaunch &L,
         }
         __syncwarp();
         if (lane == 0) {
-            uint64_t h = mix64(L.seed ^ mix64(((uint64_t)L.iter << 40) ^ ((uint64_t)f << 20) ^
+            uint64_t h = mix64(L.seed ^ mix64(((uint64_t)iter << 40) ^ ((uint64_t)f << 20) ^
                                              (uint64_t)(sy * L.n_sv_x + sx)));
             for (int i = n - 1; i > 0; i--) {  // Fisher-Yates
                 h = mix64(h);
@@ -450,7 +454,7 @@ __device__ __forceinline__ void icd_update_sv(const Geom &g, const IcdLaunch &L,
                 S.pos[warp][lane] = pos;
                 // a column is skipped only if every slice is zero with no positive
                 // neighbour (in-column neighbours are the column's own values)
-                active_pred = !L.zero_skipping || L.iter <= 1 || (zl && V != 0.0f) || pos;
+                active_pred = !L.zero_skipping || iter <= 1 || (zl && V != 0.0f) || pos;
                 if (ovl && warp > 0) active_pred = 0;  // only warp 0 saw the neighbourhood
             }
             if (kStaged && ch == 0 && !ovl)  // issued one column earlier
@@ -525,7 +529,7 @@ __device__ __forceinline__ void icd_update_sv(const Geom &g, const IcdLaunch &L,
                     if (z >= 1 && vm > 0.0f) pos = 1;
                     if (z + 1 < NZ && vp > 0.0f) pos = 1;
                 }
-                const bool skip = !zl || (L.zero_skipping && L.iter > 1 && V0 == 0.0f && !pos);
+                const bool skip = !zl || (L.zero_skipping && iter > 1 && V0 == 0.0f && !pos);
                 __syncwarp();
                 S.th1[0][lane] = t1;
                 S.th2[0][lane] = t2;
@@ -691,12 +695,33 @@ static void launch_staged(const Geom &g, const IcdLaunch &L, const IcdConst &K, 
 {
     const int threads = L.warps * 32;
     const size_t smem = kStaged ? 2 * (size_t)stage_words * sizeof(uint32_t) : 0;
+    // resident CTAs per SM, cached per (device, block size, shared memory) so a
+    // launch being captured into a CUDA graph makes no occupancy query
+    struct Occ {
+        int dev, threads, sms, per_sm;
+        size_t smem;
+    };
+    static std::mutex mu;
+    static std::vector<Occ> cache;
     int dev = 0, sms = 148, per_sm = 1;
     cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, icd_phase_kernel<KW, U, VEC, kStaged, kHuber, kOverlap>,
-                                                  threads,
-                                                  smem);
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        bool hit = false;
+        for (const Occ &o : cache)
+            if (o.dev == dev && o.threads == threads && o.smem == smem) {
+                sms = o.sms;
+                per_sm = o.per_sm;
+                hit = true;
+                break;
+            }
+        if (!hit) {
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                &per_sm, icd_phase_kernel<KW, U, VEC, kStaged, kHuber, kOverlap>, threads, smem);
+            cache.push_back({dev, threads, sms, per_sm, smem});
+        }
+    }
     const long long items = (long long)g.N_time * sv_slots(g.N_x, g.N_y, L.sv, L.colors_k);
     long long grid = (long long)sms * (per_sm > 0 ? per_sm : 1);
     if (grid > items) grid = items;

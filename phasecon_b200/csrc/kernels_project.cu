@@ -216,8 +216,12 @@ static bool launch_views_g(const Geom &g, const uint32_t *d_table, const int32_t
 {
     constexpr int U = 4;
     const size_t smem = (size_t)G * g.N_r * g.N_t * sizeof(double);
-    // per call: the attribute belongs to the current device
-    if (cudaFuncSetAttribute(forward_project_views_kernel<G, U>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    // the attribute belongs to the current device; a launch being captured
+    // into a CUDA graph relies on the one set by an earlier direct launch
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cs) != cudaSuccess) return false;
+    if (cs == cudaStreamCaptureStatusNone &&
+        cudaFuncSetAttribute(forward_project_views_kernel<G, U>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              kViewProjMaxSmem) != cudaSuccess)
         return false;
     const unsigned blocks = (unsigned)((n_assigned + G - 1) / G);

@@ -73,6 +73,31 @@ Session::~Session()
         cudaEventDestroy(ev.first);
         cudaEventDestroy(ev.second);
     }
+    drop_graphs();
+    if (d_iter) cudaFree(d_iter);
+}
+
+void Session::drop_graphs()
+{
+    for (auto &row : graphs)
+        for (auto &ge : row)
+            if (ge) {
+                cudaGraphExecDestroy(ge);
+                ge = nullptr;
+            }
+    for (auto &row : graph_seen)
+        for (int &n : row) n = 0;
+}
+
+// An iteration is replayed from a CUDA graph when its launches depend on
+// nothing the host decides during the iteration: a stream of the session's
+// own (the legacy default stream cannot be captured), no ring correction (its
+// offset updates interleave with the phases; kept on direct launches), no
+// variance re-estimation (it reads a value back to the host), and no
+// schedule measurement in progress.
+bool Session::graph_ok() const
+{
+    return opt.graph_iterations && st != nullptr && !rings && !update_var && !tuning;
 }
 
 int Session::init(const mbirgpu_problem *pb, const mbirgpu_options *o, int mult_xy, int mult_z, void *stream)
@@ -239,6 +264,7 @@ int Session::autotune()
     CK(cudaMemcpyAsync(d_acc, d_err, n_sino * sizeof(float), cudaMemcpyDeviceToDevice, st));
     const bool save_timing = timing;
     timing = true;
+    tuning = true;
     const int cand[5][2] = {{4, 2}, {4, 4}, {8, 2}, {8, 4}, {16, 2}};
     const int ws[2] = {2, 4};
     auto allowed = [&](int a, int b) {
@@ -278,6 +304,8 @@ int Session::autotune()
         }
     }
     timing = save_timing;
+    tuning = false;
+    drop_graphs();
     sv = best_sv;
     warps = best_w;
     colors = best_k;
@@ -333,7 +361,11 @@ int Session::cost(double *total, double *data, double *prior)
     return 0;
 }
 
-int Session::icd_iteration(int iter, mbirgpu_iter_stats *out)
+// Every launch of one ICD iteration on the session's stream (memsets, the
+// full-sweep colour phases, the non-homogeneous passes, the periodic FP64
+// refresh). graph_mode: the kernels read the iteration number from d_iter and
+// the timing events are recorded as graph nodes.
+int Session::enqueue_iteration(int iter, bool graph_mode, int *launches_out)
 {
     const Geom &g = hs.g;
     CK(cudaMemsetAsync(d_stats, 0, sizeof(IcdStats), st));
@@ -344,6 +376,7 @@ int Session::icd_iteration(int iter, mbirgpu_iter_stats *out)
     L.n_sv_y = (g.N_y + sv - 1) / sv;
     L.warps = warps;
     L.iter = iter;
+    L.iter_dev = graph_mode ? d_iter : nullptr;
     L.zero_skipping = opt.zero_skipping;
     L.unroll = opt.icd_unroll > 0 ? opt.icd_unroll : 4;
     L.seed = opt.seed;
@@ -355,27 +388,22 @@ int Session::icd_iteration(int iter, mbirgpu_iter_stats *out)
     const int phases = colors * colors;
     Geom gb = g;
     gb.N_p = n_assigned;
-    if (timing && ev_pairs.size() < 2) {
-        while (ev_pairs.size() < 2) {
-            cudaEvent_t a, b;
-            CK(cudaEventCreate(&a));
-            CK(cudaEventCreate(&b));
-            ev_pairs.push_back({a, b});
-        }
-    }
-    if (timing) CK(cudaEventRecord(ev_pairs[0].first, st));
+    auto record = [&](cudaEvent_t e) -> cudaError_t {
+        return graph_mode ? cudaEventRecordWithFlags(e, st, cudaEventRecordExternal) : cudaEventRecord(e, st);
+    };
+    if (timing) CK(record(ev_pairs[0].first));
     for (int ph = 0; ph < phases; ph++) {
         L.phase = ph;
         launch_icd_phase(gb, L, d_table, d_view_first, d_mask, d_x, d_err, d_w, d_mag, d_stats, d_queue + ph, st);
         if (rings && update_offset()) return -1;
     }
-    if (timing) CK(cudaEventRecord(ev_pairs[0].second, st));
+    if (timing) CK(record(ev_pairs[0].second));
     int launches = phases;
     // non-homogeneous passes (the reference's NH-ICD, from iteration 2): each
     // re-updates the k columns per frame with the largest filtered update
     // magnitude, k = masked columns / NHICD_Iterations (XT_NHICD.c:176)
     const int nh = (d_sel && iter > 1) ? std::min(opt.nhicd_passes, kMaxNhPasses) : 0;
-    if (nh > 0 && timing) CK(cudaEventRecord(ev_pairs[1].first, st));
+    if (nh > 0 && timing) CK(record(ev_pairs[1].first));
     for (int pass = 0; pass < nh; pass++) {
         const int k = (int)(masked_columns / std::max(1, g.N_time)) / kNhicdIterations;
         launch_nh_select(g.N_time, g.N_y, g.N_x, d_mag, d_mask, k, d_filt, d_sel, st, d_nh_selstate);
@@ -405,12 +433,75 @@ int Session::icd_iteration(int iter, mbirgpu_iter_stats *out)
         if (rings && update_offset()) return -1;
         launches += nh_phases + 11 + (lists ? 3 : 0);  // filter + 10 select launches, 3 list launches
     }
-    if (nh > 0 && timing) CK(cudaEventRecord(ev_pairs[1].second, st));
+    if (nh > 0 && timing) CK(record(ev_pairs[1].second));
     CK(cudaGetLastError());
-    if (update_var && variance_update(g, g.N_p, d_err, d_w, &var_est, d_var, st))
+    // the noise-variance re-estimation reads its sums back to the host, so an
+    // iteration that has it is never captured
+    if (!graph_mode && update_var && variance_update(g, g.N_p, d_err, d_w, &var_est, d_var, st))
         return fail("variance update failed: %s", cudaGetErrorString(cudaGetLastError()));
-    if (opt.refresh_every > 0 && iter % opt.refresh_every == 0)
+    if (opt.refresh_every > 0 && iter % opt.refresh_every == 0) {
         if (refresh_error()) return -1;
+        launches += 1;
+    }
+    *launches_out = launches;
+    return 0;
+}
+
+int Session::icd_iteration(int iter, mbirgpu_iter_stats *out)
+{
+    const Geom &g = hs.g;
+    if (timing && ev_pairs.size() < 2) {
+        while (ev_pairs.size() < 2) {
+            cudaEvent_t a, b;
+            CK(cudaEventCreate(&a));
+            CK(cudaEventCreate(&b));
+            ev_pairs.push_back({a, b});
+        }
+    }
+    const int nh = (d_sel && iter > 1) ? std::min(opt.nhicd_passes, kMaxNhPasses) : 0;
+    int launches = 0;
+    const bool refresh_it = opt.refresh_every > 0 && iter % opt.refresh_every == 0;
+    // the first iteration of each kind launches directly (it sets the kernel
+    // attributes and occupancy figures the captured launches reuse); later
+    // ones replay a graph
+    if (graph_ok() && graph_seen[nh > 0][refresh_it] == 0) {
+        if (enqueue_iteration(iter, false, &launches)) return -1;
+        graph_seen[nh > 0][refresh_it] = 1;
+    } else if (graph_ok()) {
+        // one graph per (NH passes or not, FP64 refresh or not); the kernels
+        // read this iteration's number from d_iter
+        if (graphs_timed != timing) {
+            drop_graphs();
+            graphs_timed = timing;
+        }
+        if (!d_iter) {
+            cudaError_t e = cudaMalloc((void **)&d_iter, sizeof(int));
+            if (e != cudaSuccess) return fail("cudaMalloc of the iteration counter failed: %s", cudaGetErrorString(e));
+        }
+        const bool refresh = refresh_it;
+        cudaGraphExec_t &ge = graphs[nh > 0][refresh];
+        h_iter = iter;
+        CK(cudaMemcpyAsync(d_iter, &h_iter, sizeof(int), cudaMemcpyHostToDevice, st));
+        if (!ge) {
+            cudaGraph_t gr = nullptr;
+            CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            const int rc = enqueue_iteration(iter, true, &launches);
+            cudaError_t e = cudaStreamEndCapture(st, &gr);
+            if (rc) {
+                if (gr) cudaGraphDestroy(gr);
+                return -1;
+            }
+            if (e != cudaSuccess) return fail("capturing the ICD iteration failed: %s", cudaGetErrorString(e));
+            e = cudaGraphInstantiate(&ge, gr, 0);
+            cudaGraphDestroy(gr);
+            if (e != cudaSuccess) return fail("instantiating the ICD iteration graph failed: %s", cudaGetErrorString(e));
+        }
+        graph_launches_[nh > 0][refresh] = launches ? launches : graph_launches_[nh > 0][refresh];
+        launches = graph_launches_[nh > 0][refresh];
+        CK(cudaGraphLaunch(ge, st));
+    } else {
+        if (enqueue_iteration(iter, false, &launches)) return -1;
+    }
     IcdStats hst;
     CK(cudaMemcpyAsync(&hst, d_stats, sizeof(hst), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
@@ -672,6 +763,7 @@ void mbirgpu_default_options(mbirgpu_options *o)
     o->nh_work_lists = 1;
     o->autotune = 0;
     o->icd_overlap = 0;
+    o->graph_iterations = 1;
 }
 
 int mbirgpu_set_options(const mbirgpu_options *o)
@@ -691,6 +783,7 @@ int mbirgpu_set_options(const mbirgpu_options *o)
     if (o->nh_cta_warps < 0 || o->nh_cta_warps > 8) return fail("nh_cta_warps must be 0 (auto) or 1..8");
     if (o->autotune != 0 && o->autotune != 1) return fail("autotune must be 0 (schedule by rule) or 1 (measured)");
     if (o->icd_overlap != 0 && o->icd_overlap != 1) return fail("icd_overlap must be 0 or 1");
+    if (o->graph_iterations != 0 && o->graph_iterations != 1) return fail("graph_iterations must be 0 or 1");
     mbirgpu_options cur = mbirgpu::current_options();
     (void)cur;
     std::lock_guard<std::mutex> lk(mbirgpu::g_opt_mu);

@@ -47,6 +47,15 @@ struct Session {
     uint64_t *d_nh_selstate = nullptr;  // radix-select state (nh_select_scratch_bytes)
     size_t nh_items_cap = 0, nh_scratch_cap = 0;  // ints allocated
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pairs;
+    // CUDA graphs of one ICD iteration, by [non-homogeneous passes][FP64
+    // refresh]; the iteration number the kernels read lives in d_iter
+    cudaGraphExec_t graphs[2][2] = {};
+    bool graphs_timed = false;  // the captured graphs record the timing events
+    bool tuning = false;        // schedule candidates are being measured: no graphs
+    int *d_iter = nullptr;
+    int h_iter = 0;
+    int graph_launches_[2][2] = {};  // kernel launches inside each graph
+    int graph_seen[2][2] = {};       // direct runs of each kind of iteration so far
     // ring correction: offset d [N_r][N_t] of e = y - Ax - d, updated after
     // every full-sweep phase and every NH pass while rings != 0
     int rings = 0;
@@ -73,6 +82,9 @@ struct Session {
     int get_object(float *obj);
     int cost(double *total, double *data, double *prior);
     int icd_iteration(int iter, mbirgpu_iter_stats *out);
+    int enqueue_iteration(int iter, bool graph_mode, int *launches);  // every launch of one iteration
+    bool graph_ok() const;
+    void drop_graphs();
     int run(int max_iter, double *costs, int *iters, mbirgpu_iter_stats *total);
     int amatrix(int32_t *first, int32_t *count, float *values);
     int forward_project(const float *obj, float *sino);

@@ -123,6 +123,25 @@ def test_icd_converges_to_reference_cost_4d(overlap):
     assert rmse <= 0.005 * (xr.max() - xr.min())
 
 
+def test_graph_replayed_iterations_match_direct_launches():
+    """On a stream of its own a session replays ICD iterations from CUDA graphs
+    (captured from the second iteration of each kind on, the iteration number
+    read from device memory); the result equals direct launches of the same
+    schedule up to the order of FP32 atomic updates: costs within 1e-6."""
+    import torch
+    pb, _ = make_problem(ncol=64, nrow=8, nview=48, nframe=3, seed=13, moving=True)
+    runs = []
+    for graphs in (0, 1):
+        stream = torch.cuda.Stream()
+        s = gpu_session(pb, graph_iterations=graphs, nhicd_passes=2, refresh_every=3)
+        s.set_stream(stream.cuda_stream)
+        s.set_object(np.zeros(s.shape, np.float32))
+        costs = _run_icd(s, 9)
+        runs.append(costs)
+        s.close()
+    assert np.allclose(runs[0], runs[1], rtol=1e-6, atol=0), runs
+
+
 def test_icd_huber_branch_converges():
     pb = golden_problem("huber")
     s = gpu_session(pb, sv_size=4)
