@@ -27,25 +27,107 @@ __device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(
 __device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
 __device__ __forceinline__ float cabs2(float2 a) { return a.x * a.x + a.y * a.y; }
 
-// nseq sequences of length n (power of two) stored back to back in `a`;
-// radix-2 Stockham passes ping-pong between a and b. Returns the buffer
-// holding the result. tw[m] = exp(-2 pi i m / nmax), m < nmax / 2.
-__device__ float2 *fft_smem(float2 *a, float2 *b, int n, int log2n, int nseq, const float2 *tw, int nmax,
-                            bool inverse)
+// Shared-memory layout of the FFT buffers: element i of sequence q sits at
+// q * sstride + i + i / 16 (one float2 of padding after every 16, and a
+// sequence stride fft_seq_stride(n) = n + n / 16 + 1 that is odd in float2
+// units), so both the contiguous accesses of a stage and the strided ones of
+// the column pass's transposed staging spread over the banks.
+__device__ __forceinline__ int fpos(int q, int i, int sstride) { return q * sstride + i + (i >> 4); }
+
+// exp(-+ 2 pi i m / nmax) for any 0 <= m < nmax from the half-circle table
+// (tw[m] = exp(-2 pi i m / nmax), m < nmax / 2; the other half is -tw).
+__device__ __forceinline__ float2 twid(const float2 *tw, int m, int nmax, bool inverse)
 {
-    const int half = n >> 1;
-    for (int L = 1, s = 0; L < n; L <<= 1, s++) {
-        const int tstride = nmax / (L << 1);
-        for (int idx = threadIdx.x; idx < nseq * half; idx += blockDim.x) {
-            const int q = idx >> (log2n - 1), j = idx & (half - 1);
-            const int k = j & (L - 1);
-            float2 w = tw[k * tstride];
-            if (inverse) w.y = -w.y;
-            const float2 x0 = a[q * n + j], x1 = a[q * n + j + half];
-            const float2 t = cmul(w, x1);
-            const int o = q * n + ((j - k) << 1) + k;
-            b[o] = cadd(x0, t);
-            b[o + L] = csub(x0, t);
+    const int h = nmax >> 1;
+    float2 w = m < h ? tw[m] : make_float2(-tw[m - h].x, -tw[m - h].y);
+    if (inverse) w.y = -w.y;
+    return w;
+}
+
+__host__ __device__ constexpr int bit_reverse(int i, int bits)
+{
+    int r = 0;
+    for (int b = 0; b < bits; b++)
+        if (i & (1 << b)) r |= 1 << (bits - 1 - b);
+    return r;
+}
+
+__host__ __device__ constexpr int log2_const(int n) { return n <= 1 ? 0 : 1 + log2_const(n >> 1); }
+
+// R-point DFT of x in registers, natural order in and out (radix-2
+// decimation in time over a bit-reversed copy; every index is a constant).
+template <int R>
+__device__ __forceinline__ void dft_regs(float2 (&x)[R], const float2 *tw, int nmax, bool inverse)
+{
+    constexpr int bits = log2_const(R);
+    float2 y[R];
+#pragma unroll
+    for (int i = 0; i < R; i++) y[bit_reverse(i, bits)] = x[i];
+#pragma unroll
+    for (int len = 2; len <= R; len <<= 1) {
+#pragma unroll
+        for (int i = 0; i < R; i += len)
+#pragma unroll
+            for (int k = 0; k < len / 2; k++) {
+                const float2 t = cmul(twid(tw, k * (nmax / len), nmax, inverse), y[i + k + len / 2]);
+                y[i + k + len / 2] = csub(y[i + k], t);
+                y[i + k] = cadd(y[i + k], t);
+            }
+    }
+#pragma unroll
+    for (int i = 0; i < R; i++) x[i] = y[i];
+}
+
+// One radix-R stage of a Stockham autosort FFT over nseq sequences of length
+// n whose sub-transforms have length L so far: butterfly j of a sequence
+// takes x_p = a[j + p n / R], p < R, multiplies x_p by w_{RL}^{p (j mod L)},
+// transforms the R points in registers and writes them to b at
+// (j - j mod L) R + j mod L + p L.
+template <int R>
+__device__ __forceinline__ void stockham_stage(const float2 *a, float2 *b, int n, int log2n, int L, int nseq,
+                                               int sstride, const float2 *tw, int nmax, bool inverse)
+{
+    constexpr int lr = log2_const(R);
+    const int lm = log2n - lr;  // butterflies per sequence: n / R = 2^lm
+    const int m = 1 << lm;
+    const int tscale = nmax / (R * L);
+    for (int idx = threadIdx.x; idx < (nseq << lm); idx += blockDim.x) {
+        const int q = idx >> lm, j = idx & (m - 1);
+        const int k = j & (L - 1);
+        float2 x[R];
+#pragma unroll
+        for (int p = 0; p < R; p++) x[p] = a[fpos(q, j + p * m, sstride)];
+        if (L > 1) {
+#pragma unroll
+            for (int p = 1; p < R; p++) x[p] = cmul(twid(tw, k * p * tscale, nmax, inverse), x[p]);
+        }
+        dft_regs<R>(x, tw, nmax, inverse);
+        const int o = ((j - k) << lr) + k;
+#pragma unroll
+        for (int p = 0; p < R; p++) b[fpos(q, o + p * L, sstride)] = x[p];
+    }
+}
+
+// nseq sequences of length n (power of two) in the padded layout of `a`;
+// radix-16 stages (radix 8, 4 or 2 for the rest) ping-pong between a and b.
+// Returns the buffer holding the result.
+__device__ float2 *fft_smem(float2 *a, float2 *b, int n, int log2n, int nseq, int sstride, const float2 *tw,
+                            int nmax, bool inverse)
+{
+    for (int L = 1; L < n;) {
+        const int rem = n / L;
+        if (rem >= 16) {
+            stockham_stage<16>(a, b, n, log2n, L, nseq, sstride, tw, nmax, inverse);
+            L <<= 4;
+        } else if (rem == 8) {
+            stockham_stage<8>(a, b, n, log2n, L, nseq, sstride, tw, nmax, inverse);
+            L <<= 3;
+        } else if (rem == 4) {
+            stockham_stage<4>(a, b, n, log2n, L, nseq, sstride, tw, nmax, inverse);
+            L <<= 2;
+        } else {
+            stockham_stage<2>(a, b, n, log2n, L, nseq, sstride, tw, nmax, inverse);
+            L <<= 1;
         }
         __syncthreads();
         float2 *tmp = a;
@@ -102,8 +184,8 @@ __global__ void pc_rows_forward(PcDims d, PcArgs A, int prologue)
     extern __shared__ float2 smem[];
     const int v = blockIdx.y;
     if (A.active && !A.active[v]) return;
-    const int C = d.C, rpc = d.rows_per_cta;
-    float2 *s_tw = smem, *a = smem + d.nmax / 2, *b = a + rpc * C;
+    const int C = d.C, rpc = d.rows_per_cta, S = fft_seq_stride(C);
+    float2 *s_tw = smem, *a = smem + d.nmax / 2, *b = a + rpc * S;
     load_twiddles(s_tw, A.tw, d.nmax);
     const int r0 = blockIdx.x * rpc;
     const size_t vb = (size_t)v * d.N;
@@ -122,12 +204,13 @@ __global__ void pc_rows_forward(PcDims d, PcArgs A, int prologue)
             } break;
             }
         }
-        a[e] = x;
+        a[fpos(e / C, e % C, S)] = x;
     }
     __syncthreads();
     const int nrows = min(rpc, d.R - r0);
-    float2 *res = fft_smem(a, b, C, d.logC, nrows, s_tw, d.nmax, false);
-    for (int e = threadIdx.x; e < nrows * C; e += blockDim.x) A.work[vb + (size_t)r0 * C + e] = res[e];
+    float2 *res = fft_smem(a, b, C, d.logC, nrows, S, s_tw, d.nmax, false);
+    for (int e = threadIdx.x; e < nrows * C; e += blockDim.x)
+        A.work[vb + (size_t)r0 * C + e] = res[fpos(e / C, e % C, S)];
 }
 
 // ---------------------------------------------------------------------------- pass 2
@@ -136,27 +219,28 @@ __global__ void pc_cols_filter(PcDims d, PcArgs A, const float2 *__restrict__ tr
     extern __shared__ float2 smem[];
     const int v = blockIdx.y;
     if (A.active && !A.active[v]) return;
-    const int R = d.R, C = d.C, cb = d.cols_per_cta;
-    float2 *s_tw = smem, *a = smem + d.nmax / 2, *b = a + cb * R;
+    const int R = d.R, C = d.C, cb = d.cols_per_cta, S = fft_seq_stride(R);
+    float2 *s_tw = smem, *a = smem + d.nmax / 2, *b = a + cb * S;
     load_twiddles(s_tw, A.tw, d.nmax);
     const int c0 = blockIdx.x * cb;
     const size_t vb = (size_t)v * d.N;
     for (int e = threadIdx.x; e < cb * R; e += blockDim.x) {
         const int r = e / cb, q = e % cb;
-        a[q * R + r] = A.work[vb + (size_t)r * C + c0 + q];
+        a[fpos(q, r, S)] = A.work[vb + (size_t)r * C + c0 + q];
     }
     __syncthreads();
-    float2 *res = fft_smem(a, b, R, d.logR, cb, s_tw, d.nmax, false);
+    float2 *res = fft_smem(a, b, R, d.logR, cb, S, s_tw, d.nmax, false);
     float2 *other = res == a ? b : a;
     for (int e = threadIdx.x; e < cb * R; e += blockDim.x) {
-        const int q = e / R, r = e % R;
-        res[e] = cmul(res[e], transfer[(size_t)r * C + c0 + q]);
+        const int r = e / cb, q = e % cb;
+        const int i = fpos(q, r, S);
+        res[i] = cmul(res[i], transfer[(size_t)r * C + c0 + q]);
     }
     __syncthreads();
-    res = fft_smem(res, other, R, d.logR, cb, s_tw, d.nmax, true);
+    res = fft_smem(res, other, R, d.logR, cb, S, s_tw, d.nmax, true);
     for (int e = threadIdx.x; e < cb * R; e += blockDim.x) {
         const int r = e / cb, q = e % cb;
-        A.work[vb + (size_t)r * C + c0 + q] = res[q * R + r];
+        A.work[vb + (size_t)r * C + c0 + q] = res[fpos(q, r, S)];
     }
 }
 
@@ -167,20 +251,20 @@ __global__ void pc_rows_inverse(PcDims d, PcArgs A, int epilogue)
     __shared__ double s_red[32];
     const int v = blockIdx.y;
     if (A.active && !A.active[v]) return;
-    const int C = d.C, rpc = d.rows_per_cta;
-    float2 *s_tw = smem, *a = smem + d.nmax / 2, *b = a + rpc * C;
+    const int C = d.C, rpc = d.rows_per_cta, S = fft_seq_stride(C);
+    float2 *s_tw = smem, *a = smem + d.nmax / 2, *b = a + rpc * S;
     load_twiddles(s_tw, A.tw, d.nmax);
     const int r0 = blockIdx.x * rpc;
     const int nrows = min(rpc, d.R - r0);
     const size_t vb = (size_t)v * d.N;
-    for (int e = threadIdx.x; e < nrows * C; e += blockDim.x) a[e] = A.work[vb + (size_t)r0 * C + e];
+    for (int e = threadIdx.x; e < nrows * C; e += blockDim.x) a[fpos(e / C, e % C, S)] = A.work[vb + (size_t)r0 * C + e];
     __syncthreads();
-    float2 *res = fft_smem(a, b, C, d.logC, nrows, s_tw, d.nmax, true);
+    float2 *res = fft_smem(a, b, C, d.logC, nrows, S, s_tw, d.nmax, true);
     const float inv_n = 1.0f / (float)d.N;
     double acc = 0.0;
     for (int e = threadIdx.x; e < nrows * C; e += blockDim.x) {
         const size_t i = vb + (size_t)r0 * C + e, p = (size_t)r0 * C + e;
-        const float2 t = cscale(res[e], inv_n);
+        const float2 t = cscale(res[fpos(e / C, e % C, S)], inv_n);
         switch (epilogue) {
         case PC_OUT_PLAIN: A.out[i] = t; break;
         case PC_OUT_GRES: {  // conj(Omega) Lambda (Omega t - y)

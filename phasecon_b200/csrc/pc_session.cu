@@ -43,10 +43,12 @@ int pc_transform_dims(PcDims &d, int V, int R, int C, size_t *smem_rows, size_t 
     d.logR = ilog2(R);
     d.logC = ilog2(C);
     d.nmax = std::max(R, C);
-    d.rows_per_cta = std::max(1, std::min(R, 2048 / C));
+    // sequences per CTA: enough radix-16 butterflies (n / 16 per sequence) for
+    // the 256 threads, within the shared memory of the two padded buffers
+    d.rows_per_cta = std::max(1, std::min(R, 4096 / C));
     d.cols_per_cta = std::max(1, std::min(C, 4096 / R));
-    *smem_rows = (size_t)(d.nmax / 2 + 2 * d.rows_per_cta * C) * sizeof(float2);
-    *smem_cols = (size_t)(d.nmax / 2 + 2 * d.cols_per_cta * R) * sizeof(float2);
+    *smem_rows = (size_t)(d.nmax / 2 + 2 * d.rows_per_cta * fft_seq_stride(C)) * sizeof(float2);
+    *smem_cols = (size_t)(d.nmax / 2 + 2 * d.cols_per_cta * fft_seq_stride(R)) * sizeof(float2);
     cudaError_t e = cudaFuncSetAttribute(pc_rows_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem_rows);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(pc_rows_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem_rows);
