@@ -451,6 +451,17 @@ struct NmsCtx {
     const PcPrior *P;
 };
 
+// a^e for a > 0 with the hardware base-2 logarithm and exponential (the
+// search's stop rule, a 0.005 % relative vertex movement, is far above their
+// error)
+__device__ __forceinline__ float pow_fast(float a, float e)
+{
+    float l, r;
+    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(l) : "f"(a));
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(e * l));
+    return r;
+}
+
 __device__ float nms_cost(const NmsCtx &c, float zr, float zi)
 {
     const float2 ez = expz_fast(zr, zi);
@@ -463,8 +474,10 @@ __device__ float nms_cost(const NmsCtx &c, float zr, float zi)
             const float dph = P.T00_f * dd + P.T01_f * db, dmg = P.T10_f * dd + P.T11_f * db;
             const float aph = fabsf(dph), amg = fabsf(dmg);
             const float fw = P.f_f[a];
-            if (aph > 0.f) cost += fw * (aph * aph * P.ph_isq_f) / (P.ph_c_f + __expf(P.qmp_f * __logf(aph)) * P.ph_isqp_f);
-            if (amg > 0.f) cost += fw * (amg * amg * P.mg_isq_f) / (P.mg_c_f + __expf(P.qmp_f * __logf(amg)) * P.mg_isqp_f);
+            if (aph > 0.f)
+                cost += fw * __fdividef(aph * aph * P.ph_isq_f, P.ph_c_f + pow_fast(aph, P.qmp_f) * P.ph_isqp_f);
+            if (amg > 0.f)
+                cost += fw * __fdividef(amg * amg * P.mg_isq_f, P.mg_c_f + pow_fast(amg, P.qmp_f) * P.mg_isqp_f);
         }
     }
     return cost;
