@@ -29,7 +29,7 @@ __device__ __forceinline__ float cabs2(float2 a) { return a.x * a.x + a.y * a.y;
 
 // Shared-memory layout of the FFT buffers: element i of sequence q sits at
 // q * sstride + i + i / 16 (one float2 of padding after every 16, and a
-// sequence stride fft_seq_stride(n) = n + n / 16 + 1 that is odd in float2
+// sequence stride fft_seq_stride(n) = (n + n / 16) | 1, odd in float2
 // units), so both the contiguous accesses of a stage and the strided ones of
 // the column pass's transposed staging spread over the banks.
 __device__ __forceinline__ int fpos(int q, int i, int sstride) { return q * sstride + i + (i >> 4); }

@@ -83,8 +83,9 @@ __global__ void pc_nms_wavefront(PcDims d, PcArgs A, const __grid_constant__ PcP
 // two): fills d's sizes and per-CTA tiles, the dynamic shared memory of the
 // row and column passes, and raises the kernels' shared-memory limits.
 int pc_transform_dims(PcDims &d, int V, int R, int C, size_t *smem_rows, size_t *smem_cols);
-// float2 slots one FFT sequence of length n takes in shared memory (padded)
-__host__ __device__ inline int fft_seq_stride(int n) { return n + n / 16 + 1; }
+// float2 slots one FFT sequence of length n takes in shared memory: n plus
+// one padding slot per 16, rounded up to an odd count
+__host__ __device__ inline int fft_seq_stride(int n) { return (n + n / 16) | 1; }
 // exp(-2 pi i m / nmax), m < nmax / 2, computed in double and rounded once
 std::vector<float2> pc_twiddles(int nmax);
 // One Fresnel-type transform of every view: prologue + FFT along C, FFT along
