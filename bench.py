@@ -19,9 +19,16 @@ One JSON line on rank 0 carries:
   roofline    the ICD sweep kernel's algorithmic bytes (12 nnz_v + 8 per voxel
               update) over its measured launch time, against MEASURED_PEAKS.json;
   cpu_baseline the reference C (oracle/_ref, built from source) on a bounded
-              sample of the workload on this host's cores.
+              sample of the workload on this host's cores;
+  warm_start  the learned warm start: the U-Net trained from --ws-seeds seeds
+              on seeded Cahn-Hilliard scans and ellipsoid phantoms, and the
+              wall time of plain ICD to the plain method's converged cost
+              from zero, from FBP and from each network (speedup_vs_zero_init
+              is the smallest over the seeds), with its clock record.
 With --gpus N > 1 (torchrun) every rank runs an independent replica (the path
 does not shard on one problem); value is the sum over ranks / max time.
+--workload pc|batch|warmstart print the phase-contrast, batched and warm-start
+lines instead.
 """
 from __future__ import annotations
 
@@ -420,7 +427,10 @@ def run_ours(args, world, rank, local, pg):
 
     ws = None
     if not args.no_warmstart and not args.no_converge:
-        ws = warmstart_section(args, rank, local, pb, p)
+        try:
+            ws = warmstart_section(args, rank, local, pb, p)
+        except Exception as ex:  # the ICD line above stands on its own
+            ws = {"speedup_vs_zero_init": None, "error": f"{type(ex).__name__}: {ex}"}
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
