@@ -355,7 +355,7 @@ def run_ours(args, world, rank, local, pg):
     # time to converged cost from zero (plain GPU ICD), FP64 cost every iteration
     conv = {}
     if not args.no_converge:
-        s.set_object(np.zeros(s.shape, np.float32))
+        s.set_object_zero()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         costs = [s.cost()[0]]
@@ -542,7 +542,7 @@ def warmstart_section(args, rank: int, local: int, pb, p: float) -> dict:
     opt = pc.get_options()
     opt.mrf_p = p
     s = pc.Session(pb, options=opt, stream=torch.cuda.current_stream().cuda_stream)
-    s.set_object(np.zeros(s.shape, np.float32))
+    s.set_object_zero()
     _, c_conv = WS.converge(s, rel=1e-7, max_iter=400)
     target = c_conv[-1] * (1 + 1e-4)
 
@@ -557,7 +557,7 @@ def warmstart_section(args, rank: int, local: int, pb, p: float) -> dict:
         return {"time_to_converged_cost_s": time.perf_counter() - t0, "init_s": t_init, "iterations": it,
                 "initial_cost": costs[0], "final_cost": costs[-1]}
 
-    starts = {"zero": lambda: s.set_object(np.zeros(s.shape, np.float32)), "fbp": s.set_object_fbp}
+    starts = {"zero": s.set_object_zero, "fbp": s.set_object_fbp}
     res, seeds, train_s, losses = {}, [], [], []
     with ClockSampler(local) as clk:
         for name, fn in starts.items():

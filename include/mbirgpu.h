@@ -200,6 +200,10 @@ int mbirgpu_session_back_project(mbirgpu_session *s, const float *sino, float *o
  * MBIR_4D/XT_ICD_update.c:540-647); FBP has no counterpart there. */
 int mbirgpu_session_fbp(mbirgpu_session *s, float *object);
 int mbirgpu_session_set_object_fbp(mbirgpu_session *s);
+/* The current object becomes zero on the device (the reference's zero
+ * initialisation, XT_ICD_update.c:540-647 with no previous stage), then
+ * e = y - A x - d; no host buffer is involved. */
+int mbirgpu_session_set_object_zero(mbirgpu_session *s);
 
 /* Ring correction (remove_rings of reconstruct, MBIR_4D/XT_Engine.c:73):
  * the session estimates one offset d per detector pixel, shared by all views,

@@ -17,7 +17,8 @@ constexpr double kPi = 3.14159265358979323846;
 
 // One CTA per view: the view's [N_r][N_t] block in shared memory, every
 // (channel, row) output a direct convolution over the channels (FP32 sums of
-// an exactly tabulated filter).
+// an exactly tabulated filter). The filter is zero at even nonzero offsets,
+// so the sum runs over the centre tap and the odd offsets only.
 __global__ void ramp_filter_kernel(int N_r, int N_t, double delta_r, const float *__restrict__ y,
                                    float *__restrict__ q)
 {
@@ -35,8 +36,9 @@ __global__ void ramp_filter_kernel(int N_r, int N_t, double delta_r, const float
     __syncthreads();
     for (int o = threadIdx.x; o < N_r * N_t; o += blockDim.x) {
         const int r = o / N_t, t = o - r * N_t;
-        float acc = 0.0f;
-        for (int k = 0; k < N_r; k++) acc += sy[k * N_t + t] * h[r - k + N_r - 1];
+        float acc = sy[r * N_t + t] * h[N_r - 1];
+        // channels k = r - n for odd n: k runs over the parity opposite to r's
+        for (int k = (r & 1) ^ 1; k < N_r; k += 2) acc += sy[k * N_t + t] * h[r - k + N_r - 1];
         q[base + o] = acc;
     }
 }

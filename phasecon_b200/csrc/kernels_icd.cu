@@ -331,8 +331,11 @@ __device__ __forceinline__ void icd_update_sv(const Geom &g, const IcdLaunch &L,
     // over W - 1 warps and the neighbourhood needs no cross-warp sum
     const bool ovl = kOverlap && W >= 2;
     const int tw = ovl ? W - 1 : W, twarp = ovl ? warp - 1 : warp;  // theta warps, this warp's rank
-    const int gstride = tw * G;
-    const int gfirst = twarp * G + grp;
+    // theta: the view groups of the theta warps; apply: those of every warp
+    const int tgstride = tw * G;
+    const int tgfirst = twarp * G + grp;  // negative for warp 0 in overlap mode, which runs no theta
+    const int gstride = W * G;
+    const int gfirst = warp * G + grp;
     const int fv0 = view_first[f], nv = view_first[f + 1] - fv0;
     const int iter = L.iter_dev ? *L.iter_dev : L.iter;  // 1-based iteration number
 
@@ -404,7 +407,7 @@ __device__ __forceinline__ void icd_update_sv(const Geom &g, const IcdLaunch &L,
                 wait_staged(&S.stage_bar[ci & 1], cnt.phases, ci & 1, cnt.timeouts, S.abort, S.abort_bar,
                             S.abort_parity);
             if (ovl && warp > 0 && row_ok)
-                theta_pass<KW, kUnroll, VEC, kStaged, kHuber>(K, col_rec, err, wgt, gfirst, gstride, nv, RW, NT,
+                theta_pass<KW, kUnroll, VEC, kStaged, kHuber>(K, col_rec, err, wgt, tgfirst, tgstride, nv, RW, NT,
                                                              rbase + t0, th1, th2);
             {
                 float num = 0.0f, den = 0.0f;
@@ -481,7 +484,7 @@ __device__ __forceinline__ void icd_update_sv(const Geom &g, const IcdLaunch &L,
             // ---- 2. theta over the column's views (already done in overlap mode) ---
             {
                 if (!ovl && row_ok)
-                    theta_pass<KW, kUnroll, VEC, kStaged, kHuber>(K, col_rec, err, wgt, gfirst, gstride, nv, RW, NT,
+                    theta_pass<KW, kUnroll, VEC, kStaged, kHuber>(K, col_rec, err, wgt, tgfirst, tgstride, nv, RW, NT,
                                                                  rbase + t0, th1, th2);
                 // fold the view groups of the warp onto group 0
                 for (int off = lprp; off < 32; off <<= 1) {

@@ -267,7 +267,30 @@ __global__ void back_project_kernel(Geom g, const uint32_t *__restrict__ table,
     const int fv0 = view_first[f], nv = view_first[f + 1] - fv0;
     const uint32_t *rec = table + ((size_t)fv0 * nxy + (size_t)c * nv) * g.rec_words;
     double acc = 0.0;
-    if (t < g.N_t) {
+    if (t < g.N_t && g.rec_words == 4) {
+        // records of one 16-byte word (header + up to 3 weights): four views'
+        // records, then their sinogram entries, in flight at once
+        constexpr int U = 4;
+        const uint4 *r4 = reinterpret_cast<const uint4 *>(rec);
+        for (int v0 = 0; v0 < nv; v0 += U) {
+            uint4 R[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) R[u] = v0 + u < nv ? __ldg(r4 + v0 + u) : make_uint4(0, 0, 0, 0);
+            float s[U][3];
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const int cnt = R[u].x >> 24;
+                const float *p = sino + (size_t)(R[u].x & 0xFFFFFFu) * g.N_t + t;
+#pragma unroll
+                for (int q = 0; q < 3; q++) s[u][q] = q < cnt ? __ldg(p + (size_t)q * g.N_t) : 0.0f;
+            }
+#pragma unroll
+            for (int u = 0; u < U; u++)
+                acc += (double)__uint_as_float(R[u].y) * (double)s[u][0] +
+                       (double)__uint_as_float(R[u].z) * (double)s[u][1] +
+                       (double)__uint_as_float(R[u].w) * (double)s[u][2];
+        }
+    } else if (t < g.N_t) {
         for (int v = 0; v < nv; v++, rec += g.rec_words) {
             const uint32_t hdr = __ldg(rec);
             const int cnt = hdr >> 24, row = hdr & 0xFFFFFF;

@@ -935,6 +935,14 @@ int mbirgpu_session_set_object_fbp(mbirgpu_session *sp)
     return s->set_object_fbp();
 }
 
+int mbirgpu_session_set_object_zero(mbirgpu_session *sp)
+{
+    SESSION(sp);
+    cudaError_t e = cudaMemsetAsync(s->d_x, 0, s->n_vox * sizeof(float), s->st);
+    if (e != cudaSuccess) return fail("clearing the object failed: %s", cudaGetErrorString(e));
+    return s->refresh_error();
+}
+
 int mbirgpu_session_set_ring_correction(mbirgpu_session *sp, int32_t remove_rings, const float *offset)
 {
     SESSION(sp);

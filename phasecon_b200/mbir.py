@@ -28,7 +28,8 @@ EXPORTS = (
     "mbirgpu_session_cost", "mbirgpu_session_icd_iteration", "mbirgpu_session_forward_project",
     "mbirgpu_session_back_project", "mbirgpu_session_get_amatrix", "mbirgpu_session_get_detector_response",
     "mbirgpu_session_run", "mbirgpu_session_forward_project_noalloc", "mbirgpu_session_nh_select",
-    "mbirgpu_session_fbp", "mbirgpu_session_set_object_fbp", "mbirgpu_session_set_ring_correction",
+    "mbirgpu_session_fbp", "mbirgpu_session_set_object_fbp", "mbirgpu_session_set_object_zero",
+    "mbirgpu_session_set_ring_correction",
     "mbirgpu_session_get_offset", "mbirgpu_session_update_offset", "mbirgpu_session_set_variance_estimation",
     "mbirgpu_session_update_variance", "mbirgpu_session_get_variance",
     "mbirgpu_unet_create", "mbirgpu_unet_destroy", "mbirgpu_unet_num_params", "mbirgpu_unet_set_input_scale",
@@ -139,6 +140,7 @@ def lib() -> C.CDLL:
         L.mbirgpu_session_nh_select.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         L.mbirgpu_session_fbp.argtypes = [C.c_void_p, C.c_void_p]
         L.mbirgpu_session_set_object_fbp.argtypes = [C.c_void_p]
+        L.mbirgpu_session_set_object_zero.argtypes = [C.c_void_p]
         L.mbirgpu_session_set_ring_correction.argtypes = [C.c_void_p, C.c_int32, C.c_void_p]
         L.mbirgpu_session_update_offset.argtypes = [C.c_void_p]
         L.mbirgpu_session_get_offset.argtypes = [C.c_void_p, C.c_void_p]
@@ -353,6 +355,10 @@ class Session:
 
     def set_object_fbp(self) -> None:
         _check(lib().mbirgpu_session_set_object_fbp(self.h))
+
+    def set_object_zero(self) -> None:
+        """x = 0 on the device, then e = y - A x (no host copy)."""
+        _check(lib().mbirgpu_session_set_object_zero(self.h))
 
     def set_ring_correction(self, remove_rings: int, offset: np.ndarray | None = None) -> None:
         """Estimate a per-detector-pixel offset d (remove_rings 1, 2, 3; 0 off),

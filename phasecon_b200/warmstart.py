@@ -202,7 +202,7 @@ def training_pair(seed: int, n_xy: int = 256, n_z: int = 32, kind: str = "mixed"
     o.mrf_p = p
     s = Session(pb, options=o)
     fbp = s.fbp()[0]
-    s.set_object(np.zeros(s.shape, np.float32))
+    s.set_object_zero()
     converge(s, rel=icd_rel)
     target = s.get_object()[0]
     s.close()
@@ -222,7 +222,7 @@ def training_pairs_4d(seed: int, ch_steps: int | None = None, rel: float = 1e-4)
     o.mrf_p = p
     s = Session(pb, options=o)
     fbp = s.fbp()
-    s.set_object(np.zeros(s.shape, np.float32))
+    s.set_object_zero()
     converge(s, rel=rel)
     target = s.get_object()
     s.close()
