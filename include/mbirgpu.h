@@ -403,6 +403,9 @@ typedef struct {
     int32_t nms_order;         /* proximal sweep order: 0 = the reference's raster order,
                                   kept exactly by anti-diagonal wavefronts (default);
                                   1 = four colour classes (more parallel, other order) */
+    int32_t fft_radix;         /* largest radix of the FFT stages: 2, 4, 8 or 16; 0 = the
+                                  library's choice. Every stage keeps its points in registers
+                                  between two passes through shared memory */
 } mbirgpu_pc_options;
 
 typedef struct {

@@ -109,20 +109,21 @@ __device__ __forceinline__ void stockham_stage(const float2 *a, float2 *b, int n
 }
 
 // nseq sequences of length n (power of two) in the padded layout of `a`;
-// radix-16 stages (radix 8, 4 or 2 for the rest) ping-pong between a and b.
+// stages of radix max_radix (16, 8, 4 or 2; smaller for the rest) ping-pong
+// between a and b.
 // Returns the buffer holding the result.
 __device__ float2 *fft_smem(float2 *a, float2 *b, int n, int log2n, int nseq, int sstride, const float2 *tw,
-                            int nmax, bool inverse)
+                            int nmax, bool inverse, int max_radix)
 {
     for (int L = 1; L < n;) {
-        const int rem = n / L;
+        const int rem = n / L < max_radix ? n / L : max_radix;
         if (rem >= 16) {
             stockham_stage<16>(a, b, n, log2n, L, nseq, sstride, tw, nmax, inverse);
             L <<= 4;
-        } else if (rem == 8) {
+        } else if (rem >= 8) {
             stockham_stage<8>(a, b, n, log2n, L, nseq, sstride, tw, nmax, inverse);
             L <<= 3;
-        } else if (rem == 4) {
+        } else if (rem >= 4) {
             stockham_stage<4>(a, b, n, log2n, L, nseq, sstride, tw, nmax, inverse);
             L <<= 2;
         } else {
@@ -208,7 +209,7 @@ __global__ void pc_rows_forward(PcDims d, PcArgs A, int prologue)
     }
     __syncthreads();
     const int nrows = min(rpc, d.R - r0);
-    float2 *res = fft_smem(a, b, C, d.logC, nrows, S, s_tw, d.nmax, false);
+    float2 *res = fft_smem(a, b, C, d.logC, nrows, S, s_tw, d.nmax, false, d.fft_radix);
     for (int e = threadIdx.x; e < nrows * C; e += blockDim.x)
         A.work[vb + (size_t)r0 * C + e] = res[fpos(e / C, e % C, S)];
 }
@@ -229,7 +230,7 @@ __global__ void pc_cols_filter(PcDims d, PcArgs A, const float2 *__restrict__ tr
         a[fpos(q, r, S)] = A.work[vb + (size_t)r * C + c0 + q];
     }
     __syncthreads();
-    float2 *res = fft_smem(a, b, R, d.logR, cb, S, s_tw, d.nmax, false);
+    float2 *res = fft_smem(a, b, R, d.logR, cb, S, s_tw, d.nmax, false, d.fft_radix);
     float2 *other = res == a ? b : a;
     for (int e = threadIdx.x; e < cb * R; e += blockDim.x) {
         const int r = e / cb, q = e % cb;
@@ -237,7 +238,7 @@ __global__ void pc_cols_filter(PcDims d, PcArgs A, const float2 *__restrict__ tr
         res[i] = cmul(res[i], transfer[(size_t)r * C + c0 + q]);
     }
     __syncthreads();
-    res = fft_smem(res, other, R, d.logR, cb, S, s_tw, d.nmax, true);
+    res = fft_smem(res, other, R, d.logR, cb, S, s_tw, d.nmax, true, d.fft_radix);
     for (int e = threadIdx.x; e < cb * R; e += blockDim.x) {
         const int r = e / cb, q = e % cb;
         A.work[vb + (size_t)r * C + c0 + q] = res[fpos(q, r, S)];
@@ -259,7 +260,7 @@ __global__ void pc_rows_inverse(PcDims d, PcArgs A, int epilogue)
     const size_t vb = (size_t)v * d.N;
     for (int e = threadIdx.x; e < nrows * C; e += blockDim.x) a[fpos(e / C, e % C, S)] = A.work[vb + (size_t)r0 * C + e];
     __syncthreads();
-    float2 *res = fft_smem(a, b, C, d.logC, nrows, S, s_tw, d.nmax, true);
+    float2 *res = fft_smem(a, b, C, d.logC, nrows, S, s_tw, d.nmax, true, d.fft_radix);
     const float inv_n = 1.0f / (float)d.N;
     double acc = 0.0;
     for (int e = threadIdx.x; e < nrows * C; e += blockDim.x) {

@@ -36,6 +36,7 @@ struct PcDims {
     int V, R, C, N, logR, logC, nmax;
     int rows_per_cta, cols_per_cta;
     float nu, delta_over_beta;
+    int fft_radix;  // largest radix of an FFT stage (2, 4, 8, 16)
 };
 
 // Device pointers (any may be null when the op does not use it).
@@ -82,7 +83,9 @@ __global__ void pc_nms_wavefront(PcDims d, PcArgs A, const __grid_constant__ PcP
 // Launch geometry of the three-pass transform for V views of R x C (powers of
 // two): fills d's sizes and per-CTA tiles, the dynamic shared memory of the
 // row and column passes, and raises the kernels' shared-memory limits.
-int pc_transform_dims(PcDims &d, int V, int R, int C, size_t *smem_rows, size_t *smem_cols);
+int pc_transform_dims(PcDims &d, int V, int R, int C, size_t *smem_rows, size_t *smem_cols, int fft_radix = 0);
+// the FFT stage radix used when none is asked for
+constexpr int kPcDefaultFftRadix = 4;
 // float2 slots one FFT sequence of length n takes in shared memory: n plus
 // one padding slot per 16, rounded up to an odd count
 __host__ __device__ inline int fft_seq_stride(int n) { return (n + n / 16) | 1; }

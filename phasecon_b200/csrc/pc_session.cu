@@ -34,7 +34,7 @@ double freq(int i, int n, double delta) { return i >= n / 2 ? -(double)(n - i) /
 
 }  // namespace
 
-int pc_transform_dims(PcDims &d, int V, int R, int C, size_t *smem_rows, size_t *smem_cols)
+int pc_transform_dims(PcDims &d, int V, int R, int C, size_t *smem_rows, size_t *smem_cols, int fft_radix)
 {
     d.V = V;
     d.R = R;
@@ -43,10 +43,14 @@ int pc_transform_dims(PcDims &d, int V, int R, int C, size_t *smem_rows, size_t 
     d.logR = ilog2(R);
     d.logC = ilog2(C);
     d.nmax = std::max(R, C);
-    // sequences per CTA: enough radix-16 butterflies (n / 16 per sequence) for
-    // the 256 threads, within the shared memory of the two padded buffers
-    d.rows_per_cta = std::max(1, std::min(R, 4096 / C));
-    d.cols_per_cta = std::max(1, std::min(C, 4096 / R));
+    d.fft_radix = fft_radix > 0 ? fft_radix : kPcDefaultFftRadix;
+    if (d.fft_radix != 2 && d.fft_radix != 4 && d.fft_radix != 8 && d.fft_radix != 16)
+        return fail("fft_radix must be 2, 4, 8 or 16 (got %d)", fft_radix);
+    // sequences per CTA: two radix-R butterflies per thread (n / R per
+    // sequence, 256 threads), at most 4,096 points in the two padded buffers
+    auto seqs = [&](int n) { return std::max(1, std::min(n, std::min(4096 / n, 512 * d.fft_radix / n))); };
+    d.rows_per_cta = seqs(C);
+    d.cols_per_cta = seqs(R);
     *smem_rows = (size_t)(d.nmax / 2 + 2 * d.rows_per_cta * fft_seq_stride(C)) * sizeof(float2);
     *smem_cols = (size_t)(d.nmax / 2 + 2 * d.cols_per_cta * fft_seq_stride(R)) * sizeof(float2);
     cudaError_t e = cudaFuncSetAttribute(pc_rows_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem_rows);
@@ -190,7 +194,7 @@ int PcSession::init(const mbirgpu_pc_problem *pb, const mbirgpu_pc_options *o, v
         return fail("phase retrieval needs power-of-two detector sizes up to 1024 (got %d x %d)", C, R);
     if (V < 1) return fail("proj_num must be positive");
     if (opt.nms_order != 0 && opt.nms_order != 1) return fail("nms_order must be 0 (raster) or 1 (colour classes)");
-    if (pc_transform_dims(d, V, R, C, &smem_rows, &smem_cols)) return -1;
+    if (pc_transform_dims(d, V, R, C, &smem_rows, &smem_cols, opt.fft_radix)) return -1;
     d.nu = (float)opt.nu;
     dob = pb->pag_regparam;
     d.delta_over_beta = (float)dob;
@@ -482,6 +486,7 @@ void mbirgpu_pc_default_options(mbirgpu_pc_options *o)
     o->mrf_p = 1.2;
     o->mrf_q = 2.0;
     o->nms_order = 0;
+    o->fft_radix = 0;
 }
 
 int mbirgpu_pc_session_create(mbirgpu_pc_session **out, const mbirgpu_pc_problem *pb, const mbirgpu_pc_options *opt,

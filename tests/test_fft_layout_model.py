@@ -7,7 +7,7 @@ of sequence q at q * S + i + i // 16, S = (n + n // 16) | 1) and run radix-16
 Stockham stages (radix 8, 4 or 2 for the rest) whose butterfly j reads
 x_p = a[j + p n / R], multiplies by w_{RL}^{p (j mod L)}, transforms the R
 points and writes them to (j - j mod L) R + j mod L + p L. This model runs
-the same formulas (the same twiddle table: the half circle exp(-2 pi i m /
+the same formulas for each largest stage radix (the same twiddle table: the half circle exp(-2 pi i m /
 nmax), m < nmax / 2) in FP64; it must reproduce the DFT for every power of
 two the kernels accept and never address outside its buffers.
 """
@@ -50,7 +50,7 @@ def _fpos(q, i, S):
     return q * S + i + (i >> 4)
 
 
-def fft_model(seqs, nmax, inv):
+def fft_model(seqs, nmax, inv, max_radix=16):
     nseq, n = seqs.shape
     S = (n + n // 16) | 1
     size = nseq * S
@@ -62,8 +62,8 @@ def fft_model(seqs, nmax, inv):
             a[_fpos(q, i, S)] = seqs[q, i]
     L, log2n = 1, n.bit_length() - 1
     while L < n:
-        rem = n // L
-        R = 16 if rem >= 16 else rem if rem in (8, 4) else 2
+        rem = min(n // L, max_radix)
+        R = 16 if rem >= 16 else 8 if rem >= 8 else 4 if rem >= 4 else 2
         lr = R.bit_length() - 1
         lm = log2n - lr
         m = 1 << lm
@@ -89,13 +89,14 @@ def fft_model(seqs, nmax, inv):
     return np.array([[a[_fpos(q, i, S)] for i in range(n)] for q in range(nseq)])
 
 
+@pytest.mark.parametrize("max_radix", [2, 4, 8, 16])
 @pytest.mark.parametrize("n", [2, 4, 8, 16, 32, 64, 128, 256, 512, 1024])
-def test_stockham_schedule_reproduces_the_dft(n):
+def test_stockham_schedule_reproduces_the_dft(n, max_radix):
     rng = np.random.default_rng(n)
     for nmax in sorted({n, 1024}):
         x = rng.normal(size=(2, n)) + 1j * rng.normal(size=(2, n))
-        fwd = fft_model(x, nmax, False)
-        inv = fft_model(x, nmax, True)
+        fwd = fft_model(x, nmax, False, max_radix)
+        inv = fft_model(x, nmax, True, max_radix)
         assert np.abs(fwd - np.fft.fft(x, axis=1)).max() <= 1e-12 * np.abs(fwd).max()
         assert np.abs(inv - np.fft.ifft(x, axis=1) * n).max() <= 1e-12 * np.abs(inv).max()
 
