@@ -86,10 +86,6 @@ typedef struct {
                                 same schedule and the same image on every run; 1: a single
                                 session measures the candidate schedules on its own problem and
                                 keeps the fastest (timing-dependent); batches always measure */
-    int32_t icd_overlap;     /* 1: in each column update one warp gathers the prior neighbourhood
-                                while the CTA's other warps accumulate theta1 / theta2 (the two
-                                are independent); 0 (default): every warp takes part in both,
-                                one after the other */
     int32_t graph_iterations;/* 1 (default): a session on a stream of its own (not the legacy
                                 default stream) replays each ICD iteration -- colour phases,
                                 non-homogeneous passes, FP64 refresh -- from a CUDA graph captured

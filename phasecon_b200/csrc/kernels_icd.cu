@@ -317,9 +317,7 @@ __device__ __forceinline__ void theta_pass(const IcdConst &K, const uint32_t *co
 // round trip per view group instead of two and the apply pass on none.
 // kHuber: 0 the quadratic data term, 1 the generalised Huber one
 // (XT_VoxUpdate.c:68-82), 2 decided per problem at run time (K.huber).
-// kOverlap: warp 0 gathers the prior neighbourhood while warps 1..W-1 run the
-// theta pass (used when the launch has at least 2 warps).
-template <int KW, int kUnroll, int VEC, bool kStaged, int kHuber, bool kOverlap>
+template <int KW, int kUnroll, int VEC, bool kStaged, int kHuber>
 __device__ __forceinline__ void icd_update_sv(const Geom &g, const IcdLaunch &L, const IcdConst &K,
                                               const uint32_t *__restrict__ table,
                                               const int32_t *__restrict__ view_first,
@@ -346,14 +344,6 @@ __device__ __forceinline__ void icd_update_sv(const Geom &g, const IcdLaunch &L,
     const int G = 32 / lprp;  // view groups per warp
     const int grp = lane / lprp, tq = lane % lprp;
     const int t0 = tq * VEC;  // first detector row of this lane within the chunk
-    // overlap mode: warp 0 gathers the prior neighbourhood of the column while
-    // warps 1..W-1 run the theta pass (independent work), so theta is split
-    // over W - 1 warps and the neighbourhood needs no cross-warp sum
-    const bool ovl = kOverlap && W >= 2;
-    const int tw = ovl ? W - 1 : W, twarp = ovl ? warp - 1 : warp;  // theta warps, this warp's rank
-    // theta: the view groups of the theta warps; apply: those of every warp
-    const int tgstride = tw * G;
-    const int tgfirst = twarp * G + grp;  // negative for warp 0 in overlap mode, which runs no theta
     const int gstride = W * G;
     const int gfirst = warp * G + grp;
     const int fv0 = view_first[f], nv = view_first[f + 1] - fv0;
@@ -412,28 +402,13 @@ __device__ __forceinline__ void icd_update_sv(const Geom &g, const IcdLaunch &L,
             const int z = z0 + lane;                                 // this lane's slice
             const bool row_ok = tq < ct / VEC;
 
-            // overlap mode: the previous chunk's / column's apply pass is complete
-            // before this theta pass reads e (the neighbourhood barrier below
-            // comes after theta in that mode)
-            if (ovl) __syncthreads();
-
-            // ---- 1. neighbourhood (sources split over warps, or all on warp 0) ----
+            // ---- 1. neighbourhood (sources split over warps) + column activity ------
             int active_pred;
             const float V = zl ? x[col_off + z] : 0.0f;  // the column itself (warp 0 reuses it in the solve)
-            float th1[VEC], th2[VEC];
-#pragma unroll
-            for (int i = 0; i < VEC; i++) th1[i] = th2[i] = 0.0f;
-            if (kStaged && ch == 0 && ovl)  // issued one column earlier; theta reads it next
-                wait_staged(&S.stage_bar[ci & 1], cnt.phases, ci & 1, cnt.timeouts, S.abort, S.abort_bar,
-                            S.abort_parity);
-            if (ovl && warp > 0 && row_ok)
-                theta_pass<KW, kUnroll, VEC, kStaged, kHuber>(K, col_rec, err, wgt, tgfirst, tgstride, nv, RW, NT,
-                                                             rbase + t0, th1, th2);
             {
                 float num = 0.0f, den = 0.0f;
                 int pos = 0;
-                const int s_first = ovl ? (warp == 0 ? 0 : 10) : warp, s_step = ovl ? 1 : W;
-                for (int s = s_first; s < 10; s += s_step) {
+                for (int s = warp; s < 10; s += W) {
                     if (s < 8) {
                         const int o = s < 4 ? s : s + 1;  // skip the centre of the 3x3
                         const int dy = o / 3 - 1, dx = o % 3 - 1;
@@ -478,9 +453,8 @@ __device__ __forceinline__ void icd_update_sv(const Geom &g, const IcdLaunch &L,
                 // a column is skipped only if every slice is zero with no positive
                 // neighbour (in-column neighbours are the column's own values)
                 active_pred = !L.zero_skipping || iter <= 1 || (zl && V != 0.0f) || pos;
-                if (ovl && warp > 0) active_pred = 0;  // only warp 0 saw the neighbourhood
             }
-            if (kStaged && ch == 0 && !ovl)  // issued one column earlier
+            if (kStaged && ch == 0)  // issued one column earlier
                 wait_staged(&S.stage_bar[ci & 1], cnt.phases, ci & 1, cnt.timeouts, S.abort, S.abort_bar,
                             S.abort_parity);
             const int any_active = __syncthreads_or(active_pred);
@@ -501,10 +475,13 @@ __device__ __forceinline__ void icd_update_sv(const Geom &g, const IcdLaunch &L,
                 continue;  // uniform across the CTA
             }
 
-            // ---- 2. theta over the column's views (already done in overlap mode) ---
+            // ---- 2. theta over the column's views -----------------------------------
             {
-                if (!ovl && row_ok)
-                    theta_pass<KW, kUnroll, VEC, kStaged, kHuber>(K, col_rec, err, wgt, tgfirst, tgstride, nv, RW, NT,
+                float th1[VEC], th2[VEC];
+#pragma unroll
+                for (int i = 0; i < VEC; i++) th1[i] = th2[i] = 0.0f;
+                if (row_ok)
+                    theta_pass<KW, kUnroll, VEC, kStaged, kHuber>(K, col_rec, err, wgt, gfirst, gstride, nv, RW, NT,
                                                                  rbase + t0, th1, th2);
                 // fold the view groups of the warp onto group 0
                 for (int off = lprp; off < 32; off <<= 1) {
@@ -514,7 +491,7 @@ __device__ __forceinline__ void icd_update_sv(const Geom &g, const IcdLaunch &L,
                         th2[i] += __shfl_xor_sync(0xffffffffu, th2[i], off);
                     }
                 }
-                if (grp == 0 && row_ok && !(ovl && warp == 0)) {
+                if (grp == 0 && row_ok) {
 #pragma unroll
                     for (int i = 0; i < VEC; i++) {
                         S.th1[warp][t0 + i] = th1[i];
@@ -522,7 +499,7 @@ __device__ __forceinline__ void icd_update_sv(const Geom &g, const IcdLaunch &L,
                     }
                 }
             }
-            if (!ovl) __syncthreads();  // in overlap mode theta finished before the neighbourhood barrier
+            __syncthreads();
 
             // ---- 3. zero-skipping and solve (warp 0, lane = slice of the chunk) ------
             if (warp == 0) {
@@ -530,12 +507,10 @@ __device__ __forceinline__ void icd_update_sv(const Geom &g, const IcdLaunch &L,
                 float numA = 0.0f, denA = 0.0f, t1 = 0.0f, t2 = 0.0f;
                 int pos = 0;
                 for (int w = 0; w < W; w++) {
-                    if (!ovl || w == 0) {
-                        numA += S.num[w][lane];
-                        denA += S.den[w][lane];
-                        pos |= S.pos[w][lane];
-                    }
-                    if (lane < ct && !(ovl && w == 0)) {
+                    numA += S.num[w][lane];
+                    denA += S.den[w][lane];
+                    pos |= S.pos[w][lane];
+                    if (lane < ct) {
                         t1 += S.th1[w][lane];
                         t2 += S.th2[w][lane];
                     }
@@ -655,8 +630,8 @@ __device__ __forceinline__ void icd_update_sv(const Geom &g, const IcdLaunch &L,
 // One colour phase of one problem: persistent CTAs drain the phase's SV queue.
 // With kStaged, the dynamic shared memory holds two record buffers of
 // stage_words words each (the current and the next column's A records).
-template <int KW, int kUnroll, int VEC, bool kStaged, int kHuber, bool kOverlap>
-__global__ void __launch_bounds__(kMaxWarps * 32, kOverlap ? 3 : 4) icd_phase_kernel(
+template <int KW, int kUnroll, int VEC, bool kStaged, int kHuber>
+__global__ void __launch_bounds__(kMaxWarps * 32, 4) icd_phase_kernel(
     Geom g, IcdLaunch L, IcdConst K, const uint32_t *__restrict__ table, const int32_t *__restrict__ view_first,
     const uint8_t *__restrict__ mask, float *__restrict__ x, float *__restrict__ err, const float *__restrict__ wgt,
     float *__restrict__ mag, IcdStats *__restrict__ stats, unsigned int *__restrict__ queue, int stage_words)
@@ -696,8 +671,8 @@ __global__ void __launch_bounds__(kMaxWarps * 32, kOverlap ? 3 : 4) icd_phase_ke
             sy = KC * (rem / hx) + color / KC;
         }
         if (sx >= L.n_sv_x || sy >= L.n_sv_y) continue;  // uniform
-        icd_update_sv<KW, kUnroll, VEC, kStaged, kHuber, kOverlap>(g, L, K, table, view_first, mask, x, err, wgt, mag, f,
-                                                                   sx, sy, S,
+        icd_update_sv<KW, kUnroll, VEC, kStaged, kHuber>(g, L, K, table, view_first, mask, x, err, wgt, mag, f, sx, sy,
+                                                         S,
                                                  cnt, s_rec, stage_words);
     }
     // after an abort, the late copy may still write into this CTA's shared
@@ -710,7 +685,7 @@ __global__ void __launch_bounds__(kMaxWarps * 32, kOverlap ? 3 : 4) icd_phase_ke
 // above this size the sweep reads records from global memory instead.
 constexpr int kMaxStageBytes = 16 * 1024;
 
-template <int KW, int U, int VEC, bool kStaged, int kHuber, bool kOverlap>
+template <int KW, int U, int VEC, bool kStaged, int kHuber>
 static void launch_staged(const Geom &g, const IcdLaunch &L, const IcdConst &K, const uint32_t *d_table,
                           const int32_t *d_view_first, const uint8_t *d_mask, float *d_x, float *d_err,
                           const float *d_w, float *d_mag, IcdStats *d_stats, unsigned int *d_queue, int stage_words,
@@ -741,7 +716,7 @@ static void launch_staged(const Geom &g, const IcdLaunch &L, const IcdConst &K, 
         if (!hit) {
             cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                &per_sm, icd_phase_kernel<KW, U, VEC, kStaged, kHuber, kOverlap>, threads, smem);
+                &per_sm, icd_phase_kernel<KW, U, VEC, kStaged, kHuber>, threads, smem);
             cache.push_back({dev, threads, sms, per_sm, smem});
         }
     }
@@ -749,7 +724,7 @@ static void launch_staged(const Geom &g, const IcdLaunch &L, const IcdConst &K, 
     long long grid = (long long)sms * (per_sm > 0 ? per_sm : 1);
     if (grid > items) grid = items;
     if (L.max_ctas > 0 && grid > L.max_ctas) grid = L.max_ctas;
-    icd_phase_kernel<KW, U, VEC, kStaged, kHuber, kOverlap><<<(unsigned)grid, threads, smem, st>>>(
+    icd_phase_kernel<KW, U, VEC, kStaged, kHuber><<<(unsigned)grid, threads, smem, st>>>(
         g, L, K, d_table, d_view_first, d_mask, d_x, d_err, d_w, d_mag, d_stats, d_queue, stage_words);
 }
 
@@ -760,20 +735,15 @@ static void launch_kw(const Geom &g, const IcdLaunch &L, const IcdConst &K, cons
 {
     const int stage_words = g.max_views * g.rec_words;  // a multiple of 4 words: 16-byte aligned buffers
     const bool staged = L.stage_records && 2 * (size_t)stage_words * sizeof(uint32_t) <= (size_t)kMaxStageBytes;
-#define MBIR_STAGED(S, H, O)                                                                                      \
-    launch_staged<KW, U, VEC, S, H, O>(g, L, K, d_table, d_view_first, d_mask, d_x, d_err, d_w, d_mag, d_stats,       \
-                                       d_queue, S ? stage_words : 0, st)
-    // the overlapped column update is built for the staged single-record-word
-    // sweep (voxel scale 1, the common case)
-    if (staged && KW == 1 && L.overlap && L.warps >= 2) {
-        if (K.huber) MBIR_STAGED(true, 1, true);
-        else MBIR_STAGED(true, 0, true);
-    } else if (staged) {
-        if (K.huber) MBIR_STAGED(true, 1, false);
-        else MBIR_STAGED(true, 0, false);
+#define MBIR_STAGED(S, H)                                                                                         \
+    launch_staged<KW, U, VEC, S, H>(g, L, K, d_table, d_view_first, d_mask, d_x, d_err, d_w, d_mag, d_stats, d_queue, \
+                                    S ? stage_words : 0, st)
+    if (staged) {
+        if (K.huber) MBIR_STAGED(true, 1);
+        else MBIR_STAGED(true, 0);
     } else {
-        if (K.huber) MBIR_STAGED(false, 1, false);
-        else MBIR_STAGED(false, 0, false);
+        if (K.huber) MBIR_STAGED(false, 1);
+        else MBIR_STAGED(false, 0);
     }
 #undef MBIR_STAGED
 }
@@ -875,7 +845,7 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 4) icd_batch_kernel(const Batc
         const int sx = K * (rem % hx) + color % K;
         const int sy = K * (rem / hx) + color / K;
         if (sx >= P.L.n_sv_x || sy >= P.L.n_sv_y) continue;
-        icd_update_sv<KW, kUnroll, VEC, false, 2, false>(P.g, P.L, P.K, P.table, P.view_first, P.mask, P.x, P.err, P.w, P.mag,
+        icd_update_sv<KW, kUnroll, VEC, false, 2>(P.g, P.L, P.K, P.table, P.view_first, P.mask, P.x, P.err, P.w, P.mag,
                                                f, sx, sy, S, cnt, nullptr, 0);
     }
     if (cur >= 0) flush_counts(cnt, P.stats);
@@ -927,7 +897,7 @@ int icd_grid(int warps)
     int dev = 0, sms = 148, per_sm = 1;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, icd_phase_kernel<1, 2, 4, false, 0, false>, warps * 32, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, icd_phase_kernel<1, 2, 4, false, 0>, warps * 32, 0);
     return sms * (per_sm > 0 ? per_sm : 1);
 }
 

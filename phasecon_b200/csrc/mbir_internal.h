@@ -140,7 +140,6 @@ struct IcdLaunch {
     int colors_k;         // K x K colour classes; phase p updates colour (p + frame) mod K^2
     long long max_ctas;   // cap on the persistent grid (sv_max_concurrent); 0 = none
     int stage_records;    // prefetch each next column's A records into shared memory (cp.async)
-    int overlap;          // warp 0 gathers the prior neighbourhood while the other warps run theta
     const int *iter_dev;  // if set, the iteration number is read here (graph-captured iterations)
     // optional explicit work list of the phase (non-homogeneous passes): items[i]
     // = frame << 22 | sv_y << 11 | sv_x, *n_items of them (device memory);

@@ -384,7 +384,6 @@ int Session::enqueue_iteration(int iter, bool graph_mode, int *launches_out)
     L.perm = spread_multiplier(sv_slots(g.N_x, g.N_y, sv, colors));
     L.max_ctas = sv_max_concurrent(g.N_x, g.N_y, g.N_time, sv, colors);
     L.stage_records = opt.stage_records;
-    L.overlap = opt.icd_overlap;
     const int phases = colors * colors;
     Geom gb = g;
     gb.N_p = n_assigned;
@@ -762,7 +761,6 @@ void mbirgpu_default_options(mbirgpu_options *o)
     o->nh_cta_warps = 0;
     o->nh_work_lists = 1;
     o->autotune = 0;
-    o->icd_overlap = 0;
     o->graph_iterations = 1;
 }
 
@@ -782,7 +780,6 @@ int mbirgpu_set_options(const mbirgpu_options *o)
         return fail("nh_sv_colors must be 0 (auto), 2 or 4");
     if (o->nh_cta_warps < 0 || o->nh_cta_warps > 8) return fail("nh_cta_warps must be 0 (auto) or 1..8");
     if (o->autotune != 0 && o->autotune != 1) return fail("autotune must be 0 (schedule by rule) or 1 (measured)");
-    if (o->icd_overlap != 0 && o->icd_overlap != 1) return fail("icd_overlap must be 0 or 1");
     if (o->graph_iterations != 0 && o->graph_iterations != 1) return fail("graph_iterations must be 0 or 1");
     mbirgpu_options cur = mbirgpu::current_options();
     (void)cur;

@@ -58,7 +58,7 @@ class Options(C.Structure):
         ("sv_size", C.c_int32), ("cta_warps", C.c_int32), ("icd_unroll", C.c_int32), ("seed", C.c_uint64),
         ("nhicd_passes", C.c_int32), ("sv_colors", C.c_int32), ("stage_records", C.c_int32),
         ("nh_sv_size", C.c_int32), ("nh_sv_colors", C.c_int32), ("nh_cta_warps", C.c_int32),
-        ("nh_work_lists", C.c_int32), ("autotune", C.c_int32), ("icd_overlap", C.c_int32),
+        ("nh_work_lists", C.c_int32), ("autotune", C.c_int32), 
         ("graph_iterations", C.c_int32),
     ]
 

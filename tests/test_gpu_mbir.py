@@ -104,12 +104,9 @@ def _run_icd(s, iters):
     return np.array(costs)
 
 
-@pytest.mark.parametrize("overlap", [0, 1])
-def test_icd_converges_to_reference_cost_4d(overlap):
-    """Both column-update forms: every warp through neighbourhood then theta,
-    or warp 0 on the neighbourhood while the other warps run theta."""
+def test_icd_converges_to_reference_cost_4d():
     pb = golden_problem("quad")
-    s = gpu_session(pb, sv_size=4, icd_overlap=overlap)
+    s = gpu_session(pb, sv_size=4)
     costs = _run_icd(s, 60)
     ref = GOLD["quad_icd20_cost"]
     assert costs[0] == pytest.approx(ref[0], rel=1e-6)
