@@ -521,7 +521,8 @@ def warmstart_section(args, rank: int, local: int, pb, p: float) -> dict:
     `--train-ellipsoids` seeded single-frame ellipsoid phantoms scanned with one
     frame's views; input = the GPU FBP, target = plain GPU ICD to rel 1e-4;
     seeds other than the benchmark's), `--ws-seeds` networks trained on it from
-    different seeds, then plain ICD on the benchmark scan timed to the plain
+    different seeds (each ending on the checkpoint with the lowest loss on two
+    held-out scans), then plain ICD on the benchmark scan timed to the plain
     method's converged cost (x (1 + 1e-4)) from zero, from FBP and from each
     network's output; each time includes its initialisation (FBP, network,
     error sinogram) and follows one untimed run of the same start."""
@@ -538,6 +539,8 @@ def warmstart_section(args, rank: int, local: int, pb, p: float) -> dict:
     for i in range(args.train_ellipsoids):
         x, t, _ = WS.training_pair(5000 + rank * 100000 + i, kind="ellipsoids")
         pairs.append((x, t))
+    # two held-out scans pick each training's checkpoint (never trained on)
+    val_pairs = WS.training_pairs_4d(9000 + rank * 100000) + WS.training_pairs_4d(9001 + rank * 100000)
     t_data = time.perf_counter() - t0
     opt = pc.get_options()
     opt.mrf_p = p
@@ -568,7 +571,8 @@ def warmstart_section(args, rank: int, local: int, pb, p: float) -> dict:
         net = WS.UNet(16, seed=rank * 1000 + k)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        hist = WS.train(net, pairs, args.train_steps, lr=1e-3, seed=rank * 1000 + k, average_from=args.average_from)
+        hist = WS.train(net, pairs, args.train_steps, lr=1e-3, seed=rank * 1000 + k, average_from=args.average_from,
+                        val_pairs=val_pairs)
         torch.cuda.synchronize()
         train_s.append(time.perf_counter() - t0)
         losses.append([float(np.mean(hist[:20])), float(np.mean(hist[-20:]))])
@@ -587,6 +591,7 @@ def warmstart_section(args, rank: int, local: int, pb, p: float) -> dict:
             "speedup_vs_fbp_init_per_seed": [tf / r["time_to_converged_cost_s"] for r in seeds],
             "target_cost": target, "starts": res, "unet_starts": seeds,
             "train": {"pairs": len(pairs), "cahn_hilliard_pairs": n_ch, "ellipsoid_pairs": len(pairs) - n_ch,
+                      "held_out_pairs": len(val_pairs),
                       "steps": args.train_steps, "seeds": args.ws_seeds, "data_s": t_data, "train_s": train_s,
                       "loss_first_last": losses},
             "unet": "4 levels 16/32/64/128, 3x3x3, BF16 weights and activations, FP32 accumulation",

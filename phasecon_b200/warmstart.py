@@ -230,19 +230,41 @@ def training_pairs_4d(seed: int, ch_steps: int | None = None, rel: float = 1e-4)
 
 
 def train(net: UNet, pairs, steps: int, lr: float = 1e-3, seed: int = 0, log_every: int = 0,
-          average_from: float = 1.0, average_every: int = 50):
+          average_from: float = 1.0, average_every: int = 50, val_pairs=None, val_every: int = 250):
     """Adam steps over randomly drawn (input, target) pairs of host arrays;
     returns the loss history. The network's input scale is set so that it
     sees values of order one. Learning rate: a cosine schedule from `lr` down
     to lr / 100 over all steps; with average_from < 1, the cosine runs down to
     lr / 10 over the first average_from of the steps, the rest run at lr / 10
     and the network ends as the average of its weights taken every
-    `average_every` steps over that tail (stochastic weight averaging)."""
+    `average_every` steps over that tail (stochastic weight averaging).
+
+    With `val_pairs` (held-out pairs, never trained on) the network ends as the
+    candidate with the lowest mean loss on them, the candidates being the
+    weights every `val_every` steps over the second half of the run, the
+    running weight average at the same points of the tail, and the final
+    average: single-sample Adam steps occasionally land on a worse point late
+    in a run, and a held-out loss picks the checkpoint before it."""
     import torch
     rng = np.random.default_rng(seed)
     net.input_scale = 1.0 / max(float(np.mean([np.abs(t).max() for _, t in pairs])), 1e-12)
-    dev = [(torch.from_numpy(np.ascontiguousarray(x, np.float32)).cuda(),
-            torch.from_numpy(np.ascontiguousarray(t, np.float32)).cuda()) for x, t in pairs]
+
+    def to_dev(ps):
+        return [(torch.from_numpy(np.ascontiguousarray(x, np.float32)).cuda(),
+                 torch.from_numpy(np.ascontiguousarray(t, np.float32)).cuda()) for x, t in ps]
+
+    dev = to_dev(pairs)
+    val = to_dev(val_pairs) if val_pairs else []
+    best = [np.inf, None]
+
+    def consider(params):
+        keep = net.get_params()
+        net.set_params(params.astype(np.float32))
+        loss = float(np.mean([net.gradients(x, t)[0] for x, t in val]))
+        net.set_params(keep)
+        if loss < best[0]:
+            best[0], best[1] = loss, params.astype(np.float32).copy()
+
     hist = []
     tail = int(average_from * steps) if average_from < 1.0 else steps
     avg, navg = None, 0
@@ -257,8 +279,15 @@ def train(net: UNet, pairs, steps: int, lr: float = 1e-3, seed: int = 0, log_eve
             p = net.get_params().astype(np.float64)
             avg = p if avg is None else avg + p
             navg += 1
+        if val and s >= steps // 2 and (s + 1) % val_every == 0:
+            consider(net.get_params())
+            if navg:
+                consider(avg / navg)
         if log_every and (s + 1) % log_every == 0:
             print(f"step {s + 1}: loss {np.mean(hist[-log_every:]):.4g}", flush=True)
     if navg:
         net.set_params((avg / navg).astype(np.float32))
+    if val:
+        consider(net.get_params())
+        net.set_params(best[1])
     return hist
