@@ -34,12 +34,11 @@ __device__ __forceinline__ float cabs2(float2 a) { return a.x * a.x + a.y * a.y;
 // the column pass's transposed staging spread over the banks.
 __device__ __forceinline__ int fpos(int q, int i, int sstride) { return q * sstride + i + (i >> 4); }
 
-// exp(-+ 2 pi i m / nmax) for any 0 <= m < nmax from the half-circle table
-// (tw[m] = exp(-2 pi i m / nmax), m < nmax / 2; the other half is -tw).
+// exp(-+ 2 pi i m / nmax), 0 <= m < nmax, from the full-circle table the
+// kernels keep in shared memory (load_twiddles).
 __device__ __forceinline__ float2 twid(const float2 *tw, int m, int nmax, bool inverse)
 {
-    const int h = nmax >> 1;
-    float2 w = m < h ? tw[m] : make_float2(-tw[m - h].x, -tw[m - h].y);
+    float2 w = tw[m];
     if (inverse) w.y = -w.y;
     return w;
 }
@@ -138,9 +137,16 @@ __device__ float2 *fft_smem(float2 *a, float2 *b, int n, int log2n, int nseq, in
     return a;
 }
 
+// The full circle exp(-2 pi i m / nmax), m < nmax, from the half-circle
+// table tw (m < nmax / 2; the other half is -tw).
 __device__ __forceinline__ void load_twiddles(float2 *s_tw, const float2 *tw, int nmax)
 {
-    for (int i = threadIdx.x; i < nmax / 2; i += blockDim.x) s_tw[i] = tw[i];
+    const int h = nmax / 2;
+    for (int i = threadIdx.x; i < h; i += blockDim.x) {
+        const float2 w = tw[i];
+        s_tw[i] = w;
+        s_tw[i + h] = make_float2(-w.x, -w.y);
+    }
 }
 
 // FP64 block sum of per-thread values, one atomicAdd per CTA.
@@ -186,7 +192,7 @@ __global__ void pc_rows_forward(PcDims d, PcArgs A, int prologue)
     const int v = blockIdx.y;
     if (A.active && !A.active[v]) return;
     const int C = d.C, rpc = d.rows_per_cta, S = fft_seq_stride(C);
-    float2 *s_tw = smem, *a = smem + d.nmax / 2, *b = a + rpc * S;
+    float2 *s_tw = smem, *a = smem + d.nmax, *b = a + rpc * S;
     load_twiddles(s_tw, A.tw, d.nmax);
     const int r0 = blockIdx.x * rpc;
     const size_t vb = (size_t)v * d.N;
@@ -221,7 +227,7 @@ __global__ void pc_cols_filter(PcDims d, PcArgs A, const float2 *__restrict__ tr
     const int v = blockIdx.y;
     if (A.active && !A.active[v]) return;
     const int R = d.R, C = d.C, cb = d.cols_per_cta, S = fft_seq_stride(R);
-    float2 *s_tw = smem, *a = smem + d.nmax / 2, *b = a + cb * S;
+    float2 *s_tw = smem, *a = smem + d.nmax, *b = a + cb * S;
     load_twiddles(s_tw, A.tw, d.nmax);
     const int c0 = blockIdx.x * cb;
     const size_t vb = (size_t)v * d.N;
@@ -253,7 +259,7 @@ __global__ void pc_rows_inverse(PcDims d, PcArgs A, int epilogue)
     const int v = blockIdx.y;
     if (A.active && !A.active[v]) return;
     const int C = d.C, rpc = d.rows_per_cta, S = fft_seq_stride(C);
-    float2 *s_tw = smem, *a = smem + d.nmax / 2, *b = a + rpc * S;
+    float2 *s_tw = smem, *a = smem + d.nmax, *b = a + rpc * S;
     load_twiddles(s_tw, A.tw, d.nmax);
     const int r0 = blockIdx.x * rpc;
     const int nrows = min(rpc, d.R - r0);

@@ -123,132 +123,6 @@ void launch_forward_project(const Geom &g, const uint32_t *d_table, const int32_
     finish_projection_kernel<<<148 * 8, 256, 0, st>>>(n, d_acc, d_y, d_out, d_off, g.N_r * g.N_t);
 }
 
-// View-driven forward projection: one CTA per group of G consecutive view
-// positions of views[] (frame-major). The group's sinogram rows, G x N_r x
-// N_t, accumulate in FP64 in shared memory while the CTA's warps sweep every
-// voxel column of the view's frame (lane = detector row, U columns in flight
-// per warp); the rows are then rounded once and written as e = y - Ax - d.
-// No global atomics: the CTA owns its rows.
-template <int G, int U>
-__global__ void __launch_bounds__(512) forward_project_views_kernel(
-    Geom g, const uint32_t *__restrict__ table, const int32_t *__restrict__ view_first,
-    const int32_t *__restrict__ views, const int32_t *__restrict__ view_frame, int n_assigned,
-    const float *__restrict__ x, const float *__restrict__ y, const float *__restrict__ off, float *__restrict__ out)
-{
-    extern __shared__ double s_acc[];  // [G][N_r * N_t]
-    const int nrt = g.N_r * g.N_t, nxy = g.N_x * g.N_y, RW = g.rec_words;
-    const int p0 = blockIdx.x * G;
-    const int np = min(G, n_assigned - p0);
-    for (int i = threadIdx.x; i < G * nrt; i += blockDim.x) s_acc[i] = 0.0;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, W = blockDim.x >> 5;
-    const bool row_ok = lane < g.N_t;
-    const int zl = row_ok ? lane / g.z_overlap : 0;
-    // per view of the group: its frame's volume, its first record and the
-    // record stride from one column to the next, its first sinogram row
-    const float *xk[G];
-    const uint32_t *rk[G];
-    size_t stride[G];
-    int row0[G];
-#pragma unroll
-    for (int k = 0; k < G; k++) {
-        const int pos = p0 + (k < np ? k : 0);
-        const int f = view_frame[pos], fv0 = view_first[f], nv = view_first[f + 1] - fv0;
-        xk[k] = x + (size_t)f * nxy * g.N_z + zl;
-        rk[k] = table + ((size_t)fv0 * nxy + (pos - fv0)) * RW;
-        stride[k] = (size_t)nv * RW;
-        row0[k] = views[pos] * g.N_r;
-    }
-    __syncthreads();
-    for (int c0 = warp * U; c0 < nxy; c0 += W * U) {
-#pragma unroll
-        for (int k = 0; k < G; k++) {
-            if (k >= np) break;
-            float xv[U];
-            uint4 rec[U];
-#pragma unroll
-            for (int u = 0; u < U; u++) {
-                const int c = c0 + u;
-                const bool in = c < nxy;
-                xv[u] = (in && row_ok) ? __ldg(xk[k] + (size_t)c * g.N_z) : 0.0f;
-                // the record's first 16 bytes: header + up to 3 weights (kmax <= 3 here)
-                rec[u] = in ? __ldg(reinterpret_cast<const uint4 *>(rk[k] + (size_t)c * stride[k])) : make_uint4(0, 0, 0, 0);
-            }
-#pragma unroll
-            for (int u = 0; u < U; u++) {
-                if (!row_ok || xv[u] == 0.0f) continue;
-                const uint32_t hdr = rec[u].x;
-                const int cnt = hdr >> 24, row = (int)(hdr & 0xFFFFFFu) - row0[k];
-                double *a = s_acc + (size_t)k * nrt + (size_t)row * g.N_t + lane;
-                const double xd = (double)xv[u];
-                if (cnt > 0) atomicAdd(a, xd * (double)__uint_as_float(rec[u].y));
-                if (cnt > 1) atomicAdd(a + g.N_t, xd * (double)__uint_as_float(rec[u].z));
-                if (cnt > 2) atomicAdd(a + 2 * g.N_t, xd * (double)__uint_as_float(rec[u].w));
-            }
-        }
-    }
-    __syncthreads();
-    for (int k = 0; k < np; k++) {
-        const size_t base = (size_t)views[p0 + k] * nrt;
-        for (int i = threadIdx.x; i < nrt; i += blockDim.x) {
-            const double a = s_acc[(size_t)k * nrt + i];
-            if (!y) {
-                out[base + i] = (float)a;
-            } else {
-                const float e = (float)((double)y[base + i] - a);
-                out[base + i] = off ? e - off[i] : e;  // initErrorSinogam, XT_ICD_update.c:689
-            }
-        }
-    }
-}
-
-// Rows of views that belong to no frame: e = y - d (or 0 without y).
-__global__ void unassigned_rows_kernel(size_t n, int nrt, const float *__restrict__ y, const float *__restrict__ off,
-                                       float *__restrict__ out)
-{
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-        out[i] = y ? (off ? y[i] - off[i % nrt] : y[i]) : 0.0f;
-}
-
-template <int G>
-static bool launch_views_g(const Geom &g, const uint32_t *d_table, const int32_t *d_view_first,
-                           const int32_t *d_views, const int32_t *d_view_frame, int n_assigned, const float *d_x,
-                           const float *d_y, float *d_out, cudaStream_t st, const float *d_off)
-{
-    constexpr int U = 4;
-    const size_t smem = (size_t)G * g.N_r * g.N_t * sizeof(double);
-    // the attribute belongs to the current device; a launch being captured
-    // into a CUDA graph relies on the one set by an earlier direct launch
-    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
-    if (cudaStreamIsCapturing(st, &cs) != cudaSuccess) return false;
-    if (cs == cudaStreamCaptureStatusNone &&
-        cudaFuncSetAttribute(forward_project_views_kernel<G, U>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             kViewProjMaxSmem) != cudaSuccess)
-        return false;
-    const unsigned blocks = (unsigned)((n_assigned + G - 1) / G);
-    forward_project_views_kernel<G, U><<<blocks, 512, smem, st>>>(g, d_table, d_view_first, d_views, d_view_frame,
-                                                                  n_assigned, d_x, d_y, d_off, d_out);
-    return true;
-}
-
-bool launch_forward_project_views(const Geom &g, const uint32_t *d_table, const int32_t *d_view_first,
-                                  const int32_t *d_views, const int32_t *d_view_frame, int n_assigned,
-                                  const float *d_x, const float *d_y, float *d_out, cudaStream_t st,
-                                  const float *d_off)
-{
-    const size_t view_bytes = (size_t)g.N_r * g.N_t * sizeof(double);
-    if (g.N_t > 32 || g.kmax > 3 || view_bytes > (size_t)kViewProjMaxSmem || n_assigned < 1) return false;
-    if (n_assigned < g.N_p) {  // every row first, the assigned views' rows are overwritten
-        const size_t n = (size_t)g.N_p * g.N_r * g.N_t;
-        unassigned_rows_kernel<<<148 * 4, 256, 0, st>>>(n, g.N_r * g.N_t, d_y, d_off, d_out);
-    }
-    // groups of views whose shared-memory rows still let two CTAs share an SM
-    if (4 * view_bytes <= (size_t)kViewProjMaxSmem / 2)
-        return launch_views_g<4>(g, d_table, d_view_first, d_views, d_view_frame, n_assigned, d_x, d_y, d_out, st, d_off);
-    if (2 * view_bytes <= (size_t)kViewProjMaxSmem / 2)
-        return launch_views_g<2>(g, d_table, d_view_first, d_views, d_view_frame, n_assigned, d_x, d_y, d_out, st, d_off);
-    return launch_views_g<1>(g, d_table, d_view_first, d_views, d_view_frame, n_assigned, d_x, d_y, d_out, st, d_off);
-}
-
 // One warp per (frame, column, chunk of 32 detector rows); out is
 // [N_time][N_y][N_x][N_z].
 __global__ void back_project_kernel(Geom g, const uint32_t *__restrict__ table,

@@ -83,17 +83,6 @@ void launch_forward_project(const Geom &g, const uint32_t *d_table, const int32_
                             const float *d_x, const float *d_y, double *d_acc, float *d_out, cudaStream_t st,
                             const float *d_off = nullptr);
 
-// The same projection driven by views (one CTA per group of views, FP64
-// accumulation in shared memory, no global atomics) for sessions whose
-// records hold at most 3 weights, N_t <= 32 and one view's rows fit in
-// kViewProjMaxSmem bytes of FP64; returns false (nothing launched) otherwise.
-// d_views / d_view_frame: view index and frame of each view position.
-constexpr int kViewProjMaxSmem = 200 * 1024;
-bool launch_forward_project_views(const Geom &g, const uint32_t *d_table, const int32_t *d_view_first,
-                                  const int32_t *d_views, const int32_t *d_view_frame, int n_assigned,
-                                  const float *d_x, const float *d_y, float *d_out, cudaStream_t st,
-                                  const float *d_off = nullptr);
-
 // Ring correction (kernels_offset.cu): one update of the per-detector-pixel
 // offset d (mode 1 unconstrained, 2 zero mean, 3 the reference's window mode,
 // which in its reconstruct has no windows) with e changed by the offset's

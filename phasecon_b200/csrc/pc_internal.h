@@ -85,7 +85,7 @@ __global__ void pc_nms_wavefront(PcDims d, PcArgs A, const __grid_constant__ PcP
 // row and column passes, and raises the kernels' shared-memory limits.
 int pc_transform_dims(PcDims &d, int V, int R, int C, size_t *smem_rows, size_t *smem_cols, int fft_radix = 0);
 // the FFT stage radix used when none is asked for
-constexpr int kPcDefaultFftRadix = 4;
+constexpr int kPcDefaultFftRadix = 8;
 // float2 slots one FFT sequence of length n takes in shared memory: n plus
 // one padding slot per 16, rounded up to an odd count
 __host__ __device__ inline int fft_seq_stride(int n) { return (n + n / 16) | 1; }

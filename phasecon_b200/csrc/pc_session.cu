@@ -46,13 +46,14 @@ int pc_transform_dims(PcDims &d, int V, int R, int C, size_t *smem_rows, size_t 
     d.fft_radix = fft_radix > 0 ? fft_radix : kPcDefaultFftRadix;
     if (d.fft_radix != 2 && d.fft_radix != 4 && d.fft_radix != 8 && d.fft_radix != 16)
         return fail("fft_radix must be 2, 4, 8 or 16 (got %d)", fft_radix);
-    // sequences per CTA: two radix-R butterflies per thread (n / R per
-    // sequence, 256 threads), at most 4,096 points in the two padded buffers
-    auto seqs = [&](int n) { return std::max(1, std::min(n, std::min(4096 / n, 512 * d.fft_radix / n))); };
-    d.rows_per_cta = seqs(C);
-    d.cols_per_cta = seqs(R);
-    *smem_rows = (size_t)(d.nmax / 2 + 2 * d.rows_per_cta * fft_seq_stride(C)) * sizeof(float2);
-    *smem_cols = (size_t)(d.nmax / 2 + 2 * d.cols_per_cta * fft_seq_stride(R)) * sizeof(float2);
+    // sequences per CTA: up to 4,096 points in each of the two padded buffers,
+    // no more sequences than there are (rows: R sequences of length C;
+    // columns: C sequences of length R)
+    d.rows_per_cta = std::max(1, std::min(R, 4096 / C));
+    d.cols_per_cta = std::max(1, std::min(C, 4096 / R));
+    // the full twiddle circle (nmax) and the two buffers
+    *smem_rows = (size_t)(d.nmax + 2 * d.rows_per_cta * fft_seq_stride(C)) * sizeof(float2);
+    *smem_cols = (size_t)(d.nmax + 2 * d.cols_per_cta * fft_seq_stride(R)) * sizeof(float2);
     cudaError_t e = cudaFuncSetAttribute(pc_rows_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem_rows);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(pc_rows_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem_rows);

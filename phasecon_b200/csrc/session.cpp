@@ -318,10 +318,7 @@ int Session::autotune()
 int Session::refresh_error()
 {
     // views outside every frame keep e = y (they never enter the problem)
-    const float *off = rings ? d_off : nullptr;
-    if (!launch_forward_project_views(hs.g, d_table, d_view_first, d_views, d_view_frame, n_assigned, d_x, d_y, d_err,
-                                      st, off))
-        launch_forward_project(hs.g, d_table, d_view_first, d_x, d_y, d_acc, d_err, st, off);
+    launch_forward_project(hs.g, d_table, d_view_first, d_x, d_y, d_acc, d_err, st, rings ? d_off : nullptr);
     CK(cudaGetLastError());
     return 0;
 }
@@ -602,9 +599,7 @@ int Session::forward_project(const float *obj, float *sino)
     cudaError_t e = cudaMemcpyAsync(d_tmp, obj, n_vox * sizeof(float), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) {
         launch_vol_to_zfast(d_tmp, d_obj, g.N_time, g.N_z, g.N_y, g.N_x, st);
-        if (!launch_forward_project_views(g, d_table, d_view_first, d_views, d_view_frame, n_assigned, d_obj,
-                                          nullptr, d_out, st))
-            launch_forward_project(g, d_table, d_view_first, d_obj, nullptr, d_acc, d_out, st);
+        launch_forward_project(g, d_table, d_view_first, d_obj, nullptr, d_acc, d_out, st);
     }
     if (e == cudaSuccess) e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaMemcpyAsync(sino, d_out, n_sino * sizeof(float), cudaMemcpyDeviceToHost, st);
