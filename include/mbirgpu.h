@@ -402,6 +402,10 @@ typedef struct {
     int32_t fft_radix;         /* largest radix of the FFT stages: 2, 4, 8 or 16; 0 = the
                                   library's choice. Every stage keeps its points in registers
                                   between two passes through shared memory */
+    int32_t nms_lanes;         /* lanes that share one pixel's Nelder-Mead search: 1, 2, 4
+                                  or 8; 0 = the library's choice */
+    int32_t nms_ctas_per_view; /* raster order: CTAs (one thread-block cluster) per view,
+                                  1, 2 or 4; 0 = the library's choice */
 } mbirgpu_pc_options;
 
 typedef struct {

@@ -185,39 +185,140 @@ __device__ __forceinline__ float2 expz_fast(float zr, float zi)
 
 }  // namespace
 
+// Global <-> shared staging of the passes: each thread takes kStage elements
+// a blockDim.x apart per round and issues all their global loads before any
+// of its shared-memory stores, so that a round keeps kStage loads in flight
+// per thread instead of one.
+constexpr int kStage = 8;
+
+namespace {
+// prologue input of element i (pixel p of the view)
+__device__ __forceinline__ float2 prologue_in(const PcArgs &A, int prologue, size_t i, size_t p)
+{
+    switch (prologue) {
+    case PC_IN_DW: return cscale(__ldg(A.in + i), __ldg(A.D + p));
+    case PC_IN_DEZ: return cscale(expz(__ldg(A.zr + i), __ldg(A.zi + i)), __ldg(A.D + p));
+    case PC_IN_PAG: {
+        const float m = __ldg(A.y + i), dp = __ldg(A.D + p);
+        return make_float2(m * m / (dp * dp), 0.f);
+    }
+    default: return __ldg(A.in + i);
+    }
+}
+
+// the operands an epilogue reads besides the transform's value t
+struct EpiIn {
+    float2 a, b;
+    float s0, s1;
+};
+
+__device__ __forceinline__ EpiIn epilogue_in(const PcArgs &A, int epilogue, size_t i, size_t p)
+{
+    EpiIn r = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), 1.f, 0.f};
+    switch (epilogue) {
+    case PC_OUT_GRES:
+        r.a = A.omega[i];
+        r.s0 = A.lam ? __ldg(A.lam + i) : 1.0f;
+        r.s1 = __ldg(A.y + i);
+        break;
+    case PC_OUT_GRAD:
+        r.a = A.w[i];
+        r.b = A.buf[i];
+        r.s0 = __ldg(A.D + p);
+        break;
+    case PC_OUT_SFWD:
+        r.a = A.omega[i];
+        r.s0 = A.lam ? __ldg(A.lam + i) : 1.0f;
+        break;
+    case PC_OUT_SDEN:
+        r.a = A.g[i];
+        r.s0 = __ldg(A.D + p);
+        break;
+    case PC_OUT_OMEGA: r.s1 = __ldg(A.y + i); break;
+    case PC_OUT_PCOST:
+        r.s0 = A.lam ? __ldg(A.lam + i) : 1.0f;
+        r.s1 = __ldg(A.y + i);
+        break;
+    default: break;
+    }
+    return r;
+}
+
+// writes element i's epilogue result; returns its term of the per-view sum
+__device__ __forceinline__ double epilogue_out(const PcDims &d, const PcArgs &A, int epilogue, size_t i, float2 t,
+                                               const EpiIn &in)
+{
+    switch (epilogue) {
+    case PC_OUT_GRES: {  // conj(Omega) Lambda (Omega t - y)
+        const float2 r = csub(cmul(in.a, t), make_float2(in.s1, 0.f));
+        A.out[i] = cmul(cconj(in.a), cscale(r, in.s0));
+        return 0.0;
+    }
+    case PC_OUT_GRAD: {  // g = D t + nu (w - buf); sum |g|^2
+        const float2 g = cadd(cscale(t, in.s0), cscale(csub(in.a, in.b), d.nu));
+        A.g[i] = g;
+        return (double)cabs2(g);
+    }
+    case PC_OUT_SFWD:  // conj(Omega) Lambda Omega t
+        A.out[i] = cmul(cconj(in.a), cscale(cmul(in.a, t), in.s0));
+        return 0.0;
+    case PC_OUT_SDEN: {  // sum Re(conj(g) D t)
+        const float2 dt = cscale(t, in.s0);
+        return (double)in.a.x * (double)dt.x + (double)in.a.y * (double)dt.y;
+    }
+    case PC_OUT_OMEGA: {  // Omega = (y / t) / |y / t|
+        const float den = cabs2(t) + FLT_MIN;
+        const float2 q = make_float2(in.s1 * t.x / den, -in.s1 * t.y / den);
+        const float m = sqrtf(cabs2(q)) + FLT_MIN;
+        A.omega[i] = make_float2(q.x / m, q.y / m);
+        return 0.0;
+    }
+    case PC_OUT_PCOST: {  // sum Lambda (y - |t|)^2 / 2
+        const double rr = (double)in.s1 - sqrt((double)cabs2(t));
+        return rr * rr * in.s0 / 2.0;
+    }
+    case PC_OUT_PAG: {  // Paganin: thickness -log|Re t|
+        const float th = -logf(fabsf(t.x));
+        A.zr[i] = th / 2.0f;
+        A.zi[i] = th * d.delta_over_beta / 2.0f;
+        return 0.0;
+    }
+    default: A.out[i] = t; return 0.0;
+    }
+}
+
+__device__ __forceinline__ int ilog2_pow2(int n) { return 31 - __clz(n); }
+}  // namespace
+
 // ---------------------------------------------------------------------------- pass 1
 __global__ void pc_rows_forward(PcDims d, PcArgs A, int prologue)
 {
     extern __shared__ float2 smem[];
     const int v = blockIdx.y;
     if (A.active && !A.active[v]) return;
-    const int C = d.C, rpc = d.rows_per_cta, S = fft_seq_stride(C);
+    const int C = d.C, lc = d.logC, rpc = d.rows_per_cta, S = fft_seq_stride(C);
     float2 *s_tw = smem, *a = smem + d.nmax, *b = a + rpc * S;
     load_twiddles(s_tw, A.tw, d.nmax);
     const int r0 = blockIdx.x * rpc;
-    const size_t vb = (size_t)v * d.N;
-    for (int e = threadIdx.x; e < rpc * C; e += blockDim.x) {
-        const int r = r0 + e / C, c = e % C;
-        float2 x = make_float2(0.f, 0.f);
-        if (r < d.R) {
-            const size_t i = vb + (size_t)r * C + c, p = (size_t)r * C + c;
-            switch (prologue) {
-            case PC_IN_PLAIN: x = A.in[i]; break;
-            case PC_IN_DW: x = cscale(A.in[i], A.D[p]); break;
-            case PC_IN_DEZ: x = cscale(expz(A.zr[i], A.zi[i]), A.D[p]); break;
-            case PC_IN_PAG: {
-                const float m = A.y[i];
-                x = make_float2(m * m / (A.D[p] * A.D[p]), 0.f);
-            } break;
-            }
+    const int nrows = min(rpc, d.R - r0);
+    const int total = nrows * C;
+    const size_t vb = (size_t)v * d.N, pb = (size_t)r0 * C;
+    for (int e0 = threadIdx.x; e0 < total; e0 += kStage * blockDim.x) {
+        float2 x[kStage];
+#pragma unroll
+        for (int u = 0; u < kStage; u++) {
+            const int e = e0 + u * blockDim.x;
+            if (e < total) x[u] = prologue_in(A, prologue, vb + pb + e, pb + e);
         }
-        a[fpos(e / C, e % C, S)] = x;
+#pragma unroll
+        for (int u = 0; u < kStage; u++) {
+            const int e = e0 + u * blockDim.x;
+            if (e < total) a[fpos(e >> lc, e & (C - 1), S)] = x[u];
+        }
     }
     __syncthreads();
-    const int nrows = min(rpc, d.R - r0);
-    float2 *res = fft_smem(a, b, C, d.logC, nrows, S, s_tw, d.nmax, false, d.fft_radix);
-    for (int e = threadIdx.x; e < nrows * C; e += blockDim.x)
-        A.work[vb + (size_t)r0 * C + e] = res[fpos(e / C, e % C, S)];
+    float2 *res = fft_smem(a, b, C, lc, nrows, S, s_tw, d.nmax, false, d.fft_radix);
+    for (int e = threadIdx.x; e < total; e += blockDim.x) A.work[vb + pb + e] = res[fpos(e >> lc, e & (C - 1), S)];
 }
 
 // ---------------------------------------------------------------------------- pass 2
@@ -226,29 +327,48 @@ __global__ void pc_cols_filter(PcDims d, PcArgs A, const float2 *__restrict__ tr
     extern __shared__ float2 smem[];
     const int v = blockIdx.y;
     if (A.active && !A.active[v]) return;
-    const int R = d.R, C = d.C, cb = d.cols_per_cta, S = fft_seq_stride(R);
+    const int R = d.R, C = d.C, cb = d.cols_per_cta, lcb = ilog2_pow2(cb), S = fft_seq_stride(R);
     float2 *s_tw = smem, *a = smem + d.nmax, *b = a + cb * S;
     load_twiddles(s_tw, A.tw, d.nmax);
     const int c0 = blockIdx.x * cb;
+    const int total = cb * R;
     const size_t vb = (size_t)v * d.N;
-    for (int e = threadIdx.x; e < cb * R; e += blockDim.x) {
-        const int r = e / cb, q = e % cb;
-        a[fpos(q, r, S)] = A.work[vb + (size_t)r * C + c0 + q];
+    for (int e0 = threadIdx.x; e0 < total; e0 += kStage * blockDim.x) {
+        float2 x[kStage];
+#pragma unroll
+        for (int u = 0; u < kStage; u++) {
+            const int e = e0 + u * blockDim.x;
+            if (e < total) x[u] = A.work[vb + (size_t)(e >> lcb) * C + c0 + (e & (cb - 1))];
+        }
+#pragma unroll
+        for (int u = 0; u < kStage; u++) {
+            const int e = e0 + u * blockDim.x;
+            if (e < total) a[fpos(e & (cb - 1), e >> lcb, S)] = x[u];
+        }
     }
     __syncthreads();
     float2 *res = fft_smem(a, b, R, d.logR, cb, S, s_tw, d.nmax, false, d.fft_radix);
     float2 *other = res == a ? b : a;
-    for (int e = threadIdx.x; e < cb * R; e += blockDim.x) {
-        const int r = e / cb, q = e % cb;
-        const int i = fpos(q, r, S);
-        res[i] = cmul(res[i], transfer[(size_t)r * C + c0 + q]);
+    for (int e0 = threadIdx.x; e0 < total; e0 += kStage * blockDim.x) {
+        float2 h[kStage];
+#pragma unroll
+        for (int u = 0; u < kStage; u++) {
+            const int e = e0 + u * blockDim.x;
+            if (e < total) h[u] = __ldg(transfer + (size_t)(e >> lcb) * C + c0 + (e & (cb - 1)));
+        }
+#pragma unroll
+        for (int u = 0; u < kStage; u++) {
+            const int e = e0 + u * blockDim.x;
+            if (e < total) {
+                const int i = fpos(e & (cb - 1), e >> lcb, S);
+                res[i] = cmul(res[i], h[u]);
+            }
+        }
     }
     __syncthreads();
     res = fft_smem(res, other, R, d.logR, cb, S, s_tw, d.nmax, true, d.fft_radix);
-    for (int e = threadIdx.x; e < cb * R; e += blockDim.x) {
-        const int r = e / cb, q = e % cb;
-        A.work[vb + (size_t)r * C + c0 + q] = res[fpos(q, r, S)];
-    }
+    for (int e = threadIdx.x; e < total; e += blockDim.x)
+        A.work[vb + (size_t)(e >> lcb) * C + c0 + (e & (cb - 1))] = res[fpos(e & (cb - 1), e >> lcb, S)];
 }
 
 // ---------------------------------------------------------------------------- pass 3
@@ -258,61 +378,44 @@ __global__ void pc_rows_inverse(PcDims d, PcArgs A, int epilogue)
     __shared__ double s_red[32];
     const int v = blockIdx.y;
     if (A.active && !A.active[v]) return;
-    const int C = d.C, rpc = d.rows_per_cta, S = fft_seq_stride(C);
+    const int C = d.C, lc = d.logC, rpc = d.rows_per_cta, S = fft_seq_stride(C);
     float2 *s_tw = smem, *a = smem + d.nmax, *b = a + rpc * S;
     load_twiddles(s_tw, A.tw, d.nmax);
     const int r0 = blockIdx.x * rpc;
     const int nrows = min(rpc, d.R - r0);
-    const size_t vb = (size_t)v * d.N;
-    for (int e = threadIdx.x; e < nrows * C; e += blockDim.x) a[fpos(e / C, e % C, S)] = A.work[vb + (size_t)r0 * C + e];
+    const int total = nrows * C;
+    const size_t vb = (size_t)v * d.N, pb = (size_t)r0 * C;
+    for (int e0 = threadIdx.x; e0 < total; e0 += kStage * blockDim.x) {
+        float2 x[kStage];
+#pragma unroll
+        for (int u = 0; u < kStage; u++) {
+            const int e = e0 + u * blockDim.x;
+            if (e < total) x[u] = A.work[vb + pb + e];
+        }
+#pragma unroll
+        for (int u = 0; u < kStage; u++) {
+            const int e = e0 + u * blockDim.x;
+            if (e < total) a[fpos(e >> lc, e & (C - 1), S)] = x[u];
+        }
+    }
     __syncthreads();
-    float2 *res = fft_smem(a, b, C, d.logC, nrows, S, s_tw, d.nmax, true, d.fft_radix);
+    float2 *res = fft_smem(a, b, C, lc, nrows, S, s_tw, d.nmax, true, d.fft_radix);
     const float inv_n = 1.0f / (float)d.N;
     double acc = 0.0;
-    for (int e = threadIdx.x; e < nrows * C; e += blockDim.x) {
-        const size_t i = vb + (size_t)r0 * C + e, p = (size_t)r0 * C + e;
-        const float2 t = cscale(res[fpos(e / C, e % C, S)], inv_n);
-        switch (epilogue) {
-        case PC_OUT_PLAIN: A.out[i] = t; break;
-        case PC_OUT_GRES: {  // conj(Omega) Lambda (Omega t - y)
-            const float2 om = A.omega[i];
-            const float lam = A.lam ? A.lam[i] : 1.0f;
-            const float2 r = csub(cmul(om, t), make_float2(A.y[i], 0.f));
-            A.out[i] = cmul(cconj(om), cscale(r, lam));
-        } break;
-        case PC_OUT_GRAD: {  // g = D t + nu (w - buf); sum |g|^2
-            const float2 gw = csub(A.w[i], A.buf[i]);
-            const float2 g = cadd(cscale(t, A.D[p]), cscale(gw, d.nu));
-            A.g[i] = g;
-            acc += (double)cabs2(g);
-        } break;
-        case PC_OUT_SFWD: {  // conj(Omega) Lambda Omega t
-            const float2 om = A.omega[i];
-            const float lam = A.lam ? A.lam[i] : 1.0f;
-            A.out[i] = cmul(cconj(om), cscale(cmul(om, t), lam));
-        } break;
-        case PC_OUT_SDEN: {  // sum Re(conj(g) D t)
-            const float2 g = A.g[i];
-            const float2 dt = cscale(t, A.D[p]);
-            acc += (double)g.x * (double)dt.x + (double)g.y * (double)dt.y;
-        } break;
-        case PC_OUT_OMEGA: {  // Omega = (y / t) / |y / t|
-            const float yy = A.y[i];
-            const float den = cabs2(t) + FLT_MIN;
-            const float2 q = make_float2(yy * t.x / den, -yy * t.y / den);
-            const float m = sqrtf(cabs2(q)) + FLT_MIN;
-            A.omega[i] = make_float2(q.x / m, q.y / m);
-        } break;
-        case PC_OUT_PCOST: {  // sum Lambda (y - |t|)^2 / 2
-            const float lam = A.lam ? A.lam[i] : 1.0f;
-            const double rr = (double)A.y[i] - sqrt((double)cabs2(t));
-            acc += rr * rr * lam / 2.0;
-        } break;
-        case PC_OUT_PAG: {  // Paganin: thickness -log|Re t|
-            const float th = -logf(fabsf(t.x));
-            A.zr[i] = th / 2.0f;
-            A.zi[i] = th * d.delta_over_beta / 2.0f;
-        } break;
+    constexpr int kEpi = kStage / 2;  // the epilogues read up to two complex operands per element
+    for (int e0 = threadIdx.x; e0 < total; e0 += kEpi * blockDim.x) {
+        EpiIn in[kEpi];
+#pragma unroll
+        for (int u = 0; u < kEpi; u++) {
+            const int e = e0 + u * blockDim.x;
+            if (e < total) in[u] = epilogue_in(A, epilogue, vb + pb + e, pb + e);
+        }
+#pragma unroll
+        for (int u = 0; u < kEpi; u++) {
+            const int e = e0 + u * blockDim.x;
+            if (e < total)
+                acc += epilogue_out(d, A, epilogue, vb + pb + e, cscale(res[fpos(e >> lc, e & (C - 1), S)], inv_n),
+                                    in[u]);
         }
     }
     if (epilogue == PC_OUT_GRAD || epilogue == PC_OUT_SDEN || epilogue == PC_OUT_PCOST)
@@ -450,12 +553,21 @@ __global__ void pc_pret_finish(PcDims d, PcArgs A, int iter, float pret_thresh, 
 // Nelder_Mead_Simplex_2DSearch, PCMBIR_3D/XT_Search.c:8-215), b = w - v. The
 // reference sweeps pixels in raster order (XT_CmplxProjEst.c:117-160);
 // pc_nms_wavefront keeps that order exactly, pc_nms updates colour classes.
+//
+// One pixel's search runs on a group of G adjacent lanes (G = 1, 2, 4 or 8).
+// The eight neighbour slots s = 0..7 (3x3 position s < 4 ? s : s + 1) are dealt
+// round-robin over the group's lanes; lane 0 adds the data term; a butterfly of
+// xor shuffles sums the partial costs, which leaves the same sum (the same
+// pairwise additions) in every lane, so the group takes every branch together.
 namespace {
-struct NmsCtx {
-    float br, bi, nu;
-    float nr[9], ni[9];
-    unsigned flags;
-    const PcPrior *P;
+template <int G>
+struct NmsLane {
+    static constexpr int kN = 8 / G;  // neighbour slots per lane
+    float br, bi, half_nu;
+    float nr[kN], ni[kN], fw[kN];
+    unsigned flags;  // bit m: slot g + G m lies inside the image
+    unsigned mask;   // the group's lanes within the warp
+    bool data;       // this lane adds the data term
 };
 
 // a^e for a > 0 with the hardware base-2 logarithm and exponential (the
@@ -469,56 +581,73 @@ __device__ __forceinline__ float pow_fast(float a, float e)
     return r;
 }
 
-__device__ float nms_cost(const NmsCtx &c, float zr, float zi)
+template <int G>
+__device__ __forceinline__ float nms_cost(const NmsLane<G> &c, const PcPrior &P, float zr, float zi)
 {
-    const float2 ez = expz_fast(zr, zi);
-    float cost = ((ez.x - c.br) * (ez.x - c.br) + (ez.y - c.bi) * (ez.y - c.bi)) * c.nu / 2;
-    const PcPrior &P = *c.P;
+    float cost = 0.f;
+    if (c.data) {
+        const float2 ez = expz_fast(zr, zi);
+        cost = ((ez.x - c.br) * (ez.x - c.br) + (ez.y - c.bi) * (ez.y - c.bi)) * c.half_nu;
+    }
 #pragma unroll
-    for (int a = 0; a < 9; a++) {
-        if (c.flags & (1u << a)) {
-            const float db = zr - c.nr[a], dd = zi - c.ni[a];
+    for (int m = 0; m < NmsLane<G>::kN; m++) {
+        if (c.flags & (1u << m)) {
+            const float db = zr - c.nr[m], dd = zi - c.ni[m];
             const float dph = P.T00_f * dd + P.T01_f * db, dmg = P.T10_f * dd + P.T11_f * db;
             const float aph = fabsf(dph), amg = fabsf(dmg);
-            const float fw = P.f_f[a];
-            if (aph > 0.f)
-                cost += fw * __fdividef(aph * aph * P.ph_isq_f, P.ph_c_f + pow_fast(aph, P.qmp_f) * P.ph_isqp_f);
-            if (amg > 0.f)
-                cost += fw * __fdividef(amg * amg * P.mg_isq_f, P.mg_c_f + pow_fast(amg, P.qmp_f) * P.mg_isqp_f);
+            // rho(x) = x^2 / sig^2 / (c + |x|^(q-p) / sig^(q-p)) for both channels,
+            // the two quotients over one reciprocal: x1/y1 + x2/y2 = (x1 y2 + x2 y1) / (y1 y2)
+            const float pph = aph > 0.f ? pow_fast(aph, P.qmp_f) : 0.f;
+            const float pmg = amg > 0.f ? pow_fast(amg, P.qmp_f) : 0.f;
+            const float x1 = aph * aph * P.ph_isq_f, y1 = P.ph_c_f + pph * P.ph_isqp_f;
+            const float x2 = amg * amg * P.mg_isq_f, y2 = P.mg_c_f + pmg * P.mg_isqp_f;
+            cost += c.fw[m] * __fdividef(x1 * y2 + x2 * y1, y1 * y2);
         }
     }
+#pragma unroll
+    for (int o = 1; o < G; o <<= 1) cost += __shfl_xor_sync(c.mask, cost, o);
     return cost;
 }
-}  // namespace
 
-namespace {
 // The search of Nelder_Mead_Simplex_2DSearch for pixel (j, k) of view v,
-// written back to z. Neighbours are read from z as it stands (Gauss-Seidel).
+// written back to z by the group's lane 0. Neighbours are read from z as it
+// stands (Gauss-Seidel). Each iteration evaluates the reflected point, then
+// at most one second point (expansion, outside or inside contraction; which
+// one follows the reference's case analysis), then the shrink's two points:
+// the cost is called from one place per kind, so lanes of a warp that take
+// different cases share the calls instead of running them one case at a time.
+template <int G>
 __device__ void nms_pixel(const PcDims &d, const PcArgs &A, const PcPrior &P, int v, int j, int k, int max_iter,
-                          float threshold)
+                          float threshold, int g, unsigned mask)
 {
     const int R = d.R, C = d.C;
     const size_t i = (size_t)v * d.N + (size_t)j * C + k;
-    NmsCtx c;
-    c.P = &P;
-    c.nu = d.nu;
+    NmsLane<G> c;
     const float2 b = csub(A.w[i], A.vdual[i]);
     c.br = b.x;
     c.bi = b.y;
+    c.half_nu = d.nu / 2;
+    c.mask = mask;
+    c.data = g == 0;
     c.flags = 0;
-    for (int a = 0; a < 9; a++) {
+#pragma unroll
+    for (int m = 0; m < NmsLane<G>::kN; m++) {
+        const int s = g + G * m, a = s < 4 ? s : s + 1;
         const int jj = j + a / 3 - 1, kk = k + a % 3 - 1;
-        c.nr[a] = c.ni[a] = 0.f;
+        c.nr[m] = c.ni[m] = 0.f;
+        c.fw[m] = P.f_f[a];
         if (jj >= 0 && jj < R && kk >= 0 && kk < C) {
             const size_t n = (size_t)v * d.N + (size_t)jj * C + kk;
-            c.nr[a] = A.zr[n];
-            c.ni[a] = A.zi[n];
-            if (a != 4) c.flags |= 1u << a;  // the centre's weight is zero
+            c.nr[m] = __ldcg(A.zr + n);
+            c.ni[m] = __ldcg(A.zi + n);
+            c.flags |= 1u << m;
         }
     }
-    const float z0r = c.nr[4], z0i = c.ni[4];
+    const float z0r = __ldcg(A.zr + i), z0i = __ldcg(A.zi + i);
     float pr[3] = {z0r, 2 * z0r, z0r}, pi[3] = {z0i, z0i, 2 * z0i};
-    float cc[3] = {nms_cost(c, pr[0], pi[0]), nms_cost(c, pr[1], pi[1]), nms_cost(c, pr[2], pi[2])};
+    float cc[3];
+#pragma unroll
+    for (int q = 0; q < 3; q++) cc[q] = nms_cost<G>(c, P, pr[q], pi[q]);
     auto swap_pts = [&](int a2, int b2) {
         float t = pr[a2]; pr[a2] = pr[b2]; pr[b2] = t;
         t = pi[a2]; pi[a2] = pi[b2]; pi[b2] = t;
@@ -529,60 +658,86 @@ __device__ void nms_pixel(const PcDims &d, const PcArgs &A, const PcPrior &P, in
         if (cc[1] < cc[0]) swap_pts(0, 1);
         if (cc[2] < cc[1]) swap_pts(1, 2);
     };
-    auto accept = [&](float ar, float ai, float ac) {
-        pr[2] = ar; pi[2] = ai; cc[2] = ac;
-        if (cc[2] < cc[1]) swap_pts(1, 2);
-        if (cc[1] < cc[0]) swap_pts(0, 1);
-    };
-    auto shrink = [&]() {
-        for (int q = 1; q < 3; q++) {
-            pr[q] = pr[0] + 0.5f * (pr[q] - pr[0]);
-            pi[q] = pi[0] + 0.5f * (pi[q] - pi[0]);
-            cc[q] = nms_cost(c, pr[q], pi[q]);
-        }
-        sort3();
-    };
     sort3();
     float cr0 = (pr[0] + pr[1]) / 2.0f, ci0 = (pi[0] + pi[1]) / 2.0f;
     for (int it = 0; it < max_iter; it++) {
         const float o_r[4] = {cr0, pr[0], pr[1], pr[2]}, o_i[4] = {ci0, pi[0], pi[1], pi[2]};
         const float rr = cr0 + (cr0 - pr[2]), ri = ci0 + (ci0 - pi[2]);
-        const float crf = nms_cost(c, rr, ri);
-        if (crf < cc[1] && crf >= cc[0]) {
-            accept(rr, ri, crf);
-        } else if (crf < cc[0]) {
-            const float er = cr0 + 2.0f * (rr - cr0), ei = ci0 + 2.0f * (ri - ci0);
-            const float ce = nms_cost(c, er, ei);
-            if (ce < crf) accept(er, ei, ce);
-            else accept(rr, ri, crf);
-        } else if (crf >= cc[1] && crf < cc[2]) {
-            const float orr = cr0 + 0.5f * (rr - cr0), oi = ci0 + 0.5f * (ri - ci0);
-            const float co = nms_cost(c, orr, oi);
-            if (co <= crf) accept(orr, oi, co);
-            else shrink();
-        } else if (crf >= cc[2]) {
-            const float ir = cr0 - 0.5f * (cr0 - pr[2]), ii = ci0 - 0.5f * (ci0 - pi[2]);
-            const float ci = nms_cost(c, ir, ii);
-            if (ci < cc[2]) accept(ir, ii, ci);
-            else shrink();
+        const float crf = nms_cost<G>(c, P, rr, ri);
+        // 0: accept the reflection; 1: expansion; 2: outside contraction;
+        // 3: inside contraction; -1: no case holds (a NaN cost), nothing moves
+        const int kind = (crf < cc[1] && crf >= cc[0]) ? 0
+                         : crf < cc[0]                 ? 1
+                         : (crf >= cc[1] && crf < cc[2]) ? 2
+                         : crf >= cc[2]                ? 3
+                                                       : -1;
+        float sr = rr, si = ri;
+        if (kind == 1) { sr = cr0 + 2.0f * (rr - cr0); si = ci0 + 2.0f * (ri - ci0); }
+        if (kind == 2) { sr = cr0 + 0.5f * (rr - cr0); si = ci0 + 0.5f * (ri - ci0); }
+        if (kind == 3) { sr = cr0 - 0.5f * (cr0 - pr[2]); si = ci0 - 0.5f * (ci0 - pi[2]); }
+        float cs = crf;
+        if (kind > 0) cs = nms_cost<G>(c, P, sr, si);
+        bool take_s = kind == 1 ? cs < crf : kind == 2 ? cs <= crf : kind == 3 ? cs < cc[2] : false;
+        const bool take_r = kind == 0 || (kind == 1 && !take_s);
+        const bool shrink = (kind == 2 || kind == 3) && !take_s;
+        if (take_r || take_s) {
+            pr[2] = take_s ? sr : rr;
+            pi[2] = take_s ? si : ri;
+            cc[2] = take_s ? cs : crf;
+            if (cc[2] < cc[1]) swap_pts(1, 2);
+            if (cc[1] < cc[0]) swap_pts(0, 1);
+        }
+        if (shrink) {
+#pragma unroll
+            for (int q = 1; q < 3; q++) {
+                pr[q] = pr[0] + 0.5f * (pr[q] - pr[0]);
+                pi[q] = pi[0] + 0.5f * (pi[q] - pi[0]);
+                cc[q] = nms_cost<G>(c, P, pr[q], pi[q]);
+            }
+            sort3();
         }
         cr0 = (pr[0] + pr[1]) / 2.0f;
         ci0 = (pi[0] + pi[1]) / 2.0f;
         const float n_r[4] = {cr0, pr[0], pr[1], pr[2]}, n_i[4] = {ci0, pi[0], pi[1], pi[2]};
         float num = 0.f, den = 0.f;
+#pragma unroll
         for (int q = 0; q < 4; q++) {
             num += fabsf(o_r[q] - n_r[q]) + fabsf(o_i[q] - n_i[q]);
             den += fabsf(o_r[q]) + fabsf(o_i[q]);
         }
         if (num / den * 100.0f < threshold && it > 1) break;
     }
-    A.zr[i] = pr[0];
-    A.zi[i] = pi[0];
+    if (g == 0) {
+        A.zr[i] = pr[0];
+        A.zi[i] = pi[0];
+    }
+}
+
+// lanes of the G-lane group that thread t belongs to
+template <int G>
+__device__ __forceinline__ unsigned group_mask(int t)
+{
+    return G == 32 ? 0xffffffffu : (((1u << G) - 1u) << ((t & 31) & ~(G - 1)));
+}
+
+__device__ __forceinline__ unsigned cluster_rank()
+{
+    unsigned r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+
+// every thread of the cluster, with release/acquire at cluster scope so that
+// the z written before it is seen by the cluster's CTAs after it
+__device__ __forceinline__ void cluster_sync_all()
+{
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
 }
 }  // namespace
 
 // Colour-class sweep: pixels of one (row parity, column parity) class
 // together -- no two 8-neighbours share a class -- over four launches.
+template <int G>
 __global__ void pc_nms(PcDims d, PcArgs A, const __grid_constant__ PcPrior P, int color, int max_iter,
                        float threshold)
 {
@@ -590,29 +745,80 @@ __global__ void pc_nms(PcDims d, PcArgs A, const __grid_constant__ PcPrior P, in
     if (A.active && !A.active[v]) return;
     const int cj = color >> 1, ck = color & 1;
     const int hr = (d.R - cj + 1) / 2, hc = (d.C - ck + 1) / 2;
-    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < hr * hc; e += gridDim.x * blockDim.x)
-        nms_pixel(d, A, P, v, 2 * (e / hc) + cj, 2 * (e % hc) + ck, max_iter, threshold);
+    const int g = threadIdx.x % G, groups = gridDim.x * blockDim.x / G;
+    const unsigned mask = group_mask<G>(threadIdx.x);
+    for (int e = (blockIdx.x * blockDim.x + threadIdx.x) / G; e < hr * hc; e += groups)
+        nms_pixel<G>(d, A, P, v, 2 * (e / hc) + cj, 2 * (e % hc) + ck, max_iter, threshold, g, mask);
 }
 
 // The reference's raster order, exactly: pixel (j, k) reads the updated
 // (j-1, k-1..k+1) and (j, k-1) and the not yet updated (j, k+1) and row j+1,
 // so every pixel of the anti-diagonal 2j + k = t depends only on pixels of
-// smaller t and none of larger t reads it first. One CTA per view walks the
-// 2(R-1) + C wavefronts with a block barrier between them (global-memory
-// writes of the block are visible to it after the barrier).
+// smaller t and none of larger t reads it first. The CTAs of one cluster share
+// a view (the cluster size is the number of CTAs per view) and walk its
+// 2(R-1) + C wavefronts, the pixels of each dealt over all their lane groups,
+// with a barrier between wavefronts: the block barrier for one CTA per view,
+// the cluster barrier (release/acquire at cluster scope) for more.
+template <int G>
 __global__ void pc_nms_wavefront(PcDims d, PcArgs A, const __grid_constant__ PcPrior P, int max_iter,
-                                 float threshold)
+                                 float threshold, int ctas_per_view)
 {
-    const int v = blockIdx.x;
+    const int v = blockIdx.x / ctas_per_view;
+    const int part = ctas_per_view > 1 ? (int)cluster_rank() : 0;
+    // a view's CTAs all return here or none does
     if (A.active && !A.active[v]) return;
     const int R = d.R, C = d.C;
     const int T = 2 * (R - 1) + C;
+    const int g = threadIdx.x % G, groups = blockDim.x / G;
+    // groups interleaved over the cluster's CTAs, so that short anti-diagonals
+    // still spread over all of them
+    const int grp = ((int)threadIdx.x / G) * ctas_per_view + part, all_groups = groups * ctas_per_view;
+    const unsigned mask = group_mask<G>(threadIdx.x);
     for (int t = 0; t < T; t++) {
         const int j_lo = t >= C ? (t - C + 2) / 2 : 0;  // smallest j with t - 2j <= C - 1
         const int j_hi = min(R - 1, t / 2);
-        for (int j = j_lo + (int)threadIdx.x; j <= j_hi; j += blockDim.x)
-            nms_pixel(d, A, P, v, j, t - 2 * j, max_iter, threshold);
-        __syncthreads();
+        for (int j = j_lo + grp; j <= j_hi; j += all_groups)
+            nms_pixel<G>(d, A, P, v, j, t - 2 * j, max_iter, threshold, g, mask);
+        if (ctas_per_view > 1) cluster_sync_all();
+        else __syncthreads();
+    }
+}
+
+namespace {
+template <int G>
+int nms_sweep(const PcDims &d, const PcArgs &A, const PcPrior &P, int order, int ctas, int max_iter, float thr,
+              dim3 pointwise, cudaStream_t st)
+{
+    if (order == 0) {
+        // 128 lane groups per view: the most pixels an anti-diagonal of a
+        // 256-wide view holds, dealt over the view's CTAs
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(d.V * ctas);
+        cfg.blockDim = dim3(max(32, 128 * G / ctas));
+        cfg.stream = st;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = ctas;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        cudaLaunchKernelEx(&cfg, pc_nms_wavefront<G>, d, A, P, max_iter, thr, ctas);
+        return 1;
+    }
+    for (int color = 0; color < 4; color++) pc_nms<G><<<pointwise, 256, 0, st>>>(d, A, P, color, max_iter, thr);
+    return 4;
+}
+}  // namespace
+
+int launch_nms_sweep(const PcDims &d, const PcArgs &A, const PcPrior &P, int order, int lanes, int ctas,
+                     int max_iter, float threshold, dim3 pointwise, cudaStream_t st)
+{
+    switch (lanes) {
+    case 1: return nms_sweep<1>(d, A, P, order, ctas, max_iter, threshold, pointwise, st);
+    case 2: return nms_sweep<2>(d, A, P, order, ctas, max_iter, threshold, pointwise, st);
+    case 4: return nms_sweep<4>(d, A, P, order, ctas, max_iter, threshold, pointwise, st);
+    default: return nms_sweep<8>(d, A, P, order, ctas, max_iter, threshold, pointwise, st);
     }
 }
 

@@ -75,17 +75,22 @@ __global__ void pc_pret_prepare(PcDims d, PcArgs A);
 __global__ void pc_pret_dual(PcDims d, PcArgs A);
 __global__ void pc_prior_cost(PcDims d, PcArgs A, const __grid_constant__ PcPrior P);
 __global__ void pc_pret_finish(PcDims d, PcArgs A, int iter, float pret_thresh, double *costs_out);
-__global__ void pc_nms(PcDims d, PcArgs A, const __grid_constant__ PcPrior P, int color, int max_iter,
-                       float threshold);
-__global__ void pc_nms_wavefront(PcDims d, PcArgs A, const __grid_constant__ PcPrior P, int max_iter,
-                                 float threshold);
+// One Nelder-Mead proximal sweep over the active views: order 0 the raster
+// order by anti-diagonal wavefronts (one launch, clusters of ctas CTAs per
+// view), 1 the four colour classes (four launches of the pointwise grid);
+// lanes (1, 2, 4, 8) share one pixel's search. Returns the kernels launched.
+int launch_nms_sweep(const PcDims &d, const PcArgs &A, const PcPrior &P, int order, int lanes, int ctas,
+                     int max_iter, float threshold, dim3 pointwise, cudaStream_t st);
+// lanes per pixel and CTAs per view of the proximal sweep when none are asked for
+constexpr int kPcDefaultNmsLanes = 4;
+constexpr int kPcDefaultNmsCtas = 4;
 
 // Launch geometry of the three-pass transform for V views of R x C (powers of
 // two): fills d's sizes and per-CTA tiles, the dynamic shared memory of the
 // row and column passes, and raises the kernels' shared-memory limits.
 int pc_transform_dims(PcDims &d, int V, int R, int C, size_t *smem_rows, size_t *smem_cols, int fft_radix = 0);
 // the FFT stage radix used when none is asked for
-constexpr int kPcDefaultFftRadix = 8;
+constexpr int kPcDefaultFftRadix = 16;
 // float2 slots one FFT sequence of length n takes in shared memory: n plus
 // one padding slot per 16, rounded up to an odd count
 __host__ __device__ inline int fft_seq_stride(int n) { return (n + n / 16) | 1; }

@@ -161,6 +161,7 @@ struct PcSession {
     }
 
     int64_t launches = 0;  // kernels this session has launched
+    int nms_lanes = kPcDefaultNmsLanes, nms_ctas = kPcDefaultNmsCtas;  // proximal sweep layout
 
     dim3 pointwise_grid() const { return dim3(std::max(1, std::min(64, d.N / 1024)), d.V); }
 
@@ -174,14 +175,8 @@ struct PcSession {
     // one proximal sweep over every pixel of the active views
     void nms_sweep(const PcArgs &A)
     {
-        if (opt.nms_order == 0) {
-            pc_nms_wavefront<<<d.V, 128, 0, st>>>(d, A, prior, opt.nms_max_iter, (float)opt.nms_threshold);
-            launches += 1;
-            return;
-        }
-        for (int color = 0; color < 4; color++)
-            pc_nms<<<pointwise_grid(), 256, 0, st>>>(d, A, prior, color, opt.nms_max_iter, (float)opt.nms_threshold);
-        launches += 4;
+        launches += launch_nms_sweep(d, A, prior, opt.nms_order, nms_lanes, nms_ctas, opt.nms_max_iter,
+                                     (float)opt.nms_threshold, pointwise_grid(), st);
     }
 };
 
@@ -195,6 +190,12 @@ int PcSession::init(const mbirgpu_pc_problem *pb, const mbirgpu_pc_options *o, v
         return fail("phase retrieval needs power-of-two detector sizes up to 1024 (got %d x %d)", C, R);
     if (V < 1) return fail("proj_num must be positive");
     if (opt.nms_order != 0 && opt.nms_order != 1) return fail("nms_order must be 0 (raster) or 1 (colour classes)");
+    nms_lanes = opt.nms_lanes > 0 ? opt.nms_lanes : kPcDefaultNmsLanes;
+    nms_ctas = opt.nms_ctas_per_view > 0 ? opt.nms_ctas_per_view : kPcDefaultNmsCtas;
+    if (nms_lanes != 1 && nms_lanes != 2 && nms_lanes != 4 && nms_lanes != 8)
+        return fail("nms_lanes must be 1, 2, 4 or 8 (got %d)", opt.nms_lanes);
+    if (nms_ctas != 1 && nms_ctas != 2 && nms_ctas != 4)
+        return fail("nms_ctas_per_view must be 1, 2 or 4 (got %d)", opt.nms_ctas_per_view);
     if (pc_transform_dims(d, V, R, C, &smem_rows, &smem_cols, opt.fft_radix)) return -1;
     d.nu = (float)opt.nu;
     dob = pb->pag_regparam;

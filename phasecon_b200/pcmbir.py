@@ -38,6 +38,7 @@ class PcOptions(C.Structure):
         ("pret_threshold", C.c_double), ("sd_threshold", C.c_double), ("nms_threshold", C.c_double),
         ("mu", C.c_double), ("nu", C.c_double), ("mrf_p", C.c_double), ("mrf_q", C.c_double),
         ("nms_order", C.c_int32), ("fft_radix", C.c_int32),
+        ("nms_lanes", C.c_int32), ("nms_ctas_per_view", C.c_int32),
     ]
 
 

