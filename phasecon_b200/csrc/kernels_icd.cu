@@ -167,17 +167,20 @@ __device__ __forceinline__ bool wait_parity_bounded(unsigned long long *bar, uin
 // count into an error) and raises the CTA's abort flag: the caller stops
 // updating and staging after the next barrier, and the kernel waits for the
 // late copy once more before it exits (abort_bar / abort_parity).
-__device__ __forceinline__ void wait_staged(unsigned long long *bar, uint32_t &phases, int b, unsigned &timeouts,
+// Returns whether this thread's wait saw the copy land.
+__device__ __forceinline__ bool wait_staged(unsigned long long *bar, uint32_t &phases, int b, unsigned &timeouts,
                                             int &abort, int &abort_bar, uint32_t &abort_parity)
 {
     const uint32_t parity = (phases >> b) & 1u;
-    if (!wait_parity_bounded(bar, parity)) {
+    const bool ok = wait_parity_bounded(bar, parity);
+    if (!ok) {
         timeouts++;
         abort = 1;  // every writer stores the same values
         abort_bar = b;
         abort_parity = parity;
     }
     phases ^= 1u << b;
+    return ok;
 }
 
 template <int KW>
@@ -302,6 +305,35 @@ __device__ __forceinline__ void theta_pass(const IcdConst &K, const uint32_t *co
                     }
                 }
             }
+        }
+    }
+}
+
+// One column's theta: every lane's partial sums (theta_pass, when `run`),
+// folded over the view groups of the warp and stored by group 0 into the
+// warp's row of S.th1 / S.th2.
+template <int KW, int kUnroll, int VEC, bool kStaged, int kHuber>
+__device__ __forceinline__ void theta_column(const IcdConst &K, const uint32_t *col_rec, const float *__restrict__ err,
+                                             const float *__restrict__ wgt, int gfirst, int gstride, int nv, int RW,
+                                             int NT, int row0, bool run, int lprp, int grp, int t0, int warp,
+                                             IcdSmem &S)
+{
+    float th1[VEC], th2[VEC];
+#pragma unroll
+    for (int i = 0; i < VEC; i++) th1[i] = th2[i] = 0.0f;
+    if (run) theta_pass<KW, kUnroll, VEC, kStaged, kHuber>(K, col_rec, err, wgt, gfirst, gstride, nv, RW, NT, row0, th1, th2);
+    for (int off = lprp; off < 32; off <<= 1) {
+#pragma unroll
+        for (int i = 0; i < VEC; i++) {
+            th1[i] += __shfl_xor_sync(0xffffffffu, th1[i], off);
+            th2[i] += __shfl_xor_sync(0xffffffffu, th2[i], off);
+        }
+    }
+    if (grp == 0 && run) {
+#pragma unroll
+        for (int i = 0; i < VEC; i++) {
+            S.th1[warp][t0 + i] = th1[i];
+            S.th2[warp][t0 + i] = th2[i];
         }
     }
 }
@@ -454,9 +486,23 @@ __device__ __forceinline__ void icd_update_sv(const Geom &g, const IcdLaunch &L,
                 // neighbour (in-column neighbours are the column's own values)
                 active_pred = !L.zero_skipping || iter <= 1 || (zl && V != 0.0f) || pos;
             }
+            // ---- 2. theta over the column's views. When the column is surely
+            //         active (zero skipping off or in its first iteration, or a
+            //         nonzero slice: the same test in every warp, as every warp
+            //         read the column), theta runs before the barrier that also
+            //         publishes the neighbourhood sums, so its loads go out without
+            //         waiting for the other warps; otherwise after it, and only
+            //         for an active column -------------------------------------------
+            bool recs_ok = true;
             if (kStaged && ch == 0)  // issued one column earlier
-                wait_staged(&S.stage_bar[ci & 1], cnt.phases, ci & 1, cnt.timeouts, S.abort, S.abort_bar,
-                            S.abort_parity);
+                recs_ok = wait_staged(&S.stage_bar[ci & 1], cnt.phases, ci & 1, cnt.timeouts, S.abort, S.abort_bar,
+                                      S.abort_parity);
+            const bool sure = !L.zero_skipping || iter <= 1 || __any_sync(0xffffffffu, zl && V != 0.0f);
+            // a thread whose wait gave up reads no record (their headers address
+            // the sinogram); the CTA leaves after the barrier
+            if (sure)
+                theta_column<KW, kUnroll, VEC, kStaged, kHuber>(K, col_rec, err, wgt, gfirst, gstride, nv, RW, NT,
+                                                               rbase + t0, row_ok && recs_ok, lprp, grp, t0, warp, S);
             const int any_active = __syncthreads_or(active_pred);
             if (ch == 0) {
                 // a late copy leaves this column's records undefined: no update, no
@@ -474,32 +520,11 @@ __device__ __forceinline__ void icd_update_sv(const Geom &g, const IcdLaunch &L,
                 if (warp == 0 && lane == 0 && ch == 0) mag[(size_t)f * nxy + c] = 0.0f;
                 continue;  // uniform across the CTA
             }
-
-            // ---- 2. theta over the column's views -----------------------------------
-            {
-                float th1[VEC], th2[VEC];
-#pragma unroll
-                for (int i = 0; i < VEC; i++) th1[i] = th2[i] = 0.0f;
-                if (row_ok)
-                    theta_pass<KW, kUnroll, VEC, kStaged, kHuber>(K, col_rec, err, wgt, gfirst, gstride, nv, RW, NT,
-                                                                 rbase + t0, th1, th2);
-                // fold the view groups of the warp onto group 0
-                for (int off = lprp; off < 32; off <<= 1) {
-#pragma unroll
-                    for (int i = 0; i < VEC; i++) {
-                        th1[i] += __shfl_xor_sync(0xffffffffu, th1[i], off);
-                        th2[i] += __shfl_xor_sync(0xffffffffu, th2[i], off);
-                    }
-                }
-                if (grp == 0 && row_ok) {
-#pragma unroll
-                    for (int i = 0; i < VEC; i++) {
-                        S.th1[warp][t0 + i] = th1[i];
-                        S.th2[warp][t0 + i] = th2[i];
-                    }
-                }
+            if (!sure) {  // uniform across the CTA
+                theta_column<KW, kUnroll, VEC, kStaged, kHuber>(K, col_rec, err, wgt, gfirst, gstride, nv, RW, NT,
+                                                               rbase + t0, row_ok && recs_ok, lprp, grp, t0, warp, S);
+                __syncthreads();
             }
-            __syncthreads();
 
             // ---- 3. zero-skipping and solve (warp 0, lane = slice of the chunk) ------
             if (warp == 0) {

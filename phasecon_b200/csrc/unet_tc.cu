@@ -24,16 +24,18 @@
 // The halo is staged by threads rather than by a TMA tile load: a tile load
 // whose box rows are 16 bytes (8 channels of one voxel, the row of a core
 // matrix) moved about 8 bytes per cycle per SM, which bound the kernel; 128
-// producer threads with 16-byte loads fill the same tile an order of
-// magnitude faster and then make their shared-memory stores visible to the
-// tensor cores (fence.proxy.async) before arriving on the stage's mbarrier.
+// producer threads issue 16-byte asynchronous copies (cp.async, zero-filled
+// outside the grid) whose completion arrives on the stage's mbarrier, so the
+// producers run ahead over all stages without holding the data in
+// registers; the MMA issuer orders the copies before the tensor cores' reads
+// (fence.proxy.async) once the stage is full.
 //
 // Persistent, warp-specialised CTA (one per SM), 9 warps:
 //   warps 0-3       producers: per (tile, chunk) item, wait for a free stage;
 //                   thread 0 posts the weight bytes on the stage's "full"
-//                   mbarrier and issues their bulk copy; all 128 threads load
-//                   the halo (16-byte vectors, coalesced), store it, fence and
-//                   arrive;
+//                   mbarrier and issues their bulk copy; all 128 threads copy
+//                   the halo (16-byte pieces, coalesced) and arrive when their
+//                   copies land;
 //   warps 4-7       epilogue: tcgen05.ld of the accumulator (warp w reads the
 //                   TMEM lanes of its quadrant w % 4 = output rows), bias,
 //                   ReLU, BF16, 32-byte stores; then free the accumulator;
@@ -273,36 +275,33 @@ __global__ void __launch_bounds__(kThreads, 1)
                     bulk_load(st + 2 * kHalfBytes, wtc + ((size_t)ns * g.nchunks + c) * (C::kWBytes / 2),
                               (uint32_t)C::kWBytes, fb);
                 }
-                uint4 v[kPerProducer];
+                // the halo by asynchronous 16-byte copies (zero-filled outside
+                // the frame: the convolution's padding) that hold no registers
+                // while in flight, so the producers go on to the next free
+                // stage at once; the stage's mbarrier sees each thread's arrival
+                // when its copies have landed
 #pragma unroll
                 for (int r = 0; r < kPerProducer; r++) {
                     const int e = tid + r * kProducers;  // piece e: halo voxel e / 2, channel half e % 2
-                    v[r] = make_uint4(0u, 0u, 0u, 0u);
                     if (e < kHaloItems) {
                         const int hv = e >> 1, hz = hv / (HY * HX), rr = hv - hz * (HY * HX), hy = rr / HX,
                                   hx = rr - hy * HX;
                         const int z = z0 + hz - 1, y = y0 + hy - 1, x = x0 + hx - 1;
-                        if (z >= zf0 && z < zf1 && z < g.d && y >= 0 && y < g.h && x >= 0 && x < g.w)
-                            v[r] = __ldg(reinterpret_cast<const uint4 *>(
-                                in + (((long long)z * g.h + y) * g.w + x) * Kin + c * 16 + (e & 1) * 8));
-                    }
-                }
-#pragma unroll
-                for (int r = 0; r < kPerProducer; r++) {
-                    const int e = tid + r * kProducers;
-                    if (e < kHaloItems) {
+                        const bool inb = z >= zf0 && z < zf1 && z < g.d && y >= 0 && y < g.h && x >= 0 && x < g.w;
+                        const bf16 *src =
+                            inb ? in + (((long long)z * g.h + y) * g.w + x) * Kin + c * 16 + (e & 1) * 8 : in;
                         const uint32_t dst = st + (uint32_t)((e & 1) * kHalfBytes + (e >> 1) * 16);
-                        asm volatile("st.shared.v4.u32 [%0], {%1, %2, %3, %4};" ::"r"(dst), "r"(v[r].x),
-                                     "r"(v[r].y), "r"(v[r].z), "r"(v[r].w)
+                        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src),
+                                     "r"(inb ? 16 : 0)
                                      : "memory");
                     }
                 }
-                // the stores are read by the tensor cores (async proxy)
-                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                mbar_arrive(fb);
+                asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(fb) : "memory");
             }
             if (!ok) break;
         }
+        // no copy of this thread may land after the CTA has gone
+        asm volatile("cp.async.wait_all;" ::: "memory");
     } else if (warp < 8) {
         // ---- epilogue ----
         const int q = warp & 3;             // TMEM lane quadrant = output rows 32q .. 32q + 31
@@ -366,6 +365,9 @@ __global__ void __launch_bounds__(kThreads, 1)
                 const uint32_t ph = (uint32_t)(it / C::kStages) & 1u;
                 if (!(ok = mbar_wait(smem_u32(&bar_full[s]), ph, abort, 3))) break;
                 tc_fence_after();
+                // the halo was written by the producers' copies (generic proxy)
+                // and is read by the tensor cores (async proxy)
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                 const uint32_t st = base + (uint32_t)s * C::kStage;
                 // descriptors of tap 0; a tap moves the start address (16-byte
                 // units in the low bits, which cannot carry: the stage lies

@@ -229,8 +229,19 @@ def training_pairs_4d(seed: int, ch_steps: int | None = None, rel: float = 1e-4)
     return [(fbp[f], target[f]) for f in range(fbp.shape[0])]
 
 
+def warm_start_score(session: Session, net: UNet, icd_iterations: int = 2) -> float:
+    """The MAP cost a warm start leaves on a held-out scan: the session's object
+    becomes net(FBP), then `icd_iterations` plain ICD iterations run; returns
+    the FP64 cost (lower is better). The cost function judges the network."""
+    warm_start(session, net)
+    for it in range(1, icd_iterations + 1):
+        session.icd_iteration(it)
+    return float(session.cost()[0])
+
+
 def train(net: UNet, pairs, steps: int, lr: float = 1e-3, seed: int = 0, log_every: int = 0,
-          average_from: float = 1.0, average_every: int = 50, val_pairs=None, val_every: int = 250):
+          average_from: float = 1.0, average_every: int = 50, val_pairs=None, val_every: int = 250,
+          val_session: Session | None = None):
     """Adam steps over randomly drawn (input, target) pairs of host arrays;
     returns the loss history. The network's input scale is set so that it
     sees values of order one. Learning rate: a cosine schedule from `lr` down
@@ -239,12 +250,15 @@ def train(net: UNet, pairs, steps: int, lr: float = 1e-3, seed: int = 0, log_eve
     and the network ends as the average of its weights taken every
     `average_every` steps over that tail (stochastic weight averaging).
 
-    With `val_pairs` (held-out pairs, never trained on) the network ends as the
-    candidate with the lowest mean loss on them, the candidates being the
-    weights every `val_every` steps over the second half of the run, the
-    running weight average at the same points of the tail, and the final
-    average: single-sample Adam steps occasionally land on a worse point late
-    in a run, and a held-out loss picks the checkpoint before it."""
+    With `val_session` (a session on a held-out scan, never trained on) or
+    `val_pairs` (held-out pairs) the network ends as the candidate with the
+    lowest score, the candidates being the weights every `val_every` steps
+    over the second half of the run, the running weight average at the same
+    points of the tail, and the final weights: single-sample Adam steps
+    occasionally land on a worse point late in a run. The score is the MAP
+    cost the warm start leaves on the held-out scan after two ICD iterations
+    (warm_start_score) when a session is given, else the mean loss on the
+    held-out pairs."""
     import torch
     rng = np.random.default_rng(seed)
     net.input_scale = 1.0 / max(float(np.mean([np.abs(t).max() for _, t in pairs])), 1e-12)
@@ -254,16 +268,19 @@ def train(net: UNet, pairs, steps: int, lr: float = 1e-3, seed: int = 0, log_eve
                  torch.from_numpy(np.ascontiguousarray(t, np.float32)).cuda()) for x, t in ps]
 
     dev = to_dev(pairs)
-    val = to_dev(val_pairs) if val_pairs else []
+    val = to_dev(val_pairs) if (val_pairs and val_session is None) else []
     best = [np.inf, None]
 
     def consider(params):
         keep = net.get_params()
         net.set_params(params.astype(np.float32))
-        loss = float(np.mean([net.gradients(x, t)[0] for x, t in val]))
+        if val_session is not None:
+            score = warm_start_score(val_session, net)
+        else:
+            score = float(np.mean([net.gradients(x, t)[0] for x, t in val]))
         net.set_params(keep)
-        if loss < best[0]:
-            best[0], best[1] = loss, params.astype(np.float32).copy()
+        if score < best[0]:
+            best[0], best[1] = score, params.astype(np.float32).copy()
 
     hist = []
     tail = int(average_from * steps) if average_from < 1.0 else steps
@@ -279,7 +296,7 @@ def train(net: UNet, pairs, steps: int, lr: float = 1e-3, seed: int = 0, log_eve
             p = net.get_params().astype(np.float64)
             avg = p if avg is None else avg + p
             navg += 1
-        if val and s >= steps // 2 and (s + 1) % val_every == 0:
+        if (val or val_session is not None) and s >= steps // 2 and (s + 1) % val_every == 0:
             consider(net.get_params())
             if navg:
                 consider(avg / navg)
@@ -287,7 +304,7 @@ def train(net: UNet, pairs, steps: int, lr: float = 1e-3, seed: int = 0, log_eve
             print(f"step {s + 1}: loss {np.mean(hist[-log_every:]):.4g}", flush=True)
     if navg:
         net.set_params((avg / navg).astype(np.float32))
-    if val:
+    if val or val_session is not None:
         consider(net.get_params())
         net.set_params(best[1])
     return hist

@@ -6,9 +6,9 @@ weights the first one rescaled): each variance within 1e-6 relative of the
 reference's (FP64 sums in another order; the reference forms some products in
 float). The drop-in reconstruct with quad_convex = 0 (the variance is
 re-estimated in every iteration after the first multires stage) against the
-reference's own reconstruct: final cost within 2e-3 and the written
-variance_estimate within 1e-2 relative (the runs stop at different points of
-the same objective).
+reference's own reconstruct: final cost within 2e-3 at the reference's stop,
+and the written variance_estimate within 1e-2 relative with both runs taken
+to a tight stop (the runs stop at different points of the same objective).
 """
 import os
 
@@ -42,27 +42,45 @@ def test_variance_update_matches_reference():
     s.close()
 
 
-@pytest.mark.skipif(not O.ref_available(), reason="reference build not present")
-def test_reconstruct_huber_with_variance_matches_reference(tmp_path):
-    pb, _ = make_problem(ncol=64, nrow=8, nview=60, nframe=1, seed=5, quad_convex=0, huber_T=2.0, huber_delta=0.2)
-    pb.convg_thresh = 0.05
+def gpu_reconstruct(pb, tmp_path, convg_thresh, max_iterations):
     args = (pb.projections, pb.weights, pb.proj_angles, pb.proj_times, pb.recon_times, pb.proj_rows,
             pb.proj_cols, pb.proj_num, pb.recon_num, pb.vox_wid, pb.rot_center, pb.sig_s, pb.sig_t, pb.c_s, pb.c_t)
     cwd = os.getcwd()
     os.chdir(tmp_path)
     saved = pc.get_options()
     try:
-        pc.set_options(mrf_p=pb.mrf_p, max_iterations=60, cost_rel_tol=0.0)
-        pc.reconstruct(*args, convg_thresh=0.05, remove_rings=0, quad_convex=0, huber_delta=0.2, huber_T=2.0)
+        pc.set_options(mrf_p=pb.mrf_p, max_iterations=max_iterations, cost_rel_tol=0.0)
+        pc.reconstruct(*args, convg_thresh=convg_thresh, remove_rings=0, quad_convex=0, huber_delta=0.2, huber_T=2.0)
         cost = np.fromfile("cost.bin", np.float64)
         var = np.fromfile("variance_estimate.bin", np.float64)[0]
     finally:
         os.chdir(cwd)
         import ctypes
         pc.lib().mbirgpu_set_options(ctypes.byref(saved))
-    wd = str(tmp_path / "ref")
-    _, ref_cost, _ = O.ref_reconstruct(pb, wd, max_iter=60)
+    return cost, var
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference build not present")
+def test_reconstruct_huber_with_variance_matches_reference(tmp_path):
+    """Final cost at the reference's loose stop (convg_thresh 0.05 %, the build
+    with the cost pass); the variance estimate with both runs taken further
+    (convg_thresh 0.002 %, the reference as it ships, without the cost pass
+    whose rounding-level 'cost increased' check stops it early): at the loose
+    stop the GPU's estimate moves by up to 1 % run to run with the order of
+    its concurrent updates (measured), at the tight one by under 0.1 %, and
+    it lies 0.6 % from the reference's (measured)."""
+    pb, _ = make_problem(ncol=64, nrow=8, nview=60, nframe=1, seed=5, quad_convex=0, huber_T=2.0, huber_delta=0.2)
+    pb.convg_thresh = 0.05
+    (tmp_path / "loose").mkdir()
+    cost, _ = gpu_reconstruct(pb, tmp_path / "loose", 0.05, 60)
+    _, ref_cost, _ = O.ref_reconstruct(pb, str(tmp_path / "ref_loose"), max_iter=60)
+    assert abs(cost[-1] - ref_cost[-1]) / abs(ref_cost[-1]) < 2e-3, (cost[-1], ref_cost[-1])
+
+    pb.convg_thresh = 0.002
+    (tmp_path / "tight").mkdir()
+    _, var = gpu_reconstruct(pb, tmp_path / "tight", 0.002, 400)
+    wd = str(tmp_path / "ref_tight")
+    O.ref_reconstruct(pb, wd, max_iter=400, timing=True)
     ref_var = np.fromfile(os.path.join(wd, "variance_estimate.bin"), np.float64)[0]
     assert ref_var != pytest.approx(1.0, rel=1e-3)
     assert var == pytest.approx(ref_var, rel=1e-2)
-    assert abs(cost[-1] - ref_cost[-1]) / abs(ref_cost[-1]) < 2e-3, (cost[-1], ref_cost[-1])
