@@ -33,6 +33,7 @@ lines instead.
 from __future__ import annotations
 
 import argparse
+import dataclasses
 import json
 import math
 import os
@@ -385,19 +386,30 @@ def run_ours(args, world, rank, local, pg):
             conv["cost_rel_err_vs_fp64_oracle"] = abs(gpu_cost - orc_cost) / abs(orc_cost)
         except Exception as ex:  # the oracle is the checker only; its absence does not stop the bench
             conv["cost_rel_err_vs_fp64_oracle"] = f"unavailable: {ex}"
+    obj_shape = tuple(s.shape)
     s.close()
 
-    # end to end through the public API with host buffers
-    h_arrays = pb.arrays()
+    # end to end through the public API with host buffers: the measured
+    # sinogram and weights in pinned host memory (copied there before the
+    # timed region), the object read back into a pinned buffer
+    def pinned(a):
+        t = torch.empty(a.shape, dtype=torch.float32, pin_memory=True)
+        t.numpy()[...] = a
+        return t
+
+    keep = [pinned(pb.projections), pinned(pb.weights)]
+    pb_host = dataclasses.replace(pb, projections=keep[0].numpy(), weights=keep[1].numpy())
+    h_arrays = pb_host.arrays()
     h2d = sum(a.nbytes for a in h_arrays)
+    obj_t = torch.empty(obj_shape, dtype=torch.float32, pin_memory=True)
     torch.cuda.synchronize()
     barrier(pg)
     t0 = time.perf_counter()
-    s2 = pc.Session(pb, options=opt, stream=stream.cuda_stream)
+    s2 = pc.Session(pb_host, options=opt, stream=stream.cuda_stream)
     e2e_upd = 0
     for it in range(1, args.steps + 1):
         e2e_upd += s2.icd_iteration(it).voxel_updates
-    obj = s2.get_object()
+    obj = s2.get_object(out=obj_t.numpy())
     torch.cuda.synchronize()
     t_e2e = max_over_ranks(pg, time.perf_counter() - t0)
     s2.close()
@@ -405,8 +417,8 @@ def run_ours(args, world, rank, local, pg):
     e2e = {"value": sum_over_ranks(pg, float(e2e_upd)) / t_e2e, "unit": UNIT,
            "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
            "steps_per_call": args.steps,
-           "note": "one session from host arrays (H2D of y, w, angles, times), A-matrix build, K iterations, "
-                   "D2H of the object; bytes per step = bytes per call / K"}
+           "note": "one session from pinned host arrays (H2D of y, w, angles, times), A-matrix build, K "
+                   "iterations, D2H of the object into pinned memory; bytes per step = bytes per call / K"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -564,7 +576,7 @@ def warmstart_section(args, rank: int, local: int, pb, p: float) -> dict:
                 "initial_cost": costs[0], "final_cost": costs[-1]}
 
     starts = {"zero": s.set_object_zero, "fbp": s.set_object_fbp}
-    res, seeds, train_s, losses = {}, [], [], []
+    res, seeds, train_s, losses, held_out = {}, [], [], [], []
     with ClockSampler(local) as clk:
         for name, fn in starts.items():
             timed_start(fn)  # untimed: module loading, the FBP's allocations
@@ -574,8 +586,14 @@ def warmstart_section(args, rank: int, local: int, pb, p: float) -> dict:
         net = WS.UNet(16, seed=rank * 1000 + k)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
+        sc = []
         hist = WS.train(net, pairs, args.train_steps, lr=1e-3, seed=rank * 1000 + k, average_from=args.average_from,
-                        val_session=s_val)
+                        val_session=s_val, scores=sc)
+        picked = sc[sc[-1]] if sc and sc[-1] is not None else None
+        held_out.append({"candidates": len(sc) - 1, "chosen_step": picked[0] if picked else None,
+                         "chosen_averaged": picked[1] if picked else None,
+                         "chosen_cost": picked[2] if picked else None,
+                         "worst_cost": max(c[2] for c in sc[:-1]) if len(sc) > 1 else None})
         torch.cuda.synchronize()
         train_s.append(time.perf_counter() - t0)
         losses.append([float(np.mean(hist[:20])), float(np.mean(hist[-20:]))])
@@ -596,7 +614,9 @@ def warmstart_section(args, rank: int, local: int, pb, p: float) -> dict:
             "target_cost": target, "starts": res, "unet_starts": seeds,
             "train": {"pairs": len(pairs), "cahn_hilliard_pairs": n_ch, "ellipsoid_pairs": len(pairs) - n_ch,
                       "checkpoint_selection": "lowest MAP cost after the warm start and 2 ICD iterations on a "
-                                              "held-out 4-D scan (seed 9000)",
+                                              "held-out 4-D scan (seed 9000), candidates every 250 steps from "
+                                              "a quarter of the run",
+                      "held_out_selection": held_out,
                       "steps": args.train_steps, "seeds": args.ws_seeds, "data_s": t_data, "train_s": train_s,
                       "loss_first_last": losses},
             "unet": "4 levels 16/32/64/128, 3x3x3, BF16 weights and activations, FP32 accumulation",

@@ -5,8 +5,11 @@
 // compiled without multiply-add contraction) so that H_r, and therefore every
 // A-matrix value built from it on the device, equals the reference's bit for
 // bit.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <thread>
+#include <vector>
 #include "mbir_internal.h"
 
 namespace mbirgpu {
@@ -30,21 +33,16 @@ double grid_distance(int a, int b, int c, int d)
 // trapezoidal line-integral profile at the view's angle (XT_Profile.c:47-104,
 // stored as the reference's Real_arr_t: float in MBIR_4D, double in
 // PCMBIR_3D) convolved with a normalised Hamming beam (XT_Profile.c:108-124),
-// sampled every OffsetR.
+// sampled every OffsetR. Views are independent: they are split over host
+// threads (each view's arithmetic is the same whichever thread runs it).
 template <typename T>
-void detector_response_t(const Geom &g, const float *angles, T *H_r, int bins, int beam_res)
+void detector_response_views(const Geom &g, const float *angles, T *H_r, int bins, int beam_res,
+                             const std::vector<double> &beam, int v_begin, int v_end)
 {
-    std::vector<double> beam(beam_res);
     std::vector<T> prof(kProfileRes);
-    double total = 0;
-    for (int i = 0; i < beam_res; i++) {
-        beam[i] = 0.54 - 0.46 * std::cos((2 * 3.14159265358979323846 / beam_res) * i);
-        total = total + beam[i];
-    }
-    for (int i = 0; i < beam_res; i++) beam[i] /= total;
     const double r0 = -(g.delta_r) / 2, step = (g.delta_r) / beam_res;
     const double to_bin = (kProfileRes) / (2 * g.delta_xy);
-    for (int v = 0; v < g.N_p; v++) {
+    for (int v = v_begin; v < v_end; v++) {
         double ang = angles[v];
         while (ang > kHalfPi) ang -= kHalfPi;
         while (ang < 0) ang += kHalfPi;
@@ -75,6 +73,31 @@ void detector_response_t(const Geom &g, const float *angles, T *H_r, int bins, i
         }
         h[bins] = 0;
     }
+}
+
+template <typename T>
+void detector_response_t(const Geom &g, const float *angles, T *H_r, int bins, int beam_res)
+{
+    std::vector<double> beam(beam_res);
+    double total = 0;
+    for (int i = 0; i < beam_res; i++) {
+        beam[i] = 0.54 - 0.46 * std::cos((2 * 3.14159265358979323846 / beam_res) * i);
+        total = total + beam[i];
+    }
+    for (int i = 0; i < beam_res; i++) beam[i] /= total;
+    // about 32 k beam-sample steps per view: threads pay off from a few dozen views
+    const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+    const int nt = std::max(1, std::min({hw, 32, g.N_p / 16}));
+    if (nt == 1) {
+        detector_response_views<T>(g, angles, H_r, bins, beam_res, beam, 0, g.N_p);
+        return;
+    }
+    std::vector<std::thread> pool;
+    for (int t = 0; t < nt; t++) {
+        const int a = (int)((long long)g.N_p * t / nt), b = (int)((long long)g.N_p * (t + 1) / nt);
+        pool.emplace_back(detector_response_views<T>, std::cref(g), angles, H_r, bins, beam_res, std::cref(beam), a, b);
+    }
+    for (auto &th : pool) th.join();
 }
 
 }  // namespace

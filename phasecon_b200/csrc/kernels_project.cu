@@ -32,6 +32,25 @@ __global__ void transpose_rows_cols(const float *__restrict__ in, float *__restr
     }
 }
 
+// w16[i] = w[i] when w[i] is an integer in [0, 65535]; *inexact |= 1 where one is not.
+__global__ void weights_u16_kernel(const float *__restrict__ w, size_t n, uint16_t *__restrict__ w16,
+                                   int *__restrict__ inexact)
+{
+    int bad = 0;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const float v = w[i];
+        const bool ok = v >= 0.0f && v <= 65535.0f && v == rintf(v);
+        w16[i] = ok ? (uint16_t)v : (uint16_t)0;
+        bad |= !ok;
+    }
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(inexact, 1);
+}
+
+void launch_weights_u16(const float *d_w, size_t n, uint16_t *d_w16, int *d_inexact, cudaStream_t st)
+{
+    weights_u16_kernel<<<148 * 8, 256, 0, st>>>(d_w, n, d_w16, d_inexact);
+}
+
 void launch_transpose_sino(const float *in, float *out, int N_p, int N_t, int N_r, cudaStream_t st)
 {
     dim3 grid((N_r + 31) / 32, (N_t + 31) / 32, N_p), block(32, 8);
@@ -74,6 +93,9 @@ constexpr int kFpTx = 8, kFpTy = 4, kFpCols = kFpTx * kFpTy;  // 32 columns: one
 constexpr int kFpBand = 16;                                   // channels of a warp's band
 constexpr int kFpWarps = 8;
 
+// KW: 16-byte words per A record (1, 2, 3 for voxel scale 1, 2, 4), so the
+// value loop has its compile-time bound 4 KW - 1.
+template <int KW>
 __global__ void __launch_bounds__(kFpWarps * 32) forward_project_kernel(Geom g, const uint32_t *__restrict__ table,
                                                                        const int32_t *__restrict__ view_first,
                                                                        const float *__restrict__ x,
@@ -113,16 +135,17 @@ __global__ void __launch_bounds__(kFpWarps * 32) forward_project_kernel(Geom g, 
     const bool lane_col = ((active >> lane) & 1) != 0;
     const uint32_t *lane_rec = lane_col ? table + ((size_t)fv0 * nxy + ((size_t)lj * g.N_x + lk) * nv) * g.rec_words : nullptr;
     double *band = &s_band[warp][0][0];
-    const int n4 = g.rec_words >> 2;  // 16-byte words per record: 1, 2 or 3
+    double *my_band = band + lane;
     for (int v = warp; v < nv; v += kFpWarps) {
         // lane l holds column l's record for this view; the band starts at the
         // smallest first sinogram row of the view's entries
-        uint4 rw[3] = {make_uint4(0u, 0u, 0u, 0u), make_uint4(0u, 0u, 0u, 0u), make_uint4(0u, 0u, 0u, 0u)};
+        uint4 rw[KW];
+#pragma unroll
+        for (int k = 0; k < KW; k++) rw[k] = make_uint4(0u, 0u, 0u, 0u);
         if (lane_col) {
             const uint4 *r4 = reinterpret_cast<const uint4 *>(lane_rec + (size_t)v * g.rec_words);
 #pragma unroll
-            for (int k = 0; k < 3; k++)
-                if (k < n4) rw[k] = __ldg(r4 + k);
+            for (int k = 0; k < KW; k++) rw[k] = __ldg(r4 + k);
         }
         const uint32_t hdr = rw[0].x;
         int lo = (hdr >> 24) ? (int)(hdr & 0xFFFFFFu) : 0x7FFFFFFF;
@@ -135,15 +158,16 @@ __global__ void __launch_bounds__(kFpWarps * 32) forward_project_kernel(Geom g, 
             if (!cnt) continue;  // also the inactive columns (header 0); uniform over the warp
             const int row = (int)(hi & 0xFFFFFFu);
             const double xv = s_x[i][lane];
+            const int o0 = row - lo;
 #pragma unroll
-            for (int q = 0; q < 11; q++) {  // value q is word 1 + q of column i's record
+            for (int q = 0; q < 4 * KW - 1; q++) {  // value q is word 1 + q of column i's record
                 if (q < cnt) {
                     const uint4 &u = rw[(1 + q) >> 2];
                     const uint32_t mine = ((1 + q) & 3) == 0 ? u.x : ((1 + q) & 3) == 1 ? u.y : ((1 + q) & 3) == 2 ? u.z : u.w;
                     const double val = xv * (double)__uint_as_float(__shfl_sync(0xffffffffu, mine, i));
-                    const int o = row + q - lo;
+                    const int o = o0 + q;
                     if (o < kFpBand) {
-                        band[o * 32 + lane] += val;
+                        my_band[o * 32] += val;
                         used |= 1 << o;
                     } else if (row_ok) {
                         atomicAdd(acc + (size_t)(row + q) * g.N_t + t, val);
@@ -154,8 +178,8 @@ __global__ void __launch_bounds__(kFpWarps * 32) forward_project_kernel(Geom g, 
         while (used) {
             const int o = __ffs(used) - 1;
             used &= used - 1;
-            const double s = band[o * 32 + lane];
-            band[o * 32 + lane] = 0.0;
+            const double s = my_band[o * 32];
+            my_band[o * 32] = 0.0;
             if (row_ok && s != 0.0) atomicAdd(acc + (size_t)(lo + o) * g.N_t + t, s);
         }
     }
@@ -182,7 +206,12 @@ void launch_forward_project(const Geom &g, const uint32_t *d_table, const int32_
     cudaMemsetAsync(d_acc, 0, n * sizeof(double), st);
     const long long blocks = (long long)g.N_time * ((g.N_y + kFpTy - 1) / kFpTy) * ((g.N_x + kFpTx - 1) / kFpTx) *
                              ((g.N_t + kRowChunk - 1) / kRowChunk);
-    forward_project_kernel<<<(unsigned)blocks, kFpWarps * 32, 0, st>>>(g, d_table, d_view_first, d_x, d_acc);
+    if (g.rec_words == 4)
+        forward_project_kernel<1><<<(unsigned)blocks, kFpWarps * 32, 0, st>>>(g, d_table, d_view_first, d_x, d_acc);
+    else if (g.rec_words == 8)
+        forward_project_kernel<2><<<(unsigned)blocks, kFpWarps * 32, 0, st>>>(g, d_table, d_view_first, d_x, d_acc);
+    else
+        forward_project_kernel<3><<<(unsigned)blocks, kFpWarps * 32, 0, st>>>(g, d_table, d_view_first, d_x, d_acc);
     finish_projection_kernel<<<148 * 8, 256, 0, st>>>(n, d_acc, d_y, d_out, d_off, g.N_r * g.N_t);
 }
 

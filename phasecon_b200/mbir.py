@@ -58,8 +58,8 @@ class Options(C.Structure):
         ("sv_size", C.c_int32), ("cta_warps", C.c_int32), ("icd_unroll", C.c_int32), ("seed", C.c_uint64),
         ("nhicd_passes", C.c_int32), ("sv_colors", C.c_int32), ("stage_records", C.c_int32),
         ("nh_sv_size", C.c_int32), ("nh_sv_colors", C.c_int32), ("nh_cta_warps", C.c_int32),
-        ("nh_work_lists", C.c_int32), ("autotune", C.c_int32), 
-        ("graph_iterations", C.c_int32),
+        ("nh_work_lists", C.c_int32), ("autotune", C.c_int32),
+        ("graph_iterations", C.c_int32), ("weights16", C.c_int32),
     ]
 
 
@@ -80,7 +80,7 @@ class SessionInfo(C.Structure):
         ("N_y", C.c_int32), ("N_z", C.c_int32), ("mult_xy", C.c_int32), ("mult_z", C.c_int32),
         ("max_views", C.c_int32), ("kmax", C.c_int32), ("sv_size", C.c_int32), ("cta_warps", C.c_int32),
         ("masked_columns", C.c_int64), ("nnz", C.c_int64), ("delta_t", C.c_double), ("device_bytes", C.c_size_t),
-        ("sv_colors", C.c_int32),
+        ("sv_colors", C.c_int32), ("weights16", C.c_int32),
     ]
 
 
@@ -305,10 +305,15 @@ class Session:
         a = np.ascontiguousarray(obj, np.float32).reshape(self.shape)
         _check(lib().mbirgpu_session_set_object(self.h, a.ctypes.data))
 
-    def get_object(self) -> np.ndarray:
-        a = np.zeros(self.shape, np.float32)
-        _check(lib().mbirgpu_session_get_object(self.h, a.ctypes.data))
-        return a
+    def get_object(self, out: np.ndarray | None = None) -> np.ndarray:
+        """The object [N_time][N_z][N_y][N_x]; into `out` (a C-contiguous float32
+        array of that shape, e.g. in pinned memory) when given."""
+        if out is None:
+            out = np.zeros(self.shape, np.float32)
+        elif out.dtype != np.float32 or out.shape != tuple(self.shape) or not out.flags.c_contiguous:
+            raise ValueError(f"out must be a C-contiguous float32 array of shape {tuple(self.shape)}")
+        _check(lib().mbirgpu_session_get_object(self.h, out.ctypes.data))
+        return out
 
     def refresh_error(self) -> None:
         _check(lib().mbirgpu_session_refresh_error(self.h))

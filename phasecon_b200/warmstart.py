@@ -241,7 +241,7 @@ def warm_start_score(session: Session, net: UNet, icd_iterations: int = 2) -> fl
 
 def train(net: UNet, pairs, steps: int, lr: float = 1e-3, seed: int = 0, log_every: int = 0,
           average_from: float = 1.0, average_every: int = 50, val_pairs=None, val_every: int = 250,
-          val_session: Session | None = None):
+          val_session: Session | None = None, scores: list | None = None):
     """Adam steps over randomly drawn (input, target) pairs of host arrays;
     returns the loss history. The network's input scale is set so that it
     sees values of order one. Learning rate: a cosine schedule from `lr` down
@@ -253,12 +253,13 @@ def train(net: UNet, pairs, steps: int, lr: float = 1e-3, seed: int = 0, log_eve
     With `val_session` (a session on a held-out scan, never trained on) or
     `val_pairs` (held-out pairs) the network ends as the candidate with the
     lowest score, the candidates being the weights every `val_every` steps
-    over the second half of the run, the running weight average at the same
+    from a quarter of the run on, the running weight average at the same
     points of the tail, and the final weights: single-sample Adam steps
     occasionally land on a worse point late in a run. The score is the MAP
     cost the warm start leaves on the held-out scan after two ICD iterations
     (warm_start_score) when a session is given, else the mean loss on the
-    held-out pairs."""
+    held-out pairs. `scores`, when given, receives (step, averaged, score)
+    for every candidate and the index of the chosen one last."""
     import torch
     rng = np.random.default_rng(seed)
     net.input_scale = 1.0 / max(float(np.mean([np.abs(t).max() for _, t in pairs])), 1e-12)
@@ -271,7 +272,9 @@ def train(net: UNet, pairs, steps: int, lr: float = 1e-3, seed: int = 0, log_eve
     val = to_dev(val_pairs) if (val_pairs and val_session is None) else []
     best = [np.inf, None]
 
-    def consider(params):
+    chosen = [None]
+
+    def consider(params, step=-1, averaged=False):
         keep = net.get_params()
         net.set_params(params.astype(np.float32))
         if val_session is not None:
@@ -279,8 +282,11 @@ def train(net: UNet, pairs, steps: int, lr: float = 1e-3, seed: int = 0, log_eve
         else:
             score = float(np.mean([net.gradients(x, t)[0] for x, t in val]))
         net.set_params(keep)
+        if scores is not None:
+            scores.append((step, averaged, score))
         if score < best[0]:
             best[0], best[1] = score, params.astype(np.float32).copy()
+            chosen[0] = len(scores) - 1 if scores is not None else None
 
     hist = []
     tail = int(average_from * steps) if average_from < 1.0 else steps
@@ -296,15 +302,17 @@ def train(net: UNet, pairs, steps: int, lr: float = 1e-3, seed: int = 0, log_eve
             p = net.get_params().astype(np.float64)
             avg = p if avg is None else avg + p
             navg += 1
-        if (val or val_session is not None) and s >= steps // 2 and (s + 1) % val_every == 0:
-            consider(net.get_params())
+        if (val or val_session is not None) and s >= steps // 4 and (s + 1) % val_every == 0:
+            consider(net.get_params(), s + 1)
             if navg:
-                consider(avg / navg)
+                consider(avg / navg, s + 1, True)
         if log_every and (s + 1) % log_every == 0:
             print(f"step {s + 1}: loss {np.mean(hist[-log_every:]):.4g}", flush=True)
     if navg:
         net.set_params((avg / navg).astype(np.float32))
     if val or val_session is not None:
-        consider(net.get_params())
+        consider(net.get_params(), steps, navg > 0)
         net.set_params(best[1])
+        if scores is not None:
+            scores.append(chosen[0])
     return hist

