@@ -613,9 +613,8 @@ def warmstart_section(args, rank: int, local: int, pb, p: float) -> dict:
             "speedup_vs_fbp_init_per_seed": [tf / r["time_to_converged_cost_s"] for r in seeds],
             "target_cost": target, "starts": res, "unet_starts": seeds,
             "train": {"pairs": len(pairs), "cahn_hilliard_pairs": n_ch, "ellipsoid_pairs": len(pairs) - n_ch,
-                      "checkpoint_selection": "lowest MAP cost after the warm start and 2 ICD iterations on a "
-                                              "held-out 4-D scan (seed 9000), candidates every 250 steps from "
-                                              "a quarter of the run",
+                      "checkpoint_selection": "lowest MAP cost the warm start leaves on a held-out 4-D scan "
+                                              "(seed 9000), candidates every 250 steps from a quarter of the run",
                       "held_out_selection": held_out,
                       "steps": args.train_steps, "seeds": args.ws_seeds, "data_s": t_data, "train_s": train_s,
                       "loss_first_last": losses},

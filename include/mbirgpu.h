@@ -93,10 +93,6 @@ typedef struct {
                                 iteration number from device memory); iterations with ring
                                 correction or variance re-estimation, and the legacy default
                                 stream, launch directly. 0: always launch directly */
-    int32_t weights16;       /* 1 (default): when every weight is an integer in [0, 65535] (count
-                                weights) and the data term is quadratic, the ICD sweep reads a
-                                16-bit integer copy of the weights (exact, half the bytes);
-                                0: always the FP32 weights */
 } mbirgpu_options;
 
 /* Defaults as listed above. */
@@ -142,7 +138,6 @@ typedef struct {
     double delta_t;
     size_t device_bytes;     /* device memory the session holds */
     int32_t sv_colors;       /* K of the K x K super-voxel colouring in use */
-    int32_t weights16;       /* 1: the sweep reads the 16-bit integer weights (options.weights16) */
 } mbirgpu_session_info;
 
 typedef struct {

@@ -261,33 +261,13 @@ __device__ __forceinline__ void flush_counts(IcdCount &cnt, IcdStats *stats)
     cnt.phases = phases;
 }
 
-// VEC consecutive weights into wv: FP32 weights as one vector load; weights
-// kept as 16-bit integers (exact: every weight an integer below 2^16) as one
-// load of half the bytes, converted exactly to float.
-__device__ __forceinline__ void load_weights(const float *w, float (&wv)[4])
-{
-    VecF<4>::get(__ldg(reinterpret_cast<const float4 *>(w)), wv);
-}
-__device__ __forceinline__ void load_weights(const float *w, float (&wv)[2])
-{
-    VecF<2>::get(__ldg(reinterpret_cast<const float2 *>(w)), wv);
-}
-__device__ __forceinline__ void load_weights(const uint16_t *w, float (&wv)[4])
-{
-    const uint2 r = __ldg(reinterpret_cast<const uint2 *>(w));
-    wv[0] = (float)(r.x & 0xFFFFu);
-    wv[1] = (float)(r.x >> 16);
-    wv[2] = (float)(r.y & 0xFFFFu);
-    wv[3] = (float)(r.y >> 16);
-}
-
 // theta1 / theta2 partial sums of one lane (VEC detector rows starting at
 // sinogram row offset `row0` within each A entry's row, views gfirst,
 // gfirst + gstride, ... of the column): theta1 = -sum a w e,
 // theta2 = sum a^2 w with a = A value x delta_t (XT_VoxUpdate.c:56-85).
-template <int KW, int kUnroll, int VEC, bool kStaged, int kHuber, typename WT>
+template <int KW, int kUnroll, int VEC, bool kStaged, int kHuber>
 __device__ __forceinline__ void theta_pass(const IcdConst &K, const uint32_t *col_rec, const float *__restrict__ err,
-                                           const WT *__restrict__ wgt, int gfirst, int gstride, int nv, int RW,
+                                           const float *__restrict__ wgt, int gfirst, int gstride, int nv, int RW,
                                            int NT, int row0, float (&th1)[VEC], float (&th2)[VEC])
 {
     using VT = typename VecF<VEC>::T;
@@ -310,7 +290,7 @@ __device__ __forceinline__ void theta_pass(const IcdConst &K, const uint32_t *co
                 if (q < cnt_q) {
                     float ev[VEC], wv[VEC];
                     VecF<VEC>::get(__ldcg(reinterpret_cast<const VT *>(err + (sb + (unsigned)(q * NT)))), ev);
-                    load_weights(wgt + (sb + (unsigned)(q * NT)), wv);
+                    VecF<VEC>::get(__ldg(reinterpret_cast<const VT *>(wgt + (sb + (unsigned)(q * NT)))), wv);
                     const float a = rec_val<KW>(R[u], q) * K.dt;
 #pragma unroll
                     for (int i = 0; i < VEC; i++) {
@@ -332,17 +312,16 @@ __device__ __forceinline__ void theta_pass(const IcdConst &K, const uint32_t *co
 // One column's theta: every lane's partial sums (theta_pass, when `run`),
 // folded over the view groups of the warp and stored by group 0 into the
 // warp's row of S.th1 / S.th2.
-template <int KW, int kUnroll, int VEC, bool kStaged, int kHuber, typename WT>
+template <int KW, int kUnroll, int VEC, bool kStaged, int kHuber>
 __device__ __forceinline__ void theta_column(const IcdConst &K, const uint32_t *col_rec, const float *__restrict__ err,
-                                             const WT *__restrict__ wgt, int gfirst, int gstride, int nv, int RW,
+                                             const float *__restrict__ wgt, int gfirst, int gstride, int nv, int RW,
                                              int NT, int row0, bool run, int lprp, int grp, int t0, int warp,
                                              IcdSmem &S)
 {
     float th1[VEC], th2[VEC];
 #pragma unroll
     for (int i = 0; i < VEC; i++) th1[i] = th2[i] = 0.0f;
-    if (run)
-        theta_pass<KW, kUnroll, VEC, kStaged, kHuber, WT>(K, col_rec, err, wgt, gfirst, gstride, nv, RW, NT, row0, th1, th2);
+    if (run) theta_pass<KW, kUnroll, VEC, kStaged, kHuber>(K, col_rec, err, wgt, gfirst, gstride, nv, RW, NT, row0, th1, th2);
     for (int off = lprp; off < 32; off <<= 1) {
 #pragma unroll
         for (int i = 0; i < VEC; i++) {
@@ -370,12 +349,12 @@ __device__ __forceinline__ void theta_column(const IcdConst &K, const uint32_t *
 // round trip per view group instead of two and the apply pass on none.
 // kHuber: 0 the quadratic data term, 1 the generalised Huber one
 // (XT_VoxUpdate.c:68-82), 2 decided per problem at run time (K.huber).
-template <int KW, int kUnroll, int VEC, bool kStaged, int kHuber, typename WT>
+template <int KW, int kUnroll, int VEC, bool kStaged, int kHuber>
 __device__ __forceinline__ void icd_update_sv(const Geom &g, const IcdLaunch &L, const IcdConst &K,
                                               const uint32_t *__restrict__ table,
                                               const int32_t *__restrict__ view_first,
                                               const uint8_t *__restrict__ mask, float *__restrict__ x,
-                                              float *__restrict__ err, const WT *__restrict__ wgt,
+                                              float *__restrict__ err, const float *__restrict__ wgt,
                                               float *__restrict__ mag, int f, int sx, int sy, IcdSmem &S,
                                               IcdCount &cnt, uint32_t *srec, int stage_words)
 {
@@ -522,7 +501,7 @@ __device__ __forceinline__ void icd_update_sv(const Geom &g, const IcdLaunch &L,
             // a thread whose wait gave up reads no record (their headers address
             // the sinogram); the CTA leaves after the barrier
             if (sure)
-                theta_column<KW, kUnroll, VEC, kStaged, kHuber, WT>(K, col_rec, err, wgt, gfirst, gstride, nv, RW, NT,
+                theta_column<KW, kUnroll, VEC, kStaged, kHuber>(K, col_rec, err, wgt, gfirst, gstride, nv, RW, NT,
                                                                rbase + t0, row_ok && recs_ok, lprp, grp, t0, warp, S);
             const int any_active = __syncthreads_or(active_pred);
             if (ch == 0) {
@@ -542,7 +521,7 @@ __device__ __forceinline__ void icd_update_sv(const Geom &g, const IcdLaunch &L,
                 continue;  // uniform across the CTA
             }
             if (!sure) {  // uniform across the CTA
-                theta_column<KW, kUnroll, VEC, kStaged, kHuber, WT>(K, col_rec, err, wgt, gfirst, gstride, nv, RW, NT,
+                theta_column<KW, kUnroll, VEC, kStaged, kHuber>(K, col_rec, err, wgt, gfirst, gstride, nv, RW, NT,
                                                                rbase + t0, row_ok && recs_ok, lprp, grp, t0, warp, S);
                 __syncthreads();
             }
@@ -676,10 +655,10 @@ __device__ __forceinline__ void icd_update_sv(const Geom &g, const IcdLaunch &L,
 // One colour phase of one problem: persistent CTAs drain the phase's SV queue.
 // With kStaged, the dynamic shared memory holds two record buffers of
 // stage_words words each (the current and the next column's A records).
-template <int KW, int kUnroll, int VEC, bool kStaged, int kHuber, typename WT>
+template <int KW, int kUnroll, int VEC, bool kStaged, int kHuber>
 __global__ void __launch_bounds__(kMaxWarps * 32, 4) icd_phase_kernel(
     Geom g, IcdLaunch L, IcdConst K, const uint32_t *__restrict__ table, const int32_t *__restrict__ view_first,
-    const uint8_t *__restrict__ mask, float *__restrict__ x, float *__restrict__ err, const WT *__restrict__ wgt,
+    const uint8_t *__restrict__ mask, float *__restrict__ x, float *__restrict__ err, const float *__restrict__ wgt,
     float *__restrict__ mag, IcdStats *__restrict__ stats, unsigned int *__restrict__ queue, int stage_words)
 {
     __shared__ IcdSmem S;
@@ -717,7 +696,7 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 4) icd_phase_kernel(
             sy = KC * (rem / hx) + color / KC;
         }
         if (sx >= L.n_sv_x || sy >= L.n_sv_y) continue;  // uniform
-        icd_update_sv<KW, kUnroll, VEC, kStaged, kHuber, WT>(g, L, K, table, view_first, mask, x, err, wgt, mag, f, sx, sy,
+        icd_update_sv<KW, kUnroll, VEC, kStaged, kHuber>(g, L, K, table, view_first, mask, x, err, wgt, mag, f, sx, sy,
                                                          S,
                                                  cnt, s_rec, stage_words);
     }
@@ -731,10 +710,10 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 4) icd_phase_kernel(
 // above this size the sweep reads records from global memory instead.
 constexpr int kMaxStageBytes = 16 * 1024;
 
-template <int KW, int U, int VEC, bool kStaged, int kHuber, typename WT>
+template <int KW, int U, int VEC, bool kStaged, int kHuber>
 static void launch_staged(const Geom &g, const IcdLaunch &L, const IcdConst &K, const uint32_t *d_table,
                           const int32_t *d_view_first, const uint8_t *d_mask, float *d_x, float *d_err,
-                          const WT *d_w, float *d_mag, IcdStats *d_stats, unsigned int *d_queue, int stage_words,
+                          const float *d_w, float *d_mag, IcdStats *d_stats, unsigned int *d_queue, int stage_words,
                           cudaStream_t st)
 {
     const int threads = L.warps * 32;
@@ -762,7 +741,7 @@ static void launch_staged(const Geom &g, const IcdLaunch &L, const IcdConst &K, 
         if (!hit) {
             cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                &per_sm, icd_phase_kernel<KW, U, VEC, kStaged, kHuber, WT>, threads, smem);
+                &per_sm, icd_phase_kernel<KW, U, VEC, kStaged, kHuber>, threads, smem);
             cache.push_back({dev, threads, sms, per_sm, smem});
         }
     }
@@ -770,7 +749,7 @@ static void launch_staged(const Geom &g, const IcdLaunch &L, const IcdConst &K, 
     long long grid = (long long)sms * (per_sm > 0 ? per_sm : 1);
     if (grid > items) grid = items;
     if (L.max_ctas > 0 && grid > L.max_ctas) grid = L.max_ctas;
-    icd_phase_kernel<KW, U, VEC, kStaged, kHuber, WT><<<(unsigned)grid, threads, smem, st>>>(
+    icd_phase_kernel<KW, U, VEC, kStaged, kHuber><<<(unsigned)grid, threads, smem, st>>>(
         g, L, K, d_table, d_view_first, d_mask, d_x, d_err, d_w, d_mag, d_stats, d_queue, stage_words);
 }
 
@@ -782,8 +761,8 @@ static void launch_kw(const Geom &g, const IcdLaunch &L, const IcdConst &K, cons
     const int stage_words = g.max_views * g.rec_words;  // a multiple of 4 words: 16-byte aligned buffers
     const bool staged = L.stage_records && 2 * (size_t)stage_words * sizeof(uint32_t) <= (size_t)kMaxStageBytes;
 #define MBIR_STAGED(S, H)                                                                                         \
-    launch_staged<KW, U, VEC, S, H, float>(g, L, K, d_table, d_view_first, d_mask, d_x, d_err, d_w, d_mag, d_stats, \
-                                           d_queue, S ? stage_words : 0, st)
+    launch_staged<KW, U, VEC, S, H>(g, L, K, d_table, d_view_first, d_mask, d_x, d_err, d_w, d_mag, d_stats, d_queue, \
+                                    S ? stage_words : 0, st)
     if (staged) {
         if (K.huber) MBIR_STAGED(true, 1);
         else MBIR_STAGED(true, 0);
@@ -830,20 +809,6 @@ void launch_icd_phase(const Geom &g, const IcdLaunch &L, const uint32_t *d_table
     launch_kw<KW, U, VEC>(g, L, K, d_table, d_view_first, d_mask, d_x, d_err, d_w, d_mag, d_stats, d_queue, st)
     const int kw = g.rec_words / 4;
     const bool v4 = g.N_t % 4 == 0;
-    // 16-bit integer weights (the quadratic data term, one-word records, four
-    // rows per lane, staged records): half the weight bytes in flight per view,
-    // so three views' entries per round fit where two did
-    const int stage_words = g.max_views * g.rec_words;
-    if (L.w16 && kw == 1 && v4 && !K.huber && L.stage_records &&
-        2 * (size_t)stage_words * sizeof(uint32_t) <= (size_t)kMaxStageBytes) {
-        if (L.unroll >= 3)
-            launch_staged<1, 3, 4, true, 0, uint16_t>(g, L, K, d_table, d_view_first, d_mask, d_x, d_err, L.w16, d_mag,
-                                                      d_stats, d_queue, stage_words, st);
-        else
-            launch_staged<1, 2, 4, true, 0, uint16_t>(g, L, K, d_table, d_view_first, d_mask, d_x, d_err, L.w16, d_mag,
-                                                      d_stats, d_queue, stage_words, st);
-        return;
-    }
     if (kw == 1) {
         if (L.unroll >= 2) {
             if (v4) MBIR_LAUNCH(1, 2, 4);
@@ -905,7 +870,7 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 4) icd_batch_kernel(const Batc
         const int sx = K * (rem % hx) + color % K;
         const int sy = K * (rem / hx) + color / K;
         if (sx >= P.L.n_sv_x || sy >= P.L.n_sv_y) continue;
-        icd_update_sv<KW, kUnroll, VEC, false, 2, float>(P.g, P.L, P.K, P.table, P.view_first, P.mask, P.x, P.err, P.w, P.mag,
+        icd_update_sv<KW, kUnroll, VEC, false, 2>(P.g, P.L, P.K, P.table, P.view_first, P.mask, P.x, P.err, P.w, P.mag,
                                                f, sx, sy, S, cnt, nullptr, 0);
     }
     if (cur >= 0) flush_counts(cnt, P.stats);
@@ -957,7 +922,7 @@ int icd_grid(int warps)
     int dev = 0, sms = 148, per_sm = 1;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, icd_phase_kernel<1, 2, 4, false, 0, float>, warps * 32, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, icd_phase_kernel<1, 2, 4, false, 0>, warps * 32, 0);
     return sms * (per_sm > 0 ? per_sm : 1);
 }
 

@@ -32,25 +32,6 @@ __global__ void transpose_rows_cols(const float *__restrict__ in, float *__restr
     }
 }
 
-// w16[i] = w[i] when w[i] is an integer in [0, 65535]; *inexact |= 1 where one is not.
-__global__ void weights_u16_kernel(const float *__restrict__ w, size_t n, uint16_t *__restrict__ w16,
-                                   int *__restrict__ inexact)
-{
-    int bad = 0;
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        const float v = w[i];
-        const bool ok = v >= 0.0f && v <= 65535.0f && v == rintf(v);
-        w16[i] = ok ? (uint16_t)v : (uint16_t)0;
-        bad |= !ok;
-    }
-    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(inexact, 1);
-}
-
-void launch_weights_u16(const float *d_w, size_t n, uint16_t *d_w16, int *d_inexact, cudaStream_t st)
-{
-    weights_u16_kernel<<<148 * 8, 256, 0, st>>>(d_w, n, d_w16, d_inexact);
-}
-
 void launch_transpose_sino(const float *in, float *out, int N_p, int N_t, int N_r, cudaStream_t st)
 {
     dim3 grid((N_r + 31) / 32, (N_t + 31) / 32, N_p), block(32, 8);

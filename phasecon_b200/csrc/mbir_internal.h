@@ -62,9 +62,6 @@ std::string build_setup(HostSetup &hs, const ProblemDesc &pd, const float *angle
                         const float *recon_times, int mult_xy, int mult_z);
 
 // ---- kernel launchers (kernels_*.cu); all asynchronous on `st` -------------
-// d_w16[i] = d_w[i] for weights that are integers in [0, 65535]; *d_inexact
-// (zeroed by the caller) becomes 1 if any weight is not.
-void launch_weights_u16(const float *d_w, size_t n, uint16_t *d_w16, int *d_inexact, cudaStream_t st);
 void launch_transpose_sino(const float *h_layout_dev, float *d_out, int N_p, int N_t, int N_r, cudaStream_t st);
 void launch_untranspose_sino(const float *d_in, float *d_out, int N_p, int N_r, int N_t, cudaStream_t st);
 void launch_vol_to_zfast(const float *d_in, float *d_out, int N_time, int N_z, int N_y, int N_x, cudaStream_t st);
@@ -138,10 +135,6 @@ struct IcdLaunch {
     // null = every SV slot of the phase's colour in every frame
     const uint32_t *items;
     const int *n_items;
-    // the weights as 16-bit integers (every weight an integer in [0, 65535],
-    // so exact), read by the quadratic data term's theta pass; null = the
-    // FP32 weights
-    const uint16_t *w16;
 };
 
 // SV slots of one colour per frame and the items (all frames) of one phase.

@@ -66,7 +66,7 @@ Session::~Session()
     void *ptrs[] = {d_y, d_w, d_err, d_x, d_tmp, d_table, d_Hr, d_cos, d_sin, d_views, d_view_first, d_view_frame,
                     d_mask, d_mag, d_stats, d_cost_partials, d_cost_out, d_flag, d_acc, d_queue, d_filt, d_sel,
                     d_nh_items, d_nh_n, d_nh_scratch, d_nh_selstate, d_off, d_offx, d_onum, d_olam, d_ogamma,
-                    d_var, d_w16};
+                    d_var};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     for (auto &ev : ev_pairs) {
@@ -186,24 +186,6 @@ int Session::init(const mbirgpu_problem *pb, const mbirgpu_options *o, int mult_
     CK(cudaStreamSynchronize(st));
     CK(cudaMemcpyAsync(d_tmp, pb->weights, n_sino * sizeof(float), cudaMemcpyHostToDevice, st));
     launch_transpose_sino(d_tmp, d_w, g.N_p, g.N_t, g.N_r, st);
-    // count weights (integers below 2^16) with the quadratic data term: the
-    // sweep reads an exact 16-bit copy (the generalised-Huber term rescales
-    // the weights as it re-estimates the variance, so it keeps FP32)
-    if (opt.weights16 && !g.huber) {
-        uint16_t *w16 = nullptr;
-        if (dalloc(&w16, n_sino, &acc)) return -1;
-        CK(cudaMemsetAsync(d_flag, 0, sizeof(int), st));
-        launch_weights_u16(d_w, n_sino, w16, d_flag, st);
-        int inexact = 0;
-        CK(cudaMemcpyAsync(&inexact, d_flag, sizeof(int), cudaMemcpyDeviceToHost, st));
-        CK(cudaStreamSynchronize(st));
-        if (inexact) {
-            cudaFree(w16);
-            acc -= n_sino * sizeof(uint16_t);
-        } else {
-            d_w16 = w16;
-        }
-    }
 
     // A table over the assigned views (records of view position i in views[])
     Geom gb = g;
@@ -399,7 +381,6 @@ int Session::enqueue_iteration(int iter, bool graph_mode, int *launches_out)
     L.perm = spread_multiplier(sv_slots(g.N_x, g.N_y, sv, colors));
     L.max_ctas = sv_max_concurrent(g.N_x, g.N_y, g.N_time, sv, colors);
     L.stage_records = opt.stage_records;
-    L.w16 = d_w16;
     const int phases = colors * colors;
     Geom gb = g;
     gb.N_p = n_assigned;
@@ -776,7 +757,6 @@ void mbirgpu_default_options(mbirgpu_options *o)
     o->nh_work_lists = 1;
     o->autotune = 0;
     o->graph_iterations = 1;
-    o->weights16 = 1;
 }
 
 int mbirgpu_set_options(const mbirgpu_options *o)
@@ -787,7 +767,6 @@ int mbirgpu_set_options(const mbirgpu_options *o)
     if (o->sv_size < 0 || o->sv_size > 16) return fail("sv_size must be 0 (auto) or 1..16");
     if (o->cta_warps < 0 || o->cta_warps > 8) return fail("cta_warps must be 0 (auto) or 1..8");
     if (o->icd_unroll < 0 || o->icd_unroll > 4) return fail("icd_unroll must be 0 (auto) or 1..4");
-    if (o->weights16 != 0 && o->weights16 != 1) return fail("weights16 must be 0 or 1");
     if (o->nhicd_passes < 0 || o->nhicd_passes > mbirgpu::kMaxNhPasses)
         return fail("nhicd_passes must be 0 (off) .. %d", mbirgpu::kMaxNhPasses);
     if (o->sv_colors != 0 && o->sv_colors != 2 && o->sv_colors != 4) return fail("sv_colors must be 0 (auto), 2 or 4");
@@ -859,7 +838,6 @@ int mbirgpu_session_info_get(const mbirgpu_session *sp, mbirgpu_session_info *in
     info->sv_size = s->sv;
     info->cta_warps = s->warps;
     info->sv_colors = s->colors;
-    info->weights16 = s->d_w16 != nullptr;
     info->masked_columns = s->masked_columns;
     info->nnz = s->masked_nnz;
     info->delta_t = g.delta_t;

@@ -26,7 +26,6 @@ struct Session {
     bool timing = false;
 
     float *d_y = nullptr, *d_w = nullptr, *d_err = nullptr, *d_x = nullptr, *d_tmp = nullptr;
-    uint16_t *d_w16 = nullptr;  // the weights as exact 16-bit integers, when they all are (options.weights16)
     uint32_t *d_table = nullptr;
     float *d_Hr = nullptr;
     double *d_cos = nullptr, *d_sin = nullptr;

@@ -59,7 +59,7 @@ class Options(C.Structure):
         ("nhicd_passes", C.c_int32), ("sv_colors", C.c_int32), ("stage_records", C.c_int32),
         ("nh_sv_size", C.c_int32), ("nh_sv_colors", C.c_int32), ("nh_cta_warps", C.c_int32),
         ("nh_work_lists", C.c_int32), ("autotune", C.c_int32),
-        ("graph_iterations", C.c_int32), ("weights16", C.c_int32),
+        ("graph_iterations", C.c_int32),
     ]
 
 
@@ -80,7 +80,7 @@ class SessionInfo(C.Structure):
         ("N_y", C.c_int32), ("N_z", C.c_int32), ("mult_xy", C.c_int32), ("mult_z", C.c_int32),
         ("max_views", C.c_int32), ("kmax", C.c_int32), ("sv_size", C.c_int32), ("cta_warps", C.c_int32),
         ("masked_columns", C.c_int64), ("nnz", C.c_int64), ("delta_t", C.c_double), ("device_bytes", C.c_size_t),
-        ("sv_colors", C.c_int32), ("weights16", C.c_int32),
+        ("sv_colors", C.c_int32),
     ]
 
 
