@@ -64,8 +64,8 @@ __device__ __forceinline__ uint64_t mix64(uint64_t z)
 // t3 = c + t1. Takes isq = 1 / sq and isqp = 1 / sqp. The weight is
 // evaluated ~28 times per voxel update, so it uses the hardware base-2
 // logarithm / exponential (one logarithm for both powers) and reciprocal:
-// FP32 arithmetic whose rounding the FP64 MAP cost, the method's judge, does
-// not see.
+// FP32 arithmetic whose rounding the FP64 MAP cost, by which the method's
+// result is measured, does not see.
 __device__ __forceinline__ float lg2_hw(float x)
 {
     float r;

@@ -234,8 +234,8 @@ def warm_start_score(session: Session, net: UNet, icd_iterations: int = 0) -> fl
     becomes net(FBP), then `icd_iterations` plain ICD iterations run (none by
     default: two ICD iterations already level the candidates' costs to within
     0.2 %, while the starting costs differ by 10 % and more and set how many
-    iterations the start needs); returns the FP64 cost (lower is better). The
-    cost function judges the network."""
+    iterations the start needs); returns the FP64 cost (lower is better): the
+    MAP cost function is the measure of the network's error."""
     warm_start(session, net)
     for it in range(1, icd_iterations + 1):
         session.icd_iteration(it)
@@ -244,14 +244,15 @@ def warm_start_score(session: Session, net: UNet, icd_iterations: int = 0) -> fl
 
 def train(net: UNet, pairs, steps: int, lr: float = 1e-3, seed: int = 0, log_every: int = 0,
           average_from: float = 1.0, average_every: int = 50, val_pairs=None, val_every: int = 250,
-          val_session: Session | None = None, scores: list | None = None):
+          val_session: Session | None = None, scores: list | None = None, warmup: int = 0):
     """Adam steps over randomly drawn (input, target) pairs of host arrays;
     returns the loss history. The network's input scale is set so that it
     sees values of order one. Learning rate: a cosine schedule from `lr` down
     to lr / 100 over all steps; with average_from < 1, the cosine runs down to
     lr / 10 over the first average_from of the steps, the rest run at lr / 10
     and the network ends as the average of its weights taken every
-    `average_every` steps over that tail (stochastic weight averaging).
+    `average_every` steps over that tail (stochastic weight averaging). The
+    first `warmup` steps ramp the rate up linearly from lr / warmup.
 
     With `val_session` (a session on a held-out scan, never trained on) or
     `val_pairs` (held-out pairs) the network ends as the candidate with the
@@ -299,6 +300,8 @@ def train(net: UNet, pairs, steps: int, lr: float = 1e-3, seed: int = 0, log_eve
             lr_s = lr * 0.1 if s >= tail else lr * (0.1 + 0.9 * 0.5 * (1.0 + np.cos(np.pi * s / max(1, tail))))
         else:
             lr_s = lr * (0.01 + 0.99 * 0.5 * (1.0 + np.cos(np.pi * s / max(1, steps))))
+        if s < warmup:
+            lr_s *= (s + 1) / warmup
         hist.append(net.train_step(x, t, float(lr_s)))
         if s >= tail and (s - tail) % average_every == average_every - 1:
             p = net.get_params().astype(np.float64)

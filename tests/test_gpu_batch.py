@@ -5,7 +5,7 @@ same seeds) as a session with the same super-voxel size and CTA width. Which
 super-voxels run at the same moment differs (and varies from run to run in
 both), so the trajectories differ slightly; after 40 iterations both are
 converged: final FP64 cost within 2e-4 relative, object RMSE within 0.5 % of
-its dynamic range (the north star's ICD tolerance).
+its dynamic range (the ICD tolerance used against the reference).
 """
 import numpy as np
 import pytest
