@@ -422,6 +422,139 @@ __global__ void pc_rows_inverse(PcDims d, PcArgs A, int epilogue)
         block_add(acc, A.acc + (size_t)v * kPcAccSlots + A.acc_slot, s_red);
 }
 
+// ---------------------------------------------------------------------------- 256-point passes
+// Length-256 transforms (radix 16 x 16) with the data in registers: a thread
+// owns butterfly j (0..15) of one sequence and loads its 16 points x[j + 16p]
+// straight from global memory (the prologue applied on the way), transforms
+// them (stage 1), writes them through shared memory once, reads the stage-2
+// points x[j + 16p] back, twiddles and transforms them, and holds the outputs
+// X[j + 16p] for the epilogue or the global store. The arithmetic is that of
+// the generic passes' two radix-16 stages; one shared-memory exchange per
+// transform instead of four, and one barrier instead of four. A CTA holds 16
+// sequences (256 threads).
+namespace {
+constexpr int kF = 16;  // sequences per CTA and points per thread
+
+// stage 2 of a 256-point transform on this thread's points x[p] = a[j + 16p]:
+// twiddles w_256^(p j) (twiddle index scaled to the table's nmax), then the
+// 16-point DFT; outputs X[j + 16p] in x[p]
+__device__ __forceinline__ void stage2_256(float2 (&x)[kF], int j, const float2 *tw, int nmax, bool inverse)
+{
+    const int sc = nmax >> 8;
+#pragma unroll
+    for (int p = 1; p < kF; p++) x[p] = cmul(twid(tw, p * j * sc, nmax, inverse), x[p]);
+    dft_regs<kF>(x, tw, nmax, inverse);
+}
+}  // namespace
+
+__global__ void __launch_bounds__(256) pc_rows_forward_256(PcDims d, PcArgs A, int prologue)
+{
+    extern __shared__ float2 smem[];
+    const int v = blockIdx.y;
+    if (A.active && !A.active[v]) return;
+    const int S = fft_seq_stride(256);
+    float2 *s_tw = smem, *a = smem + d.nmax;
+    load_twiddles(s_tw, A.tw, d.nmax);
+    const int q = threadIdx.x >> 4, j = threadIdx.x & 15;  // sequence (row) of the CTA, butterfly
+    const int r = blockIdx.x * kF + q;
+    const size_t pb = (size_t)r * 256, vb = (size_t)v * d.N;
+    float2 x[kF];
+#pragma unroll
+    for (int p = 0; p < kF; p++) x[p] = prologue_in(A, prologue, vb + pb + j + 16 * p, pb + j + 16 * p);
+    __syncthreads();  // the twiddle table
+    dft_regs<kF>(x, s_tw, d.nmax, false);  // stage 1 (L = 1): outputs at 16 j + p
+#pragma unroll
+    for (int p = 0; p < kF; p++) a[fpos(q, 16 * j + p, S)] = x[p];
+    __syncthreads();
+#pragma unroll
+    for (int p = 0; p < kF; p++) x[p] = a[fpos(q, j + 16 * p, S)];
+    stage2_256(x, j, s_tw, d.nmax, false);
+#pragma unroll
+    for (int p = 0; p < kF; p++) A.work[vb + pb + j + 16 * p] = x[p];
+}
+
+__global__ void __launch_bounds__(256, 2) pc_cols_filter_256(PcDims d, PcArgs A, const float2 *__restrict__ transfer)
+{
+    extern __shared__ float2 smem[];
+    const int v = blockIdx.y;
+    if (A.active && !A.active[v]) return;
+    const int C = d.C, S = fft_seq_stride(256);
+    float2 *s_tw = smem, *a = smem + d.nmax;
+    load_twiddles(s_tw, A.tw, d.nmax);
+    const int q = threadIdx.x & 15, j = threadIdx.x >> 4;  // column of the CTA (fastest: coalesced), butterfly
+    const int c = blockIdx.x * kF + q;
+    const size_t vb = (size_t)v * d.N;
+    float2 x[kF];
+#pragma unroll
+    for (int p = 0; p < kF; p++) x[p] = A.work[vb + (size_t)(j + 16 * p) * C + c];
+    __syncthreads();  // the twiddle table
+    dft_regs<kF>(x, s_tw, d.nmax, false);
+#pragma unroll
+    for (int p = 0; p < kF; p++) a[fpos(q, 16 * j + p, S)] = x[p];
+    __syncthreads();
+#pragma unroll
+    for (int p = 0; p < kF; p++) x[p] = a[fpos(q, j + 16 * p, S)];
+    stage2_256(x, j, s_tw, d.nmax, false);
+    // the forward outputs X[j + 16p] are the inverse's stage-1 inputs of the
+    // same butterfly j: multiply by the transfer table and go on in registers
+#pragma unroll
+    for (int p = 0; p < kF; p++) x[p] = cmul(x[p], __ldg(transfer + (size_t)(j + 16 * p) * C + c));
+    dft_regs<kF>(x, s_tw, d.nmax, true);
+    __syncthreads();  // every thread has read its stage-2 points
+#pragma unroll
+    for (int p = 0; p < kF; p++) a[fpos(q, 16 * j + p, S)] = x[p];
+    __syncthreads();
+#pragma unroll
+    for (int p = 0; p < kF; p++) x[p] = a[fpos(q, j + 16 * p, S)];
+    stage2_256(x, j, s_tw, d.nmax, true);
+#pragma unroll
+    for (int p = 0; p < kF; p++) A.work[vb + (size_t)(j + 16 * p) * C + c] = x[p];
+}
+
+__global__ void __launch_bounds__(256, 3) pc_rows_inverse_256(PcDims d, PcArgs A, int epilogue)
+{
+    extern __shared__ float2 smem[];
+    __shared__ double s_red[32];
+    const int v = blockIdx.y;
+    if (A.active && !A.active[v]) return;
+    const int S = fft_seq_stride(256);
+    float2 *s_tw = smem, *a = smem + d.nmax;
+    load_twiddles(s_tw, A.tw, d.nmax);
+    const int q = threadIdx.x >> 4, j = threadIdx.x & 15;
+    const int r = blockIdx.x * kF + q;
+    const size_t pb = (size_t)r * 256, vb = (size_t)v * d.N;
+    float2 x[kF];
+#pragma unroll
+    for (int p = 0; p < kF; p++) x[p] = A.work[vb + pb + j + 16 * p];
+    __syncthreads();
+    dft_regs<kF>(x, s_tw, d.nmax, true);
+#pragma unroll
+    for (int p = 0; p < kF; p++) a[fpos(q, 16 * j + p, S)] = x[p];
+    __syncthreads();
+#pragma unroll
+    for (int p = 0; p < kF; p++) x[p] = a[fpos(q, j + 16 * p, S)];
+    stage2_256(x, j, s_tw, d.nmax, true);
+    const float inv_n = 1.0f / (float)d.N;
+    double acc = 0.0;
+    constexpr int kEpi = 4;  // operands of four elements in flight
+#pragma unroll
+    for (int p0 = 0; p0 < kF; p0 += kEpi) {
+        EpiIn in[kEpi];
+#pragma unroll
+        for (int u = 0; u < kEpi; u++) {
+            const size_t e = pb + j + 16 * (p0 + u);
+            in[u] = epilogue_in(A, epilogue, vb + e, e);
+        }
+#pragma unroll
+        for (int u = 0; u < kEpi; u++) {
+            const size_t e = pb + j + 16 * (p0 + u);
+            acc += epilogue_out(d, A, epilogue, vb + e, cscale(x[p0 + u], inv_n), in[u]);
+        }
+    }
+    if (epilogue == PC_OUT_GRAD || epilogue == PC_OUT_SDEN || epilogue == PC_OUT_PCOST)
+        block_add(acc, A.acc + (size_t)v * kPcAccSlots + A.acc_slot, s_red);
+}
+
 // ---------------------------------------------------------------------------- pointwise steps
 // w -= alpha g with alpha = sum|g|^2 / (sum Re(conj g D^H H'^H ..) + nu sum|g|^2 + eps)
 // (compute_stepsize, PCMBIR_3D/XT_PhaseRet.c:126-165); sums |alpha g| and |w|.

@@ -69,6 +69,11 @@ struct PcPrior {
 __global__ void pc_rows_forward(PcDims d, PcArgs A, int prologue);
 __global__ void pc_cols_filter(PcDims d, PcArgs A, const float2 *transfer);
 __global__ void pc_rows_inverse(PcDims d, PcArgs A, int epilogue);
+// the same passes for 256-point sequences with radix-16 stages, the points in
+// registers (16 sequences per 256-thread CTA)
+__global__ void pc_rows_forward_256(PcDims d, PcArgs A, int prologue);
+__global__ void pc_cols_filter_256(PcDims d, PcArgs A, const float2 *transfer);
+__global__ void pc_rows_inverse_256(PcDims d, PcArgs A, int epilogue);
 __global__ void pc_sd_update(PcDims d, PcArgs A);
 __global__ void pc_sd_finish(PcDims d, PcArgs A, int step, float sd_thresh);
 __global__ void pc_pret_prepare(PcDims d, PcArgs A);

@@ -79,9 +79,17 @@ void pc_transform(const PcDims &d, PcArgs A, size_t smem_rows, size_t smem_cols,
     A.out = out;
     A.acc_slot = acc_slot;
     dim3 grows((d.R + d.rows_per_cta - 1) / d.rows_per_cta, d.V), gcols(d.C / d.cols_per_cta, d.V);
-    pc_rows_forward<<<grows, 256, smem_rows, st>>>(d, A, prologue);
-    pc_cols_filter<<<gcols, 256, smem_cols, st>>>(d, A, table);
-    pc_rows_inverse<<<grows, 256, smem_rows, st>>>(d, A, epilogue);
+    // 256-point sequences with radix-16 stages: the register-resident passes
+    // (16 sequences per CTA; the twiddle table and one padded buffer, 37 KB)
+    const bool rows256 = d.C == 256 && d.R % 16 == 0 && d.fft_radix == 16;
+    const bool cols256 = d.R == 256 && d.C % 16 == 0 && d.fft_radix == 16;
+    const size_t smem256 = (size_t)(d.nmax + 16 * fft_seq_stride(256)) * sizeof(float2);
+    if (rows256) pc_rows_forward_256<<<dim3(d.R / 16, d.V), 256, smem256, st>>>(d, A, prologue);
+    else pc_rows_forward<<<grows, 256, smem_rows, st>>>(d, A, prologue);
+    if (cols256) pc_cols_filter_256<<<dim3(d.C / 16, d.V), 256, smem256, st>>>(d, A, table);
+    else pc_cols_filter<<<gcols, 256, smem_cols, st>>>(d, A, table);
+    if (rows256) pc_rows_inverse_256<<<dim3(d.R / 16, d.V), 256, smem256, st>>>(d, A, epilogue);
+    else pc_rows_inverse<<<grows, 256, smem_rows, st>>>(d, A, epilogue);
 }
 
 #define PCK(call)                                                                              \
