@@ -7,9 +7,12 @@
 //   pass 2  cols:  FFT along r (length N_r), multiply by the transfer table,
 //                  inverse FFT along r
 //   pass 3  rows:  inverse FFT along t, scale by 1/(N_r N_t), epilogue op
-// so every pass reads and writes the view once. FFTs are radix-2 Stockham
-// (self-sorting, ping-pong between two shared-memory buffers) with twiddles
-// exp(-2 pi i m / n_max) precomputed in double and rounded once to float.
+// so every pass reads and writes the view once. FFTs are Stockham autosort
+// stages of radix up to 16 (the R points of a butterfly in registers,
+// ping-pong between two shared-memory buffers; for 256-point sequences the
+// points stay in registers with one shared-memory exchange per transform)
+// with twiddles exp(-2 pi i m / n_max) precomputed in double and rounded once
+// to float.
 // Per-view sums needed by the steepest-descent step size and the stopping
 // tests are block-reduced and added in FP64. Views whose loop has stopped
 // (per-view flags) skip every launch.
