@@ -351,7 +351,11 @@ def run_ours(args, world, rank, local, pg):
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": profiled_traffic(), "peak_source": peak_kind, "kernel": "icd_phase_kernel",
                 "algorithmic_bytes_per_launch": bytes_total / icd_launches, "avg_launch_ms": avg_launch_s * 1e3,
-                "bytes_per_voxel_update": bytes_per_update, "icd_launches": icd_launches}
+                "bytes_per_voxel_update": bytes_per_update, "icd_launches": icd_launches,
+                # the captured launch behind `traffic` is one full-sweep colour
+                # phase; its algorithmic bytes are a K-squared-th of a full sweep's
+                "traffic_launch": "one full-sweep colour phase (profiles/icd_phase_kernel_4d.txt)",
+                "algorithmic_bytes_full_phase": (12.0 * entries + 8.0 * full) / phases}
 
     # time to converged cost from zero (plain GPU ICD), FP64 cost every iteration
     conv = {}
